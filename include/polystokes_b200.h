@@ -1,0 +1,165 @@
+/*
+ * polystokes_b200.h -- C-ABI of the B200-native PolyStokes per-timestep hot path.
+ *
+ * One context holds a batch of independent systems ("replicas"); a single
+ * PolyStokes system is a batch of one.  Every vector argument is a DEVICE
+ * pointer to the concatenation of the replicas' segments, each laid out exactly
+ * as the reference lays out its PETSc vectors:
+ *
+ *   saddle vector (length n = 6 Nm + 17 Nc per replica):
+ *     [ F_m (3Nm) | F_c (3Nc) | T_c (3Nc) | S_c (5Nc) | U_m (3Nm) | U_c (3Nc) | W_c (3Nc) ]
+ *   positions: 3 Np doubles per replica (monomers first, then colloids)
+ *   quaternions: 4 Nc doubles per replica
+ *
+ * Return value: 0 success; negative = error (PS_ERR_*); ps_ksp_solve returns the
+ * KSP-style converged reason of the worst replica (>0 converged, <0 diverged).
+ * Streams are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths within sgnagella/polystokes_brownian):
+ *   ps_matmult        <- ArrowheadMult(Mat,Vec,Vec)          src/matfree_A.cpp:38-80
+ *                        and dense MatMult(A) of mm_HI        src/arrays.cpp:371-408, src/mob.cpp:843-1160
+ *   ps_get_diagonal   <- ArrowheadGetDiagonal(Mat,Vec)        src/matfree_A.cpp:84-102
+ *   ps_ksp_solve      <- KSPSolve(ksp,rhs,X), MINRES+Jacobi   src/vel.cpp:7-66, src/init.cpp:27-72
+ *   ps_build_pairs    <- check_dist / build_monomer_cell_list src/check_dist.cpp:12-87, src/cell_list.cpp:23-96
+ *   ps_assemble       <- mob() + sync_mcc_schur_correction()  src/mob.cpp:635-1213, src/slip_vel.cpp:81-203
+ *   ps_rhs            <- RHS(bool drift)                      src/rhs.cpp:246-346
+ *   ps_sqrtm_apply    <- solve_slip_vel()                     src/slip_vel.cpp:19-79,205-477
+ *   ps_step           <- one iteration of the run() loop      src/run.cpp:70-162
+ */
+#ifndef POLYSTOKES_B200_H
+#define POLYSTOKES_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_OK 0
+#define PS_ERR_ARG (-1)
+#define PS_ERR_CUDA (-2)
+#define PS_ERR_NOMEM (-3)
+#define PS_ERR_STATE (-4)
+#define PS_ERR_UNSUPPORTED (-5)
+#define PS_ERR_TOO_LARGE (-6)
+
+/* AB translational block mode: reference-faithful or RPY. */
+#define PS_AB_REFERENCE 0
+#define PS_AB_RPY 1
+
+/* precision of the far-field matvec and Krylov vectors */
+#define PS_PREC_FP64 0
+#define PS_PREC_MIXED 1
+
+/* One system; mirrors PolyStokes(...) + particle_info(...) + trap_info(...)
+ * (src/bindings.cpp:45-91, src/Stokes.cpp:11-252). */
+typedef struct ps_desc {
+    int32_t Nm, Nc, Npoly, Nmono_per_chain;
+    double beta, kT, epsilon, kbond, r0, Lmax, tau;
+    double dt;
+    int32_t mm_HI, chain_HI, fene, tether, mono_ev, record_forces;
+    int32_t box_on;
+    double box[3];
+    double ktrap, tstart, trun, weaken_trap;
+    double t0;          /* start time (restart) */
+    int32_t restart;    /* nonzero: trap centres are not re-derived from x */
+    int32_t ab_mode;    /* PS_AB_REFERENCE | PS_AB_RPY */
+    double hs_kpref;    /* HS_KPREF, default 1.0 */
+    int32_t hs_kmode;   /* HS_KMODE, default 0 */
+    int32_t lanczos_nc; /* POLYSTOKES_LANCZOS_NC, default 64 */
+    int32_t lub_on;     /* near-field lubrication (not in the reference) */
+    double lub_gap;     /* lubricated pairs: gap < lub_gap * radius */
+} ps_desc;
+
+typedef struct ps_ksp_opts {
+    double rtol;        /* relative tolerance (reference hard-codes 1e-6) */
+    int32_t maxit;      /* iteration cap (PETSc default 10000) */
+    int32_t warm;       /* nonzero: x holds the initial guess */
+    int32_t check_every;/* host convergence poll period in iterations (0 = 8) */
+} ps_ksp_opts;
+
+typedef struct ps_ksp_result {
+    int32_t reason;     /* worst replica reason */
+    int32_t iters_max;  /* max iterations over replicas */
+    int64_t iters_sum;  /* sum of iterations over replicas */
+    double rnorm_max;   /* largest final residual-norm estimate */
+} ps_ksp_result;
+
+typedef struct ps_sqrt_opts {
+    int32_t kmax;       /* Lanczos subspace cap */
+    double tol;         /* relative change between successive estimates */
+} ps_sqrt_opts;
+
+typedef struct ps_sqrt_result {
+    int32_t iters_max;
+    int32_t nneg;       /* negative projected eigenvalues floored (sum over replicas) */
+} ps_sqrt_result;
+
+/* Optional injected noise for one step (device pointers, concatenated per
+ * replica); NULL members are drawn on the device from the context's seed. */
+typedef struct ps_step_inputs {
+    const double *fb;   /* nm3nc11 per replica: slip-velocity white noise (slip_vel.cpp:11-17) */
+    const double *wrfd; /* nm3nc6 per replica: RFD displacement (drift.cpp:9-15) */
+    const double *zlub; /* 6 or 12 per lubricated pair, canonical pair order */
+    double rtol;        /* MINRES rtol for the five solves */
+    int32_t maxit;
+} ps_step_inputs;
+
+typedef struct ps_step_result {
+    int32_t iters[5];   /* max over replicas, per solve */
+    int32_t reason;     /* worst KSP reason over the five solves */
+} ps_step_result;
+
+typedef struct ps_ctx ps_ctx;
+
+/* context ------------------------------------------------------------------ */
+int ps_ctx_create(const ps_desc *descs, int32_t nrep, int32_t precision, ps_ctx **out);
+int ps_ctx_destroy(ps_ctx *ctx);
+int ps_ctx_sizes(const ps_ctx *ctx, int64_t *out8); /* ntot_beads, nvec, ntop, nvel, ncoll, nrep, 0, 0 */
+int ps_ctx_offsets(const ps_ctx *ctx, int32_t rep, int64_t *out4); /* bead, vec, top, vel offsets */
+int ps_set_lub_table(ps_ctx *ctx, const double *host_tab, int32_t nrow, int32_t ncol);
+int ps_set_seed(ps_ctx *ctx, uint64_t seed);
+const char *ps_last_error(void);
+
+/* state --------------------------------------------------------------------- */
+int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream);
+int ps_get_state(ps_ctx *ctx, double *x, double *q, void *stream);
+int ps_set_time(ps_ctx *ctx, double t);
+
+/* stage pieces (check_dist, RHS, mob) --------------------------------------- */
+int ps_build_pairs(ps_ctx *ctx, void *stream);
+int ps_pair_list(ps_ctx *ctx, int32_t which, int32_t *pi, int32_t *pj, int64_t maxp,
+                 int64_t *count, void *stream);  /* which: 0 Verlet, 1 monomer WCA, 2 lubrication */
+int ps_rhs(ps_ctx *ctx, int32_t drift, const double *fext, double *rhs, void *stream);
+int ps_assemble(ps_ctx *ctx, void *stream);
+
+/* operator and solver (MatShell MatMult / GetDiagonal / KSPSolve) ----------- */
+int ps_matmult(ps_ctx *ctx, const double *x, double *y, void *stream);
+int ps_mobility_apply(ps_ctx *ctx, const double *u, double *y, void *stream);
+int ps_get_diagonal(ps_ctx *ctx, double *d, void *stream);
+int ps_ksp_solve(ps_ctx *ctx, const double *b, double *x, const ps_ksp_opts *opts,
+                 ps_ksp_result *res, void *stream);
+
+/* Brownian noise: w = M^{1/2} z (unscaled), as solve_slip_vel before scaling */
+int ps_sqrtm_apply(ps_ctx *ctx, const double *z, double *w, const ps_sqrt_opts *opts,
+                   ps_sqrt_result *res, void *stream);
+
+/* one predictor-corrector step of every replica */
+int ps_step(ps_ctx *ctx, const ps_step_inputs *in, ps_step_result *res, void *stream);
+int ps_step_outputs(ps_ctx *ctx, double *up, double *udiff, double *sb, double *fext, void *stream);
+
+/* diagnostics ---------------------------------------------------------------
+ * ps_time_kernel: average device time (ms, CUDA events on `stream`) of `reps`
+ * launches of one far-field kernel on mobility-layout input u; which: 0 the
+ * monomer-monomer pair kernel, 1 monomer-colloid, 2 colloid-colloid, 3 the whole
+ * mobility apply.  ps_fma_peak: measured FMA throughput (TFLOP/s) of the current
+ * device, FP64 when fp64 != 0, else FP32. */
+int ps_time_kernel(ps_ctx *ctx, int32_t which, int32_t reps, const double *u, double *ms, void *stream);
+int ps_fma_peak(int32_t fp64, double *tflops, void *stream);
+/* number of kernels the library has launched since it was loaded */
+uint64_t ps_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,644 @@
+// krylov.cu -- batched preconditioned MINRES (KSPSolve stand-in) and the
+// Lanczos square root M^{1/2} z, with device-side per-replica scalars and
+// convergence flags.
+//
+// MINRES follows the preconditioned Paige & Saunders (1975) recurrences with
+// PETSc KSPMINRES semantics (src/ksp/ksp/impls/minres of PETSc 3.22+; called
+// from src/vel.cpp:41-43 of the reference with PCJACOBI fix-diagonal,
+// src/init.cpp:217-241): convergence when ||B r0||_2 * prod|s_k| <= rtol * ref,
+// ref = ||B r0|| for a zero guess and ||B b|| for a nonzero guess.
+//
+// Reductions are segmented per replica: each block covers a contiguous range of
+// one replica; the last block of a replica to arrive (atomic counter) sums the
+// partials in fixed order and runs that replica's scalar update, so the result
+// never depends on other replicas or on block scheduling.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include "ps_internal.h"
+#include "ps_kernels.h"
+
+namespace ps {
+
+constexpr int RB_THREADS = 256;
+constexpr int RB_EPT = 4;                       // elements per thread
+constexpr int RB_SPAN = RB_THREADS * RB_EPT;    // elements per block
+
+int build_red_table(Engine &E, RedTable &T, bool top)
+{
+    std::vector<RBlk> blk;
+    std::vector<int> first(E.R), cnt(E.R);
+    for (int r = 0; r < E.R; r++) {
+        const Seg &s = E.segs[r];
+        int n = top ? s.nm3nc11 : s.n, off = top ? s.top_off : s.vec_off;
+        first[r] = (int)blk.size();
+        int nb = (n + RB_SPAN - 1) / RB_SPAN;
+        if (nb == 0) nb = 1;
+        for (int b = 0; b < nb; b++) {
+            int st = b * RB_SPAN, len = std::min(RB_SPAN, n - st);
+            if (len < 0) len = 0;
+            blk.push_back({r, off + st, len});
+        }
+        cnt[r] = nb;
+    }
+    T.nblk = (int)blk.size();
+    PS_CK(cudaMalloc(&T.d_blk, sizeof(RBlk) * T.nblk));
+    PS_CK(cudaMalloc(&T.d_first, sizeof(int) * E.R));
+    PS_CK(cudaMalloc(&T.d_count, sizeof(int) * E.R));
+    PS_CK(cudaMalloc(&T.d_counter, sizeof(int) * E.R));
+    PS_CK(cudaMalloc(&T.d_part, sizeof(double) * 65 * T.nblk));   // 4 for scalar sums, 65 for Lanczos dots
+    PS_CK(cudaMemcpy(T.d_blk, blk.data(), sizeof(RBlk) * T.nblk, cudaMemcpyHostToDevice));
+    PS_CK(cudaMemcpy(T.d_first, first.data(), sizeof(int) * E.R, cudaMemcpyHostToDevice));
+    PS_CK(cudaMemcpy(T.d_count, cnt.data(), sizeof(int) * E.R, cudaMemcpyHostToDevice));
+    PS_CK(cudaMemset(T.d_counter, 0, sizeof(int) * E.R));
+    return PS_OK;
+}
+
+void free_red_table(RedTable &T)
+{
+    cudaFree(T.d_blk); cudaFree(T.d_first); cudaFree(T.d_count); cudaFree(T.d_counter); cudaFree(T.d_part);
+    T = RedTable();
+}
+
+// Block-level sum of NV values; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[NV])
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+        double t = v[q];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) sh[wid][q] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            double t = 0;
+            for (int w = 0; w < RB_THREADS / 32; w++) t += sh[w][q];
+            v[q] = t;
+        }
+    }
+}
+
+// Writes this block's partials and returns true in thread 0 of the last block
+// of its replica; that thread then holds the replica totals in tot[].
+template <int NV>
+__device__ __forceinline__ bool finish_block(const RedTable &T, const RBlk &b, int bid, double (&v)[NV], double (&tot)[NV])
+{
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NV; q++) T.d_part[4 * bid + q] = v[q];
+        __threadfence();
+        int t = atomicAdd(&T.d_counter[b.rep], 1);
+        last = (t == T.d_count[b.rep] - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        int f = T.d_first[b.rep], c = T.d_count[b.rep];
+        for (int q = 0; q < NV; q++) tot[q] = 0.0;
+        for (int k = 0; k < c; k++)
+            for (int q = 0; q < NV; q++) tot[q] += ((volatile double *)T.d_part)[4 * (f + k) + q];
+        T.d_counter[b.rep] = 0;
+        return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// generic segmented dot: out[rep] = a.b
+__global__ void k_seg_dot(RedTable T, const double *__restrict__ a, const double *__restrict__ b, double *out)
+{
+    __shared__ double sh[RB_THREADS / 32][1];
+    const RBlk B = T.d_blk[blockIdx.x];
+    double v[1] = {0.0};
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) v[0] += a[B.start + e] * b[B.start + e];
+    block_sum<1>(v, sh);
+    double tot[1];
+    if (finish_block<1>(T, B, blockIdx.x, v, tot)) out[B.rep] = tot[0];
+}
+
+void seg_dot(Engine &E, RedTable &T, const double *a, const double *b, double *out, cudaStream_t st)
+{
+    ::ps_launch_count++, k_seg_dot<<<T.nblk, RB_THREADS, 0, st>>>(T, a, b, out);
+}
+
+// ---------------------------------------------------------------------------
+// MINRES
+__global__ void k_mr_init(RedTable T, const Seg *segs, const double *__restrict__ b, const double *__restrict__ Ax,
+                          const double *__restrict__ D, double *__restrict__ r, double *__restrict__ z,
+                          double *__restrict__ x, MinresScal *mr, int warm, double rtol, int maxit,
+                          double *__restrict__ v, double *__restrict__ w0, double *__restrict__ w1,
+                          double *__restrict__ w2, double *__restrict__ sinv)
+{
+    __shared__ double sh[RB_THREADS / 32][3];
+    const RBlk B = T.d_blk[blockIdx.x];
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        long k = B.start + e;
+        double bk = b[k], rk, dk = D[k];
+        if (warm) rk = bk - Ax[k];
+        else { rk = bk; x[k] = 0.0; }
+        double zk = rk / dk;
+        r[k] = rk; z[k] = zk;
+        v[k] = 0.0; w0[k] = 0.0; w1[k] = 0.0; w2[k] = 0.0;
+        s[0] += zk * zk;
+        s[1] += rk * zk;
+        double bz = bk / dk;
+        s[2] += bz * bz;
+    }
+    block_sum<3>(s, sh);
+    double tot[3];
+    if (finish_block<3>(T, B, blockIdx.x, s, tot)) {
+        MinresScal m = {};
+        double np0 = sqrt(tot[0]);
+        double ref = warm ? sqrt(tot[2]) : np0;
+        double ttol = rtol * ref;
+        if (ttol < 1e-50) ttol = 1e-50;
+        m.np = np0; m.ttol = ttol; m.it = 0; m.pending = 0;
+        (void)maxit;
+        if (tot[1] < 0) { m.done = 1; m.reason = -8; }
+        else if (np0 <= ttol || tot[1] == 0.0) { m.done = 1; m.reason = 2; }
+        else {
+            m.done = 0; m.reason = 0;
+            m.beta = sqrt(tot[1]); m.oldb = 0; m.dbar = 0; m.epsln = 0; m.phibar = m.beta;
+            m.cs = -1; m.sn = 0; m.sinv = 1.0 / m.beta;
+        }
+        mr[B.rep] = m;
+        sinv[B.rep] = m.sinv;
+    }
+}
+
+// (b) of iteration k: pending w/x update of iteration k-1, v = z/beta,
+// Av -= (beta/oldb) r_{k-1}, alfa = v.Av
+__global__ void k_mr_alpha(RedTable T, const double *__restrict__ z, double *__restrict__ v,
+                           double *__restrict__ Av, const double *__restrict__ rkm1, double *__restrict__ wnew,
+                           const double *__restrict__ w1, const double *__restrict__ w2, double *__restrict__ x,
+                           MinresScal *mr, int k)
+{
+    __shared__ double sh[RB_THREADS / 32][1];
+    const RBlk B = T.d_blk[blockIdx.x];
+    const MinresScal m = mr[B.rep];
+    double s[1] = {0.0};
+    const bool upd = m.pending != 0;
+    const bool act = !m.done;
+    const double c1 = (k >= 2) ? m.beta / m.oldb : 0.0;
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        long q = B.start + e;
+        if (upd) {
+            double wn = (v[q] - m.up_oldeps * w1[q] - m.up_delta * w2[q]) * m.up_ginv;
+            wnew[q] = wn;
+            x[q] += m.up_phi * wn;
+        }
+        if (act) {
+            double vq = z[q] * m.sinv;
+            double a = Av[q];
+            if (k >= 2) a -= c1 * rkm1[q];
+            v[q] = vq;
+            Av[q] = a;
+            s[0] += vq * a;
+        }
+    }
+    block_sum<1>(s, sh);
+    double tot[1];
+    if (finish_block<1>(T, B, blockIdx.x, s, tot)) {
+        if (upd) mr[B.rep].pending = 0;
+        if (act) mr[B.rep].alfa = tot[0];
+    }
+}
+
+// (c) of iteration k: r_{k+1} = Av - (alfa/beta) r_k, z = r_{k+1}/D,
+// beta_{k+1} = sqrt(r_{k+1}.z), Givens rotation, convergence test.
+__global__ void k_mr_beta(RedTable T, double *__restrict__ Av, const double *__restrict__ rk,
+                          const double *__restrict__ D, double *__restrict__ z, MinresScal *mr, int maxit,
+                          int *nactive, double *__restrict__ sinv)
+{
+    __shared__ double sh[RB_THREADS / 32][1];
+    const RBlk B = T.d_blk[blockIdx.x];
+    const MinresScal m0 = mr[B.rep];
+    double s[1] = {0.0};
+    const bool act = !m0.done;
+    if (act) {
+        const double c2 = m0.alfa / m0.beta;
+        for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+            long q = B.start + e;
+            double a = Av[q] - c2 * rk[q];
+            double zq = a / D[q];
+            Av[q] = a;
+            z[q] = zq;
+            s[0] += a * zq;
+        }
+    }
+    block_sum<1>(s, sh);
+    double tot[1];
+    if (finish_block<1>(T, B, blockIdx.x, s, tot)) {
+        if (!act) return;
+        MinresScal m = m0;
+        m.it += 1;
+        double bb = tot[0];
+        m.oldb = m.beta;
+        if (bb < 0) { m.done = 1; m.reason = -8; mr[B.rep] = m; atomicSub(nactive, 1); return; }
+        m.beta = sqrt(bb);
+        double oldeps = m.epsln;
+        double delta = m.cs * m.dbar + m.sn * m.alfa;
+        double gbar = m.sn * m.dbar - m.cs * m.alfa;
+        m.epsln = m.sn * m.beta;
+        m.dbar = -m.cs * m.beta;
+        double gamma = sqrt(gbar * gbar + m.beta * m.beta);
+        if (gamma < 2.2250738585072014e-308) gamma = 2.2250738585072014e-308;
+        m.cs = gbar / gamma;
+        m.sn = m.beta / gamma;
+        double phi = m.cs * m.phibar;
+        m.phibar = m.sn * m.phibar;
+        m.up_oldeps = oldeps; m.up_delta = delta; m.up_ginv = 1.0 / gamma; m.up_phi = phi;
+        m.pending = 1;
+        m.np = m.np * fabs(m.sn);
+        if (m.np <= m.ttol) { m.done = 1; m.reason = 2; }
+        else if (m.beta == 0.0) { m.done = 1; m.reason = 3; }
+        else if (m.it >= maxit) { m.done = 1; m.reason = -3; }
+        m.sinv = m.beta != 0.0 ? 1.0 / m.beta : 0.0;
+        mr[B.rep] = m;
+        sinv[B.rep] = m.sinv;
+        if (m.done) atomicSub(nactive, 1);
+    }
+}
+
+// final pending update (after the last iteration)
+__global__ void k_mr_flush(RedTable T, const double *__restrict__ v, double *__restrict__ wnew,
+                           const double *__restrict__ w1, const double *__restrict__ w2, double *__restrict__ x,
+                           MinresScal *mr)
+{
+    __shared__ double sh[RB_THREADS / 32][1];
+    const RBlk B = T.d_blk[blockIdx.x];
+    const MinresScal m = mr[B.rep];
+    if (m.pending) {
+        for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+            long q = B.start + e;
+            double wn = (v[q] - m.up_oldeps * w1[q] - m.up_delta * w2[q]) * m.up_ginv;
+            wnew[q] = wn;
+            x[q] += m.up_phi * wn;
+        }
+    }
+    double s[1] = {0.0};
+    block_sum<1>(s, sh);
+    double tot[1];
+    if (finish_block<1>(T, B, blockIdx.x, s, tot)) mr[B.rep].pending = 0;
+}
+
+int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res, cudaStream_t st)
+{
+    ps_ksp_opts opt = {1e-6, 10000, 0, 8};
+    if (o) opt = *o;
+    if (opt.check_every <= 0) opt.check_every = 8;
+    if (opt.maxit <= 0) opt.maxit = 10000;
+    RedTable &T = E.red;
+    int rc = diag_saddle(E, E.d_D, st);
+    if (rc) return rc;
+    const double *Ax = nullptr;
+    if (opt.warm) {
+        apply_operator(E, 0, x, E.d_Rr[2], nullptr, false, st);
+        Ax = E.d_Rr[2];
+    }
+    // r_1 in slot 1 (slot k % 3 holds r_k)
+    ::ps_launch_count++, k_mr_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, b, Ax, E.d_D, E.d_Rr[1], E.d_z, x, E.d_mr, opt.warm,
+                                            opt.rtol, opt.maxit, E.d_v, E.d_W[0], E.d_W[1], E.d_W[2],
+                                            E.d_sinv);
+    PS_CK(cudaGetLastError());
+    // count active replicas
+    std::vector<MinresScal> hm(E.R);
+    PS_CK(cudaMemcpyAsync(hm.data(), E.d_mr, sizeof(MinresScal) * E.R, cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    int nact = 0;
+    for (auto &m : hm) nact += !m.done;
+    *E.h_nactive = nact;
+    PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
+    int k = 0;
+    while (nact > 0 && k < opt.maxit) {
+        for (int j = 0; j < opt.check_every && k < opt.maxit; j++) {
+            k++;
+            double *Av = E.d_Rr[(k + 1) % 3];
+            const double *rk = E.d_Rr[k % 3];
+            const double *rkm1 = E.d_Rr[(k + 2) % 3];
+            // iteration k-1's update writes w_{k-1} into slot (k-1)%3; w_{k-2}, w_{k-3}... in the others
+            double *wnew = E.d_W[(k + 2) % 3];
+            const double *w1 = E.d_W[(k + 0) % 3];   // w_{k-3}
+            const double *w2 = E.d_W[(k + 1) % 3];   // w_{k-2}
+            // A v_k = (1/beta_k) A z_k: the operator applies the per-replica scale
+            apply_operator(E, 0, E.d_z, Av, E.d_sinv, E.precision == PS_PREC_MIXED, st);
+            ::ps_launch_count++, k_mr_alpha<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_z, E.d_v, Av, rkm1, wnew, w1, w2, x, E.d_mr, k);
+            ::ps_launch_count++, k_mr_beta<<<T.nblk, RB_THREADS, 0, st>>>(T, Av, rk, E.d_D, E.d_z, E.d_mr, opt.maxit, E.d_nactive,
+                                                    E.d_sinv);
+        }
+        PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PS_CK(cudaStreamSynchronize(st));
+        nact = *E.h_nactive;
+    }
+    // the last iteration's pending update: w_k into slot (k+3)%3 == k%3 ... uses w_{k-1}, w_{k-2}
+    {
+        int kk = k + 1;
+        double *wnew = E.d_W[(kk + 2) % 3];
+        const double *w1 = E.d_W[(kk + 0) % 3];
+        const double *w2 = E.d_W[(kk + 1) % 3];
+        ::ps_launch_count++, k_mr_flush<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_v, wnew, w1, w2, x, E.d_mr);
+    }
+    PS_CK(cudaMemcpyAsync(hm.data(), E.d_mr, sizeof(MinresScal) * E.R, cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    PS_CK(cudaGetLastError());
+    int worst = 1000, itmax = 0;
+    long itsum = 0;
+    double rmax = 0;
+    for (auto &m : hm) {
+        int reason = m.done ? m.reason : -3;
+        if (reason < worst) worst = reason;
+        itmax = std::max(itmax, m.it);
+        itsum += m.it;
+        rmax = std::max(rmax, m.np);
+    }
+    if (res) { res->reason = worst; res->iters_max = itmax; res->iters_sum = itsum; res->rnorm_max = rmax; }
+    return worst;
+}
+
+
+// ---------------------------------------------------------------------------
+// Lanczos square root w = M^{1/2} z on the mobility vectors (top layout), full
+// two-pass Gram-Schmidt reorthogonalisation, projected spectrum floored at 0
+// (the policy of schur_sqrt_lanczos, slip_vel.cpp:351-477, applied to the full
+// grand mobility instead of SLEPc MFN/FNSQRT, slip_vel.cpp:27-49).
+struct LzScal {
+    double b0;
+    int m, done, nneg;
+};
+constexpr int LZ_KMAX = 64;
+
+// per block: partial dots of q against V_0..V_j, then last block stores h[]
+__global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, const double *__restrict__ q, int j,
+                          const LzScal *__restrict__ lz, double *__restrict__ h)
+{
+    __shared__ double sh[RB_THREADS / 32][LZ_KMAX + 1];
+    __shared__ bool last;
+    const RBlk B = T.d_blk[blockIdx.x];
+    const bool act = !lz[B.rep].done;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = 0; i <= j; i++) {
+        double v = 0.0;
+        if (act)
+            for (int e = threadIdx.x; e < B.len; e += RB_THREADS) v += V[(long)i * ldv + B.start + e] * q[B.start + e];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[wid][i] = v;
+    }
+    __syncthreads();
+    // block partial for i stored at d_part[(LZ_KMAX+1) * blk + i]
+    if (threadIdx.x <= j) {
+        double t = 0;
+        for (int w = 0; w < RB_THREADS / 32; w++) t += sh[w][threadIdx.x];
+        T.d_part[(long)(LZ_KMAX + 1) * blockIdx.x + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = atomicAdd(&T.d_counter[B.rep], 1);
+        last = (t == T.d_count[B.rep] - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    int f = T.d_first[B.rep], c = T.d_count[B.rep];
+    if (threadIdx.x <= j) {
+        double t = 0;
+        for (int k = 0; k < c; k++) t += ((volatile double *)T.d_part)[(long)(LZ_KMAX + 1) * (f + k) + threadIdx.x];
+        h[(long)(LZ_KMAX + 1) * B.rep + threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) T.d_counter[B.rep] = 0;
+}
+
+// q -= sum_i h_i V_i ; accumulate h_j into the Lanczos diagonal
+__global__ void k_lz_sub(RedTable T, const double *__restrict__ V, long ldv, double *__restrict__ q, int j,
+                         const LzScal *__restrict__ lz, const double *__restrict__ h, double *__restrict__ alpha, int first)
+{
+    const RBlk B = T.d_blk[blockIdx.x];
+    if (lz[B.rep].done) return;
+    const double *hr = h + (long)(LZ_KMAX + 1) * B.rep;
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        double acc = q[B.start + e];
+        for (int i = 0; i <= j; i++) acc -= hr[i] * V[(long)i * ldv + B.start + e];
+        q[B.start + e] = acc;
+    }
+    if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start))
+        alpha[(long)LZ_KMAX * B.rep + j] = (first ? 0.0 : alpha[(long)LZ_KMAX * B.rep + j]) + hr[j];
+}
+
+// V_{j+1} = q / ||q||; beta_j = ||q||  (norm from nrm[rep])
+__global__ void k_lz_next(RedTable T, double *__restrict__ V, long ldv, const double *__restrict__ q, int j,
+                          LzScal *__restrict__ lz, const double *__restrict__ nrm2, double *__restrict__ betad)
+{
+    const RBlk B = T.d_blk[blockIdx.x];
+    if (lz[B.rep].done) return;
+    double bj = sqrt(nrm2[B.rep]);
+    double inv = bj > 0 ? 1.0 / bj : 0.0;
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) V[(long)(j + 1) * ldv + B.start + e] = q[B.start + e] * inv;
+    if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start)) betad[(long)LZ_KMAX * B.rep + j] = bj;
+}
+
+__global__ void k_lz_init(RedTable T, const Seg *__restrict__ segs, double *__restrict__ V,
+                          const double *__restrict__ z, LzScal *__restrict__ lz, const double *__restrict__ nrm2)
+{
+    const RBlk B = T.d_blk[blockIdx.x];
+    // shell replicas take the block-Cholesky noise path instead
+    const bool skip = !segs[B.rep].mm_HI;
+    double b0 = sqrt(nrm2[B.rep]);
+    double inv = b0 > 0 ? 1.0 / b0 : 0.0;
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) V[B.start + e] = z[B.start + e] * inv;
+    if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start)) {
+        lz[B.rep].b0 = skip ? 0.0 : b0; lz[B.rep].m = 0; lz[B.rep].done = (b0 == 0.0 || skip); lz[B.rep].nneg = 0;
+    }
+}
+
+// Implicit QL (symmetric tridiagonal, Wilkinson shift) on one warp: lane 0
+// runs the scalar recurrences, all lanes rotate the eigenvector columns.
+__device__ void warp_tql(double *d, double *e, double *Z, int n)
+{
+    const int lane = threadIdx.x & 31;
+    for (int k = lane; k < n * n; k += 32) Z[k] = (k / n == k % n) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int l = 0; l < n; l++) {
+        int iter = 0;
+        while (true) {
+            int m = l;
+            if (lane == 0) {
+                for (m = l; m < n - 1; m++) {
+                    double dd = fabs(d[m]) + fabs(d[m + 1]);
+                    if (fabs(e[m]) <= 1e-16 * dd) break;
+                }
+            }
+            m = __shfl_sync(0xffffffffu, m, 0);
+            if (m == l || iter++ >= 60) break;
+            double g = 0, r = 0, s = 1, c = 1, p = 0;
+            if (lane == 0) {
+                g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+                r = hypot(g, 1.0);
+                g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+            }
+            int i, brk = 0;
+            for (i = m - 1; i >= l; i--) {
+                if (lane == 0) {
+                    double f = s * e[i], b = c * e[i];
+                    r = hypot(f, g);
+                    e[i + 1] = r;
+                    if (r == 0.0) { d[i + 1] -= p; e[m] = 0.0; brk = 1; }
+                    else {
+                        s = f / r; c = g / r;
+                        g = d[i + 1] - p;
+                        r = (d[i] - g) * s + 2.0 * c * b;
+                        p = s * r;
+                        d[i + 1] = g + p;
+                        g = c * r - b;
+                    }
+                }
+                brk = __shfl_sync(0xffffffffu, brk, 0);
+                if (brk) break;
+                double ss = __shfl_sync(0xffffffffu, s, 0), cc = __shfl_sync(0xffffffffu, c, 0);
+                for (int k = lane; k < n; k += 32) {
+                    double f = Z[k * n + i + 1];
+                    Z[k * n + i + 1] = ss * Z[k * n + i] + cc * f;
+                    Z[k * n + i] = cc * Z[k * n + i] - ss * f;
+                }
+                __syncwarp();
+            }
+            if (brk) continue;
+            if (lane == 0) { d[l] -= p; e[l] = g; e[m] = 0.0; }
+            __syncwarp();
+        }
+    }
+}
+
+// one warp per replica: eig of T_m, g = b0 U sqrt(max(theta,0)) U^T e1,
+// convergence ||g - g_prev|| <= tol ||g|| (the Lanczos basis is orthonormal)
+__global__ void k_lz_check(int R, LzScal *__restrict__ lz, const double *__restrict__ alpha,
+                           const double *__restrict__ betad, double *__restrict__ gbuf, int m, double tol, int final_)
+{
+    extern __shared__ double sm[];
+    const int r = blockIdx.x;
+    if (lz[r].done && !final_) return;
+    const int lane = threadIdx.x;
+    int mr = lz[r].done ? lz[r].m : m;
+    if (mr <= 0) return;
+    double *d = sm, *e = sm + LZ_KMAX, *Z = sm + 2 * LZ_KMAX;
+    for (int i = lane; i < mr; i += 32) {
+        d[i] = alpha[(long)LZ_KMAX * r + i];
+        e[i] = (i < mr - 1) ? betad[(long)LZ_KMAX * r + i] : 0.0;
+    }
+    __syncwarp();
+    warp_tql(d, e, Z, mr);
+    __syncwarp();
+    double *g = gbuf + (long)(LZ_KMAX + 1) * r;   // g[0..m-1], g[LZ_KMAX] = |g|^2 of previous
+    double diff2 = 0, nrm2 = 0;
+    int nneg = 0;
+    for (int i = lane; i < LZ_KMAX; i += 32) {
+        double gi = 0;
+        if (i < mr) {
+            for (int j = 0; j < mr; j++) {
+                double th = d[j];
+                double sq = th > 0 ? sqrt(th) : 0.0;
+                gi += Z[i * mr + j] * sq * Z[0 * mr + j];
+            }
+            gi *= lz[r].b0;
+        }
+        double old = g[i];
+        diff2 += (gi - old) * (gi - old);
+        nrm2 += gi * gi;
+        if (i < mr) g[i] = gi;
+    }
+    for (int j = lane; j < mr; j += 32) nneg += d[j] < 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+        diff2 += __shfl_down_sync(0xffffffffu, diff2, o);
+        nrm2 += __shfl_down_sync(0xffffffffu, nrm2, o);
+        nneg += __shfl_down_sync(0xffffffffu, nneg, o);
+    }
+    if (lane == 0) {
+        lz[r].nneg = nneg;
+        if (!lz[r].done) {
+            lz[r].m = mr;
+            if (final_ || sqrt(diff2) <= tol * sqrt(nrm2)) lz[r].done = 1;
+        }
+    }
+}
+
+// w = V g (top layout)
+__global__ void k_lz_combine(RedTable T, const double *__restrict__ V, long ldv, const LzScal *__restrict__ lz,
+                             const double *__restrict__ gbuf, double *__restrict__ w)
+{
+    const RBlk B = T.d_blk[blockIdx.x];
+    const int m = lz[B.rep].m;
+    const double *g = gbuf + (long)(LZ_KMAX + 1) * B.rep;
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        double acc = 0;
+        for (int i = 0; i < m; i++) acc += g[i] * V[(long)i * ldv + B.start + e];
+        w[B.start + e] = (lz[B.rep].b0 == 0.0) ? 0.0 : acc;
+    }
+}
+
+// breakdown: ||q|| tiny -> invariant subspace, stop extending
+__global__ void k_lz_breakdown(int R, LzScal *__restrict__ lz, const double *__restrict__ nrm2, int j)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R || lz[r].done) return;
+    lz[r].m = j + 1;
+    if (sqrt(nrm2[r]) <= 1e-12 * lz[r].b0) lz[r].done = 2;   // 2: finalise with m = j+1
+}
+
+int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st)
+{
+    int kmax = o && o->kmax > 0 ? o->kmax : 40;
+    double tol = o && o->tol > 0 ? o->tol : 1e-6;
+    if (kmax > LZ_KMAX) kmax = LZ_KMAX;
+    RedTable &T = E.red_top;
+    long ldv = E.ntop;
+    double *V = E.d_lzV, *q = E.d_lzq;
+    LzScal *lz = (LzScal *)E.d_lzs;
+    double *h = E.d_lzT;                                    // [R][LZ_KMAX+1]
+    double *alpha = h + (long)(LZ_KMAX + 1) * E.R;          // [R][LZ_KMAX]
+    double *betad = alpha + (long)LZ_KMAX * E.R;            // [R][LZ_KMAX]
+    double *gbuf = betad + (long)LZ_KMAX * E.R;             // [R][LZ_KMAX+1]
+    double *nrm2 = gbuf + (long)(LZ_KMAX + 1) * E.R;        // [R]
+    seg_dot(E, T, z, z, nrm2, st);
+    ::ps_launch_count++, k_lz_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, V, z, lz, nrm2);
+    PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
+    int check = 4;
+    size_t smem = sizeof(double) * (2 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
+    std::vector<LzScal> hl(E.R);
+    int j = 0;
+    for (j = 0; j < kmax; j++) {
+        apply_operator(E, 1, V + (long)j * ldv, q, nullptr, E.precision == PS_PREC_MIXED, st);
+        for (int pass = 0; pass < 2; pass++) {
+            ::ps_launch_count++, k_lz_dots<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h);
+            ::ps_launch_count++, k_lz_sub<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h, alpha, pass == 0);
+        }
+        seg_dot(E, T, q, q, nrm2, st);
+        ::ps_launch_count++, k_lz_breakdown<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, nrm2, j);
+        if (j + 1 < kmax) ::ps_launch_count++, k_lz_next<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, nrm2, betad);
+        if ((j + 1) % check == 0 || j + 1 == kmax) {
+            ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, j + 1, tol, j + 1 == kmax);
+            PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
+            PS_CK(cudaStreamSynchronize(st));
+            bool all = true;
+            for (auto &l : hl) all &= (l.done != 0);
+            if (all) break;
+        }
+    }
+    // replicas stopped by breakdown (done == 2) still need their final estimate
+    ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, std::min(j + 1, kmax), tol, 1);
+    ::ps_launch_count++, k_lz_combine<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, lz, gbuf, w);
+    PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    PS_CK(cudaGetLastError());
+    if (res) {
+        res->iters_max = 0; res->nneg = 0;
+        for (auto &l : hl) { res->iters_max = std::max(res->iters_max, l.m); res->nneg += l.nneg; }
+    }
+    return PS_OK;
+}
+}  // namespace ps

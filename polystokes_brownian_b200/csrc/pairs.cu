@@ -1,0 +1,225 @@
+// pairs.cu -- explicit pair lists (CSR over beads, i < j, ascending j):
+//   which 0: Verlet pairs of check_dist.cpp:37-62 (stored pairs with dr < rverl[type];
+//            AA pairs only when mm_HI), found through the monomer cell list;
+//   which 1: monomer WCA pairs of cell_list.cpp:98-172 (dr^2 < rcut[0]^2, dr != 0);
+//   which 2: lubricated pairs (equal-radius pairs with gap < lub_gap * a).
+// Compiled with --fmad=false: distances round exactly as in the reference.
+#include <cmath>
+#include <vector>
+#include "ps_internal.h"
+#include "ps_kernels.h"
+
+namespace ps {
+
+__device__ __forceinline__ int rep_find(const int *__restrict__ offs, int R, long k)
+{
+    int lo = 0, hi = R;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (offs[mid] <= k) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void mimg(const Seg &s, double &dx, double &dy, double &dz)
+{
+    if (!s.box_on) return;
+    dx -= s.L[0] * nearbyint(dx * (1.0 / s.L[0]));
+    dy -= s.L[1] * nearbyint(dy * (1.0 / s.L[1]));
+    dz -= s.L[2] * nearbyint(dz * (1.0 / s.L[2]));
+}
+
+__device__ __forceinline__ int ccoord(double v, double org, double size, int nc)
+{
+    int c = (int)floor((v - org) / size);
+    if (c < 0) c = 0;
+    if (c >= nc) c = nc - 1;
+    return c;
+}
+
+// does pair (b, j), b < j (global indices, same replica) belong to list `which`?
+__device__ __forceinline__ bool ref_adjacent(const double *__restrict__ gref, const double *__restrict__ x, long i, long j)
+{
+    for (int d = 0; d < 3; d++) {
+        int nc = (int)gref[6 + d];
+        int ci = ccoord(x[3 * i + d], gref[d], gref[3 + d], nc);
+        int cj = ccoord(x[3 * j + d], gref[d], gref[3 + d], nc);
+        int dc = ci - cj;
+        if (gref[9] != 0.0) {
+            dc = ((dc % nc) + nc) % nc;
+            if (dc > 1 && dc < nc - 1) return false;
+        } else if (dc > 1 || dc < -1) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool in_list(const Seg &s, const double *__restrict__ x, long b, long j, int which,
+                                        const double *__restrict__ gref)
+{
+    int i = (int)(b - s.bead_off), k = (int)(j - s.bead_off);
+    bool mi = i < s.Nm, mk = k < s.Nm;
+    double dx = x[3 * b] - x[3 * j], dy = x[3 * b + 1] - x[3 * j + 1], dz = x[3 * b + 2] - x[3 * j + 2];
+    mimg(s, dx, dy, dz);
+    double d2 = dx * dx + dy * dy + dz * dz;
+    if (which == 0) {
+        int type = (mi && mk) ? 0 : ((mi || mk) ? 1 : 2);
+        if (type == 0 && !s.mm_HI) return false;
+        double dr = sqrt(d2);
+        return dr < (double)s.rverl[type];
+    }
+    if (which == 1) {
+        if (!(mi && mk)) return false;
+        double rc = (double)s.rcut[0];
+        return d2 < rc * rc && d2 != 0.0 && ref_adjacent(gref, x, b, j);
+    }
+    // which == 2
+    if (mi != mk) return false;
+    double a = mi ? s.beta : 1.0;
+    double dr = sqrt(d2);
+    return dr - 2 * a < s.lub_gap * a;
+}
+
+template <class F>
+__device__ __forceinline__ void partners(const Seg &s, int r, long b, const double *__restrict__ x,
+                                         const double *__restrict__ geo, const long *__restrict__ cell_off,
+                                         const int *__restrict__ cstart, const int *__restrict__ csorted, int which, F f)
+{
+    int i = (int)(b - s.bead_off);
+    if (i < s.Nm && (which != 0 || s.mm_HI)) {
+        const double *g = geo + 20 * r;
+        int nc[3] = {(int)g[6], (int)g[7], (int)g[8]};
+        int periodic = (int)g[9];
+        int c[3];
+        for (int d = 0; d < 3; d++) c[d] = ccoord(x[3 * b + d], g[d], g[3 + d], nc[d]);
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dxx = -1; dxx <= 1; dxx++) {
+                    int q[3] = {c[0] + dxx, c[1] + dy, c[2] + dz};
+                    bool ok = true;
+                    for (int d = 0; d < 3; d++) {
+                        if (periodic) q[d] = (q[d] % nc[d] + nc[d]) % nc[d];
+                        else if (q[d] < 0 || q[d] >= nc[d]) ok = false;
+                    }
+                    if (!ok) continue;
+                    // a periodic axis with fewer than 3 cells would visit a cell twice
+                    long cc = cell_off[r] + q[0] + (long)nc[0] * (q[1] + (long)nc[1] * q[2]);
+                    for (int k = cstart[cc]; k < cstart[cc + 1]; k++) {
+                        long j = csorted[k];
+                        if (j > b && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
+                    }
+                }
+    }
+    if (which != 1) {
+        // colloid partners (all colloids follow all monomers)
+        int c0 = i < s.Nm ? 0 : i - s.Nm + 1;
+        for (int c = c0; c < s.Nc; c++) {
+            long j = (long)s.bead_off + s.Nm + c;
+            if (j > b && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
+        }
+    }
+}
+
+__global__ void k_pairs_count(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
+                              const double *__restrict__ x, const double *__restrict__ geo,
+                              const long *__restrict__ cell_off, const int *__restrict__ cstart,
+                              const int *__restrict__ csorted, int which, int *__restrict__ cnt)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    int r = rep_find(bead_offs, R, b);
+    int n = 0;
+    partners(segs[r], r, b, x, geo, cell_off, cstart, csorted, which, [&](long) { n++; });
+    cnt[b] = n;
+}
+
+__global__ void k_pairs_fill(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
+                             const double *__restrict__ x, const double *__restrict__ geo,
+                             const long *__restrict__ cell_off, const int *__restrict__ cstart,
+                             const int *__restrict__ csorted, int which, const int *__restrict__ ptr,
+                             int *__restrict__ nbr)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    int r = rep_find(bead_offs, R, b);
+    int a = ptr[b], n = 0;
+    partners(segs[r], r, b, x, geo, cell_off, cstart, csorted, which, [&](long j) { nbr[a + n++] = (int)j; });
+    // ascending partner order
+    for (int u = a + 1; u < a + n; u++) {
+        int v = nbr[u], w = u - 1;
+        while (w >= a && nbr[w] > v) { nbr[w + 1] = nbr[w]; w--; }
+        nbr[w + 1] = v;
+    }
+}
+
+__global__ void k_scan_int(long n, const int *__restrict__ in, int *__restrict__ out)
+{
+    __shared__ int carry;
+    __shared__ int tmp[1024];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long base = 0; base < n; base += 1024) {
+        long k = base + threadIdx.x;
+        int v = k < n ? in[k] : 0;
+        tmp[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            int t = threadIdx.x >= o ? tmp[threadIdx.x - o] : 0;
+            __syncthreads();
+            tmp[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (k < n) out[k] = carry + tmp[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += tmp[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void k_pairs_expand(long ntot, const int *__restrict__ ptr, const int *__restrict__ nbr,
+                               int32_t *__restrict__ pi, int32_t *__restrict__ pj, long maxp)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    for (int k = ptr[b]; k < ptr[b + 1]; k++)
+        if (k < maxp) { pi[k] = (int32_t)b; pj[k] = nbr[k]; }
+}
+
+// Builds the CSR list into E.d_nbr_ptr / E.d_nbr (grown on demand).
+int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
+{
+    int thr = 128;
+    unsigned nbk = (unsigned)((E.ntot + thr - 1) / thr);
+    ::ps_launch_count++, k_pairs_count<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
+                                       E.d_cell_start, E.d_cell_sorted, which, E.d_nbr_count);
+    ::ps_launch_count++, k_scan_int<<<1, 1024, 0, st>>>(E.ntot, E.d_nbr_count, E.d_nbr_ptr);
+    int tot = 0;
+    PS_CK(cudaMemcpyAsync(&tot, E.d_nbr_ptr + E.ntot, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    if (tot > E.nbr_cap) {
+        cudaFree(E.d_nbr);
+        E.nbr_cap = (long)tot * 3 / 2 + 1024;
+        PS_CK(cudaMalloc(&E.d_nbr, sizeof(int) * E.nbr_cap));
+    }
+    ::ps_launch_count++, k_pairs_fill<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
+                                      E.d_cell_start, E.d_cell_sorted, which, E.d_nbr_ptr, E.d_nbr);
+    PS_CK(cudaGetLastError());
+    *npairs = tot;
+    return PS_OK;
+}
+
+int pair_list(Engine &E, int which, int32_t *pi, int32_t *pj, int64_t maxp, int64_t *count, cudaStream_t st)
+{
+    long np = 0;
+    int rc = build_list(E, which, &np, st);
+    if (rc) return rc;
+    if (pi && pj && maxp > 0) {
+        int thr = 128;
+        ::ps_launch_count++, k_pairs_expand<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_nbr_ptr, E.d_nbr, pi, pj, maxp);
+        PS_CK(cudaGetLastError());
+    }
+    if (count) *count = np;
+    return PS_OK;
+}
+
+}  // namespace ps

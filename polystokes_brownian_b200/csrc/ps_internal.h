@@ -1,0 +1,226 @@
+// ps_internal.h -- device-side data model and pair-tensor contractions of the
+// B200 PolyStokes engine.  Internal header (not part of the C-ABI).
+//
+// Pair formulas restate src/mob.cpp of sgnagella/polystokes_brownian:
+//   monomer-monomer (AA) translation block     mob.cpp:122-147
+//   monomer-colloid (AB) rotation/stresslet     mob.cpp:362-537
+//   colloid-colloid (BB) full FTS blocks        mob.cpp:96-358
+//   self blocks                                 mob.cpp:65-86, 539-633
+// and the block placement of the dense saddle matrix, mob.cpp:843-1144.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/polystokes_b200.h"
+
+#define PS_MAX_NC11_SCHUR 64   // dense Schur path limit (slip_vel.cpp:97)
+
+// number of kernels this library has launched (host-side counter)
+extern unsigned long long ps_launch_count;
+
+// Per-replica segment descriptor (device resident, one per replica).
+struct Seg {
+    int Nm, Nc, Np;
+    int bead_off;      // first bead of this replica in the global bead arrays
+    int coll_off;      // first colloid of this replica in global colloid arrays
+    int vec_off;       // saddle-vector offset
+    int top_off;       // offset in the concatenated mobility (nm3nc11) space
+    int vel_off;       // offset in the concatenated velocity (nm3nc6) space
+    int n, nm3, nc3, nc5, nc6, nc11, nm3nc3, nm3nc6, nm3nc11;
+    int mm_HI, chain_HI, ab_mode, box_on, fene, mono_ev, lub_on, tether;
+    int shell_schur;   // shell path with the dense Schur floor (nc11 <= lanczos_nc)
+    int schur_off;     // offset into the per-replica nc11^2 buffers
+    int ba_off;        // offset (in 11-vectors) of this replica's BA partials
+    int n_mtiles;      // monomer row tiles of this replica
+    int bond_off, nbonds;
+    int mt_first;      // index of this replica's first monomer tile (for BA partials)
+    double beta, beta_inv, kT, dt, epsilon, kbond, r0, Lmax;
+    double L[3];
+    double hs_k;       // HS spring constant kpref/dt (or kpref/(dt beta))
+    float sig[3], rverl[3], rcut[3];
+    double lub_gap;
+};
+
+// Row tile of the far-field pair kernels.
+struct Tile { int rep; int row0; int nrow; int mtile; };
+
+template <class T> struct V4;
+template <> struct V4<double> { typedef double4 t; };
+template <> struct V4<float> { typedef float4 t; };
+
+template <class T> __device__ __forceinline__ T rsqrt_t(T v);
+template <> __device__ __forceinline__ double rsqrt_t<double>(double v) { return rsqrt(v); }
+template <> __device__ __forceinline__ float rsqrt_t<float>(float v) { return rsqrtf(v); }
+
+// ---------------------------------------------------------------------------
+// AA: reference-specific monomer-monomer scalars (mob.cpp:122-131).
+// mob_a = x ee + y (I - ee)   =>   mob_a u = y u + (x - y)(e.u) e
+template <class T>
+__device__ __forceinline__ void aa_scalars(T r, T rinv, T two_beta, T &x, T &y)
+{
+    if (r > two_beta) {
+        T ri3 = rinv * rinv * rinv;
+        x = T(0.375) * rinv - T(2.0) * ri3;
+        y = T(0.75) * rinv - T(0.5) * ri3;
+    } else {
+        x = T(0.375) * r - T(1.0);
+        y = T(1.0) - T(0.28125) * r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Flattening of a symmetric-index rank-3 tensor g[k][i][j] to the 3x5 form of
+// mob.cpp:221-227: [g00-g22, 2 g01, 2 g02, 2 g12, g11-g22].
+// gt[k][i][j] = -xg (e_i e_j - d_ij/3) e_k + yg (e_i d_jk + e_j d_ik - 2 e_i e_j e_k)
+template <class T>
+__device__ __forceinline__ void gt_flat(const T e[3], T xg, T yg, T G[15])
+{
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        T ek = e[k];
+        // g[k][i][j] for the six (i,j) pairs that the flattening uses
+        auto g = [&](int i, int j) -> T {
+            T dij = (i == j) ? T(1) : T(0);
+            T djk = (j == k) ? T(1) : T(0);
+            T dik = (i == k) ? T(1) : T(0);
+            return -xg * (e[i] * e[j] - dij * T(1.0 / 3.0)) * ek
+                   + yg * (e[i] * djk + e[j] * dik - T(2) * e[i] * e[j] * ek);
+        };
+        T g22 = g(2, 2);
+        G[k * 5 + 0] = g(0, 0) - g22;
+        G[k * 5 + 1] = T(2) * g(0, 1);
+        G[k * 5 + 2] = T(2) * g(0, 2);
+        G[k * 5 + 3] = T(2) * g(1, 2);
+        G[k * 5 + 4] = g(1, 1) - g22;
+    }
+}
+
+// ht[k][i][j] = yh (e_i w_jk + e_j w_ik), w_ab = eps_abl e_l (mob.cpp:258-276)
+template <class T>
+__device__ __forceinline__ void ht_flat(const T e[3], T yh, T H[15])
+{
+    // w = eps . e (antisymmetric)
+    T w[3][3];
+    w[0][0] = 0; w[1][1] = 0; w[2][2] = 0;
+    w[0][1] = e[2]; w[1][0] = -e[2];
+    w[0][2] = -e[1]; w[2][0] = e[1];
+    w[1][2] = e[0]; w[2][1] = -e[0];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        auto h = [&](int i, int j) -> T { return yh * (e[i] * w[j][k] + e[j] * w[i][k]); };
+        T h22 = h(2, 2);
+        H[k * 5 + 0] = h(0, 0) - h22;
+        H[k * 5 + 1] = T(2) * h(0, 1);
+        H[k * 5 + 2] = T(2) * h(0, 2);
+        H[k * 5 + 3] = T(2) * h(1, 2);
+        H[k * 5 + 4] = h(1, 1) - h22;
+    }
+}
+
+// stress-strain rank-4 tensor entry (mob.cpp:279-298)
+template <class T>
+__device__ __forceinline__ T m4(const T e[3], int i, int j, int k, int l, T xm, T ym, T zm)
+{
+    auto d = [](int a, int b) -> T { return a == b ? T(1) : T(0); };
+    T eij = e[i] * e[j], ekl = e[k] * e[l], eik = e[i] * e[k], ejk = e[j] * e[k];
+    T eil = e[i] * e[l], ejl = e[j] * e[l];
+    return T(1.5) * xm * (eij - T(1.0 / 3.0) * d(i, j)) * (ekl - T(1.0 / 3.0) * d(k, l))
+           + T(0.5) * ym * (eik * d(j, l) + ejk * d(i, l) + eil * d(j, k) + ejl * d(i, k) - T(4) * eij * ekl)
+           + T(0.5) * zm * (d(i, k) * d(j, l) + d(j, k) * d(i, l) - d(i, j) * d(k, l) + eij * d(k, l)
+                            + ekl * d(i, j) - eik * d(j, l) - ejk * d(i, l) - eil * d(j, k) - ejl * d(i, k)
+                            + eij * ekl);
+}
+
+// 5x5 flattening through mesid (init.cpp:340-354, mob.cpp:321-355)
+template <class T>
+__device__ __forceinline__ void mm_flat(const T e[3], T xm, T ym, T zm, T Mm[25])
+{
+    const int mes0[5] = {0, 0, 0, 1, 1}, mes1[5] = {2, 1, 2, 2, 2};
+#pragma unroll
+    for (int ii = 0; ii < 5; ii++) {
+        int a = mes0[ii], b = mes1[ii];
+        if (ii == 0 || ii == 4) {
+            Mm[ii * 5 + 0] = m4(e, a, a, 0, 0, xm, ym, zm) - m4(e, a, a, 2, 2, xm, ym, zm)
+                             - (m4(e, b, b, 0, 0, xm, ym, zm) - m4(e, b, b, 2, 2, xm, ym, zm));
+            Mm[ii * 5 + 1] = T(2) * (m4(e, a, a, 0, 1, xm, ym, zm) - m4(e, b, b, 0, 1, xm, ym, zm));
+            Mm[ii * 5 + 2] = T(2) * (m4(e, a, a, 0, 2, xm, ym, zm) - m4(e, b, b, 0, 2, xm, ym, zm));
+            Mm[ii * 5 + 3] = T(2) * (m4(e, a, a, 1, 2, xm, ym, zm) - m4(e, b, b, 1, 2, xm, ym, zm));
+            Mm[ii * 5 + 4] = m4(e, a, a, 1, 1, xm, ym, zm) - m4(e, a, a, 2, 2, xm, ym, zm)
+                             - (m4(e, b, b, 1, 1, xm, ym, zm) - m4(e, b, b, 2, 2, xm, ym, zm));
+        } else {
+            Mm[ii * 5 + 0] = T(2) * (m4(e, a, b, 0, 0, xm, ym, zm) - m4(e, a, b, 2, 2, xm, ym, zm));
+            Mm[ii * 5 + 1] = T(4) * m4(e, a, b, 0, 1, xm, ym, zm);
+            Mm[ii * 5 + 2] = T(4) * m4(e, a, b, 0, 2, xm, ym, zm);
+            Mm[ii * 5 + 3] = T(4) * m4(e, a, b, 1, 2, xm, ym, zm);
+            Mm[ii * 5 + 4] = T(2) * (m4(e, a, b, 1, 1, xm, ym, zm) - m4(e, a, b, 2, 2, xm, ym, zm));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BB: contribution to colloid `row` from colloid `col`, e = (x_lo - x_hi)/r of
+// the canonically ordered pair (lo = lower colloid index); `is_lo` = row is lo.
+//   lo row: U += A F - B T + G S ; W += B F + C T + H S ; E += -G^T F + H^T T + Mm S
+//   hi row: U += A F - B T - G S ; W += B F + C T + H S ; E +=  G^T F + H^T T + Mm^T S
+// (derived from the dense block placement, mob.cpp:1042-1143)
+template <class T>
+__device__ __forceinline__ void bb_apply(const T e[3], T r, T rinv, bool is_lo, const T in[11], T out[11])
+{
+    (void)r;
+    T ri2 = rinv * rinv, ri3 = ri2 * rinv, ri4 = ri3 * rinv, ri5 = ri4 * rinv;
+    T xa = T(1.5) * rinv - ri3, ya = T(0.75) * rinv + T(0.5) * ri3;
+    T yb = T(-0.75) * ri2;
+    T xg = T(2.25) * ri2 - T(3.6) * ri4, yg = T(1.2) * ri4;
+    T xc = T(0.75) * ri3, yc = T(-0.375) * ri3;
+    T yh = T(-1.125) * ri3;
+    T xm = T(-4.5) * ri3 + T(10.8) * ri5, ym = T(2.25) * ri3 - T(7.2) * ri5, zm = T(1.8) * ri5;
+    const T *F = in, *Tq = in + 3, *S = in + 6;
+    T eF = e[0] * F[0] + e[1] * F[1] + e[2] * F[2];
+    T eT = e[0] * Tq[0] + e[1] * Tq[1] + e[2] * Tq[2];
+    // A F
+    T AF[3], CT[3], BF[3], BT[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        AF[a] = ya * F[a] + (xa - ya) * eF * e[a];
+        // reference C: diag x ee + y(1-ee), off-diagonal (x + y) ee (mob.cpp:249-254)
+        CT[a] = (xc + yc) * eT * e[a] + yc * Tq[a] - T(2) * yc * e[a] * e[a] * Tq[a];
+    }
+    // B v = yb (v x e)
+    BF[0] = yb * (F[1] * e[2] - F[2] * e[1]);
+    BF[1] = yb * (F[2] * e[0] - F[0] * e[2]);
+    BF[2] = yb * (F[0] * e[1] - F[1] * e[0]);
+    BT[0] = yb * (Tq[1] * e[2] - Tq[2] * e[1]);
+    BT[1] = yb * (Tq[2] * e[0] - Tq[0] * e[2]);
+    BT[2] = yb * (Tq[0] * e[1] - Tq[1] * e[0]);
+    T G[15], H[15], Mm[25];
+    gt_flat(e, xg, yg, G);
+    ht_flat(e, yh, H);
+    mm_flat(e, xm, ym, zm, Mm);
+    T sg = is_lo ? T(1) : T(-1);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        T gs = 0, hs = 0;
+#pragma unroll
+        for (int q = 0; q < 5; q++) { gs += G[a * 5 + q] * S[q]; hs += H[a * 5 + q] * S[q]; }
+        out[a] += AF[a] - BT[a] + sg * gs;
+        out[3 + a] += BF[a] + CT[a] + hs;
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        T gf = 0, ht = 0, ms = 0;
+#pragma unroll
+        for (int a = 0; a < 3; a++) { gf += G[a * 5 + q] * F[a]; ht += H[a * 5 + q] * Tq[a]; }
+#pragma unroll
+        for (int p = 0; p < 5; p++) ms += (is_lo ? Mm[q * 5 + p] : Mm[p * 5 + q]) * S[p];
+        out[6 + q] += -sg * gf + ht + ms;
+    }
+}
+
+// AB scalars (mob.cpp:410-412, 465-466)
+template <class T>
+__device__ __forceinline__ void ab_scalars(T rinv, T beta2, T &yb, T &xg, T &yg)
+{
+    T ri2 = rinv * rinv, ri4 = ri2 * ri2;
+    yb = T(-0.75) * ri2;
+    xg = T(2.25) * ri2 - T(0.45) * ri4 * (T(3) + T(5) * beta2);
+    yg = T(0.9) * ri4 * (T(0.5) + T(5.0 / 6.0) * beta2);
+}

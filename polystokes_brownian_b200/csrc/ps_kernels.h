@@ -1,0 +1,147 @@
+// ps_kernels.h -- host-side engine state shared by the .cu translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "ps_internal.h"
+
+namespace ps {
+
+// Per-replica MINRES scalars (device resident).  Paige & Saunders recurrences
+// in the preconditioned form used by PETSc KSPMINRES.
+struct MinresScal {
+    double beta, oldb, dbar, epsln, phibar, cs, sn, np, ttol, alfa;
+    double up_oldeps, up_delta, up_ginv, up_phi;   // pending w/x update
+    double sinv;                                     // 1 / beta for the next matvec
+    int it, done, reason, pending;
+};
+
+// Reduction block table entry: a contiguous range of one replica's segment.
+struct RBlk { int rep; int start; int len; };
+
+struct RedTable {
+    int nblk = 0;
+    RBlk *d_blk = nullptr;       // per block
+    int *d_first = nullptr;      // per replica: first block
+    int *d_count = nullptr;      // per replica: number of blocks
+    int *d_counter = nullptr;    // per replica: arrival counter (reset by last block)
+    double *d_part = nullptr;    // nblk x 4 partial sums
+};
+
+struct Engine {
+    int R = 0;
+    int precision = PS_PREC_FP64;
+    std::vector<ps_desc> desc;
+    std::vector<Seg> segs;
+    long ntot = 0, ncoll = 0, nvec = 0, ntop = 0, nvel = 0;
+    int maxNp = 0;
+    bool any_lub = false, any_shell_schur = false, any_kT = false, any_mmhi = false;
+
+    Seg *d_segs = nullptr;
+    int *d_vec_offs = nullptr, *d_top_offs = nullptr, *d_vel_offs = nullptr, *d_bead_offs = nullptr;
+
+    // state
+    double *d_x = nullptr, *d_q = nullptr, *d_xpos0 = nullptr, *d_xn = nullptr;
+    double4 *d_pos64 = nullptr;
+    float4 *d_pos32 = nullptr;
+    double *d_chain = nullptr;      // chain id per bead (monomers), -1-c for colloid c
+    int *d_coll_rep = nullptr;      // replica of each colloid
+    double *d_time = nullptr;       // per replica time
+    double *d_ktrap = nullptr;      // per replica (weaken_trap mutates it)
+    double *d_trapinfo = nullptr;   // per replica: tstop, weaken_trap, unused
+
+    // far-field pair work lists
+    Tile *d_aa_tiles = nullptr, *d_ab_tiles = nullptr, *d_bb_tiles = nullptr;
+    int n_aa_tiles = 0, n_ab_tiles = 0, n_bb_tiles = 0, nch_aa = 1, nch_bb = 1;
+    long part_stride = 0;
+    double *d_partAA = nullptr, *d_partAB = nullptr, *d_partBB = nullptr, *d_partBA = nullptr;
+    long nba = 0;
+
+    // reference-mode AB translational block and its carried state
+    double *d_tab = nullptr, *d_stale = nullptr;
+    int *d_aa_last = nullptr;       // per replica: (i,j) of the last AA pair, -1 if none
+
+    // arrowhead Schur floor (shell path)
+    long nschur = 0;
+    double *d_delta = nullptr, *d_schurQ = nullptr, *d_schurL = nullptr;
+    int *d_schur_reps = nullptr; int n_schur_reps = 0;
+
+    // bonds (per-bead CSR: partner, sign)
+    int *d_bond_ptr = nullptr, *d_bond_nbr = nullptr;
+    double *d_bond_sgn = nullptr;
+
+    // cell list / pair lists
+    int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_sorted = nullptr, *d_cell_count = nullptr;
+    long ncell_cap = 0;
+    double *d_cellgeo = nullptr;     // per replica: org[3], size[3], nc[3] (as double), periodic
+    long *d_cell_offs = nullptr;     // per replica: first cell
+    long ncells = 0;
+    bool need_cells = false;
+    int *d_nbr_ptr = nullptr, *d_nbr = nullptr;   // CSR neighbour lists (i<j pairs per i)
+    long nbr_cap = 0;
+    int *d_nbr_count = nullptr;
+
+    // lubrication
+    double *d_lubtab = nullptr; int lub_nrow = 0;
+    double *d_luby = nullptr, *d_lub_diag = nullptr;
+    int *d_lub_ptr = nullptr, *d_lub_nbr = nullptr; long lub_cap = 0; long lub_npairs = 0;
+
+    // Krylov workspace
+    RedTable red;                    // over saddle vectors
+    RedTable red_top;                // over mobility vectors
+    double *d_D = nullptr, *d_z = nullptr, *d_v = nullptr, *d_xw = nullptr;
+    double *d_Rr[3] = {nullptr, nullptr, nullptr}, *d_W[3] = {nullptr, nullptr, nullptr};
+    MinresScal *d_mr = nullptr;
+    double *d_sinv = nullptr;
+    int *d_nactive = nullptr;
+    int *h_nactive = nullptr;        // pinned
+
+    // step workspace
+    double *d_rhs = nullptr, *d_X = nullptr, *d_Xd = nullptr, *d_Xdet = nullptr, *d_Wn = nullptr;
+    double *d_vdn = nullptr, *d_vdc = nullptr, *d_vb = nullptr, *d_up = nullptr, *d_ud = nullptr;
+    double *d_drift = nullptr, *d_sb = nullptr, *d_fext = nullptr, *d_fb = nullptr, *d_wr = nullptr;
+    double *d_tmp_top = nullptr, *d_tmp_top2 = nullptr;
+    uint64_t seed = 12345, step_counter = 0;
+
+    // Lanczos workspace
+    int lz_kmax = 0;
+    double *d_lzV = nullptr, *d_lzT = nullptr, *d_lzw = nullptr, *d_lzq = nullptr;
+    double *d_lzs = nullptr;
+
+    cudaStream_t internal = nullptr;
+};
+
+// rpy.cu
+void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st);
+int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cudaStream_t st);
+int fma_peak(int fp64, double *tflops, cudaStream_t st);
+// stage.cu
+void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st);
+int stage_pack(Engine &E, cudaStream_t st);
+int stage_pairs(Engine &E, cudaStream_t st);
+int stage_rhs(Engine &E, int drift, const double *fext, double *rhs, cudaStream_t st);
+int stage_assemble(Engine &E, cudaStream_t st);
+int stage_schur(Engine &E, cudaStream_t st);
+int diag_saddle(Engine &E, double *d, cudaStream_t st);
+int pair_list(Engine &E, int which, int32_t *pi, int32_t *pj, int64_t maxp, int64_t *count, cudaStream_t st);
+int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
+int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStream_t st);
+// krylov.cu
+int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res, cudaStream_t st);
+int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
+int build_red_table(Engine &E, RedTable &T, bool top);
+void free_red_table(RedTable &T);
+void seg_dot(Engine &E, RedTable &T, const double *a, const double *b, double *out_per_rep, cudaStream_t st);
+
+void set_error(const std::string &s);
+#define PS_CK(call)                                                                    \
+    do {                                                                               \
+        cudaError_t _e = (call);                                                       \
+        if (_e != cudaSuccess) {                                                       \
+            ps::set_error(std::string(#call) + ": " + cudaGetErrorString(_e));         \
+            return PS_ERR_CUDA;                                                        \
+        }                                                                              \
+    } while (0)
+
+}  // namespace ps

@@ -1,0 +1,155 @@
+"""Parity of the CUDA path (through the C-ABI) against the CPU oracle.
+
+Tolerances: FP64 operator applies <= 1e-12 relative; solves at rtol 1e-13 in both
+<= 1e-10 relative; pair sets bit-exact; one full step with injected noise
+<= 1e-10 relative to the step displacement.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import psoracle as po
+from polystokes_brownian_b200 import configs
+from polystokes_brownian_b200.engine import Batch
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_for(sysm):
+    return po.OracleSim(po.default_params(**sysm.params), sysm.x.ravel())
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+CASES = {
+    "shell_C1": lambda: configs.polymer_probe(seed=0),
+    "mmhi_mixed": lambda: configs.small_mixed(seed=1, mm_HI=1),
+    "mmhi_chain": lambda: configs.small_mixed(seed=2, mm_HI=1, chain_HI=1),
+    "mmhi_rpy": lambda: configs.small_mixed(seed=3, mm_HI=1, ab_mode=1),
+    "shell_rpy": lambda: configs.small_mixed(seed=4, mm_HI=0, ab_mode=1),
+    "colloids": lambda: configs.suspension(n=96, phi=0.1, seed=0),
+    "brush_small": lambda: configs.brush(nchain=8, nper=8, seed=0),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_operator_parity(case):
+    sysm = CASES[case]()
+    o = oracle_for(sysm)
+    rhs_o = o.stage()
+    b = Batch([sysm])
+    rhs_g = b.stage()
+    assert rel(rhs_g.cpu().numpy(), rhs_o) < 1e-13
+    x = np.random.default_rng(7).normal(size=o.n)
+    yo = o.saddle_apply(x)
+    yg = b.matmult(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert rel(yg, yo) < 1e-12, rel(yg, yo)
+    u = x[: o.nm3nc11].copy()
+    assert rel(b.mobility_apply(torch.from_numpy(u).cuda()).cpu().numpy(), o.mobility_apply(u)) < 1e-12
+    assert rel(b.diagonal().cpu().numpy(), o.saddle_diag()) < 1e-13
+    b.close()
+
+
+@pytest.mark.parametrize("case", ["shell_C1", "mmhi_mixed", "colloids", "brush_small"])
+def test_minres_parity(case):
+    sysm = CASES[case]()
+    o = oracle_for(sysm)
+    rhs = o.stage()
+    rhs[: o.nm3nc11] += np.random.default_rng(3).normal(size=o.nm3nc11)
+    xo, reason_o, it_o, _ = o.minres(rhs, rtol=1e-13)
+    b = Batch([sysm])
+    b.stage()
+    xg, r = b.solve(torch.from_numpy(rhs).cuda(), rtol=1e-13)
+    assert r.reason > 0
+    assert rel(xg.cpu().numpy(), xo) < 1e-10, rel(xg.cpu().numpy(), xo)
+    assert abs(r.iters_max - it_o) <= max(2, it_o // 10)
+    # warm start from the solution converges immediately
+    xw, r2 = b.solve(torch.from_numpy(rhs).cuda(), x0=xg, rtol=1e-8)
+    assert r2.iters_max <= 2
+    b.close()
+
+
+@pytest.mark.parametrize("case", ["shell_C1", "mmhi_mixed", "brush_small"])
+def test_pair_lists_bitexact(case):
+    sysm = CASES[case]()
+    o = po.OracleSim(po.default_params(**dict(sysm.params, mono_ev=1)), sysm.x.ravel())
+    o.stage()
+    b = Batch([configs.System(sysm.name, dict(sysm.params, mono_ev=1), sysm.x)])
+    b.stage()
+    vi, vj = o.verlet_pairs()
+    gi, gj = b.pair_list(0)
+    assert sorted(zip(vi.tolist(), vj.tolist())) == list(zip(gi.cpu().tolist(), gj.cpu().tolist()))
+    if not sysm.params["mm_HI"]:
+        ci, cj = o.cell_pairs()
+        want = sorted((min(a, c), max(a, c)) for a, c in zip(ci.tolist(), cj.tolist()))
+        wi, wj = b.pair_list(1)
+        assert want == list(zip(wi.cpu().tolist(), wj.cpu().tolist()))
+    b.close()
+
+
+def test_sqrt_parity_dense_and_shell():
+    # dense (mm_HI) path: Lanczos vs exact eigen square root on an SPD configuration
+    sysm = configs.small_mixed(seed=5, mm_HI=1, spread=9.0)
+    o = oracle_for(sysm)
+    o.stage()
+    M = o.dense_mobility()
+    assert np.linalg.eigvalsh(M).min() > 0
+    z = np.random.default_rng(2).normal(size=M.shape[0])
+    b = Batch([sysm])
+    b.stage()
+    w, r = b.sqrtm(torch.from_numpy(z).cuda(), kmax=60, tol=1e-13)
+    assert rel(w.cpu().numpy(), po.sqrtm_eig(M, z)) < 1e-10
+    b.close()
+    # shell path: block-Cholesky with the Schur floor
+    sysm = configs.polymer_probe(seed=0)
+    o = oracle_for(sysm)
+    o.stage()
+    z = np.random.default_rng(4).normal(size=o.nm3nc11)
+    b = Batch([sysm])
+    b.stage()
+    w, _ = b.sqrtm(torch.from_numpy(z).cuda())
+    assert rel(w.cpu().numpy(), o.slip_noise(z)) < 1e-12
+    b.close()
+
+
+@pytest.mark.parametrize("case", ["shell_C1", "mmhi_mixed", "brush_small"])
+def test_step_parity(case):
+    sysm = CASES[case]()
+    o = oracle_for(sysm)
+    rng = np.random.default_rng(11)
+    fb = rng.normal(size=o.nm3nc11)
+    wr = rng.normal(size=o.nm3nc6)
+    x0 = sysm.x.ravel().copy()
+    oo = o.step(fb=fb, wrfd=wr, rtol=1e-13)
+    xo, qo = o.state()
+    b = Batch([sysm])
+    b.step(fb=torch.from_numpy(fb).cuda(), wrfd=torch.from_numpy(wr).cuda(), rtol=1e-13)
+    xg, qg = b.state()
+    xg = xg.cpu().numpy()
+    disp = np.linalg.norm(xo - x0)
+    assert np.linalg.norm(xg - xo) <= 1e-10 * max(disp, 1e-30), (np.linalg.norm(xg - xo), disp)
+    if sysm.params["Nc"]:
+        assert np.abs(qg.cpu().numpy() - qo).max() < 1e-12
+    outs = b.step_outputs()
+    assert rel(outs["udiff"].cpu().numpy(), oo["udiff"]) < 1e-8
+    b.close()
+
+
+def test_batch_matches_single():
+    systems = [CASES["mmhi_mixed"](), CASES["colloids"](), CASES["shell_C1"]()]
+    xs = [np.random.default_rng(i).normal(size=6 * s.params["Nm"] + 17 * s.params["Nc"]) for i, s in enumerate(systems)]
+    b = Batch(systems)
+    b.stage()
+    yb = b.matmult(torch.from_numpy(np.concatenate(xs)).cuda()).cpu().numpy()
+    for i, s in enumerate(systems):
+        one = Batch([s])
+        one.stage()
+        y1 = one.matmult(torch.from_numpy(xs[i]).cuda()).cpu().numpy()
+        o = b.off[i]["vec"]
+        assert rel(yb[o:o + len(xs[i])], y1) < 1e-13
+        one.close()
+    b.close()
