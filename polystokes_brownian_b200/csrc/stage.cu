@@ -674,6 +674,7 @@ int stage_schur(Engine &E, cudaStream_t st)
 {
     if (!E.n_schur_reps) return PS_OK;
     size_t smem = sizeof(double) * (2 * 64 * 64 + 64);
+    PS_CK(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ::ps_launch_count++, k_schur<<<E.n_schur_reps, 256, smem, st>>>(E.d_segs, E.d_schur_reps, E.d_x, E.d_delta, E.d_schurQ, E.d_schurL,
                                                 E.d_tab);
     PS_CK(cudaGetLastError());
