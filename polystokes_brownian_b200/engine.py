@@ -36,7 +36,7 @@ def make_desc(params: dict) -> _capi.PsDesc:
 class Batch:
     """A batch of independent systems advanced by the B200 engine."""
 
-    def __init__(self, systems: list[System], precision: int = _capi.PS_PREC_FP64, device: str = "cuda"):
+    def __init__(self, systems: list[System], precision: int = _capi.PS_PREC_FP64, device: str = "cuda:0"):
         self.systems = systems
         self.R = len(systems)
         self.device = torch.device(device)
