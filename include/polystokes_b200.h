@@ -103,6 +103,8 @@ typedef struct ps_step_inputs {
     const double *zlub; /* 6 or 12 per lubricated pair, canonical pair order */
     double rtol;        /* MINRES rtol for the five solves */
     int32_t maxit;
+    int32_t sqrt_kmax;  /* Lanczos subspace cap of the noise (0: 40) */
+    double sqrt_tol;    /* Lanczos relative tolerance of the noise (0: 1e-6) */
 } ps_step_inputs;
 
 typedef struct ps_step_result {

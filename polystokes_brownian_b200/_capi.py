@@ -56,7 +56,7 @@ class PsSqrtResult(C.Structure):
 
 class PsStepInputs(C.Structure):
     _fields_ = [("fb", C.c_void_p), ("wrfd", C.c_void_p), ("zlub", C.c_void_p),
-                ("rtol", C.c_double), ("maxit", C.c_int32)]
+                ("rtol", C.c_double), ("maxit", C.c_int32), ("sqrt_kmax", C.c_int32), ("sqrt_tol", C.c_double)]
 
 
 class PsStepResult(C.Structure):

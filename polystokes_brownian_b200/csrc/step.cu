@@ -283,7 +283,7 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
             ::ps_launch_count++, k_normals<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.seed, 2 * E.step_counter + 1, E.d_wr);
             wr = E.d_wr;
         }
-        ps_sqrt_opts so = {40, 1e-6};
+        ps_sqrt_opts so = {in && in->sqrt_kmax > 0 ? in->sqrt_kmax : 40, in && in->sqrt_tol > 0 ? in->sqrt_tol : 1e-6};
         if ((rc = slip_noise(E, fb, E.d_Wn, &so, nullptr, st))) return rc;
         ::ps_launch_count++, k_add_noise<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;

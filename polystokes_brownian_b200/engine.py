@@ -144,9 +144,9 @@ class Batch:
         return w, r
 
     def step(self, fb: torch.Tensor | None = None, wrfd: torch.Tensor | None = None, rtol: float = 1e-8,
-             maxit: int = 10000):
+             maxit: int = 10000, sqrt_kmax: int = 0, sqrt_tol: float = 0.0):
         inp = _capi.PsStepInputs(None if fb is None else fb.data_ptr(), None if wrfd is None else wrfd.data_ptr(),
-                                 None, rtol, maxit)
+                                 None, rtol, maxit, sqrt_kmax, sqrt_tol)
         res = _capi.PsStepResult()
         check(lib().ps_step(self.h, C.byref(inp), C.byref(res), self.stream), "ps_step")
         return res

@@ -118,9 +118,20 @@ def test_sqrt_parity_dense_and_shell():
     b.close()
 
 
-@pytest.mark.parametrize("case", ["shell_C1", "mmhi_mixed", "brush_small"])
+STEP_CASES = {
+    # shell path: block-Cholesky noise, Schur floor, two colloids
+    "shell_C1": lambda: configs.polymer_probe(seed=0),
+    # dense path with noise: 58 mobility DOFs, so the Lanczos square root is exact
+    "mmhi_noise": lambda: configs.small_mixed(seed=5, Nm_chain=(3, 4), Nc=2, mm_HI=1),
+    # dense path, deterministic (kT = 0), FENE chains around a colloid
+    "brush_kT0": lambda: configs.System("brush", dict(configs.brush(nchain=8, nper=8, seed=0).params, kT=0.0),
+                                        configs.brush(nchain=8, nper=8, seed=0).x),
+}
+
+
+@pytest.mark.parametrize("case", list(STEP_CASES))
 def test_step_parity(case):
-    sysm = CASES[case]()
+    sysm = STEP_CASES[case]()
     o = oracle_for(sysm)
     rng = np.random.default_rng(11)
     fb = rng.normal(size=o.nm3nc11)
@@ -129,7 +140,8 @@ def test_step_parity(case):
     oo = o.step(fb=fb, wrfd=wr, rtol=1e-13)
     xo, qo = o.state()
     b = Batch([sysm])
-    b.step(fb=torch.from_numpy(fb).cuda(), wrfd=torch.from_numpy(wr).cuda(), rtol=1e-13)
+    b.step(fb=torch.from_numpy(fb).cuda(), wrfd=torch.from_numpy(wr).cuda(), rtol=1e-13, sqrt_kmax=64,
+           sqrt_tol=1e-15)
     xg, qg = b.state()
     xg = xg.cpu().numpy()
     disp = np.linalg.norm(xo - x0)
@@ -137,7 +149,8 @@ def test_step_parity(case):
     if sysm.params["Nc"]:
         assert np.abs(qg.cpu().numpy() - qo).max() < 1e-12
     outs = b.step_outputs()
-    assert rel(outs["udiff"].cpu().numpy(), oo["udiff"]) < 1e-8
+    if sysm.params["kT"] > 0:
+        assert rel(outs["udiff"].cpu().numpy(), oo["udiff"]) < 1e-8
     b.close()
 
 
