@@ -206,6 +206,7 @@ def run_b200(args):
     lat = []
     t_total = 0.0
     iters = []
+    reasons = []
     for _ in range(args.steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -217,6 +218,7 @@ def run_b200(args):
         lat.append(ms)
         t_total += ms
         iters.append(list(r.iters))
+        reasons.append(r.reason)
     barrier()
     clocks = clk.stop()
     launches = int(L.ps_kernel_launches() - launches0)
@@ -233,9 +235,11 @@ def run_b200(args):
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
+    e2e_iters = []
     for _ in range(args.steps):
         _capi.check(L.ps_set_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_set_state")
-        b.step(rtol=args.rtol)
+        r = b.step(rtol=args.rtol)
+        e2e_iters.append(list(r.iters))
         _capi.check(L.ps_get_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_get_state")
     e1.record(st)
     e1.synchronize()
@@ -271,7 +275,7 @@ def run_b200(args):
                           "precision": args.precision, "l2": "flushed (256 MB write) before every timed step",
                           "parallelism": f"replicas x{world}"},
                "latency_ms": {"p50": lat_sorted[len(lat) // 2], "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
-               "minres_iters": iters[-1],
+               "minres_iters": iters, "minres_reason": reasons, "e2e_minres_iters": e2e_iters,
                "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * 3 * b.ntot,
                        "d2h_bytes_per_step": 8 * 3 * b.ntot},
                "gpu_launches": launches, "roofline": roof, "clocks": clocks}
