@@ -220,6 +220,8 @@ def run_b200(args):
         iters.append(list(r.iters))
         reasons.append(r.reason)
     barrier()
+    xs, _ = b.state()
+    finite = bool(torch.isfinite(xs).all().item())
     clocks = clk.stop()
     launches = int(L.ps_kernel_launches() - launches0)
     tmax = torch.tensor([t_total], dtype=torch.float64, device="cuda")
@@ -278,7 +280,7 @@ def run_b200(args):
                "minres_iters": iters, "minres_reason": reasons, "e2e_minres_iters": e2e_iters,
                "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * 3 * b.ntot,
                        "d2h_bytes_per_step": 8 * 3 * b.ntot},
-               "gpu_launches": launches, "roofline": roof, "clocks": clocks}
+               "gpu_launches": launches, "roofline": roof, "clocks": clocks, "state_finite": finite}
         if cb:
             out["cpu_baseline"] = cb
         print(json.dumps(out), flush=True)

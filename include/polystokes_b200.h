@@ -47,6 +47,11 @@ extern "C" {
 #define PS_AB_REFERENCE 0
 #define PS_AB_RPY 1
 
+/* Monomer-monomer translation scalars: the reference's own (mob.cpp:122-131)
+ * or the equal-sphere RPY of radius beta with its overlap form. */
+#define PS_AA_REFERENCE 0
+#define PS_AA_RPY 1
+
 /* precision of the far-field matvec and Krylov vectors */
 #define PS_PREC_FP64 0
 #define PS_PREC_MIXED 1
@@ -69,6 +74,7 @@ typedef struct ps_desc {
     int32_t lanczos_nc; /* POLYSTOKES_LANCZOS_NC, default 64 */
     int32_t lub_on;     /* near-field lubrication (not in the reference) */
     double lub_gap;     /* lubricated pairs: gap < lub_gap * radius */
+    int32_t aa_mode;    /* PS_AA_REFERENCE | PS_AA_RPY: monomer-monomer scalars */
 } ps_desc;
 
 typedef struct ps_ksp_opts {

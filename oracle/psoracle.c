@@ -201,11 +201,15 @@ static ld DEL(int i, int j) { return i == j ? 1.0L : 0.0L; }
 static int third(int a, int b) { int k = 3 - a - b; if (k == -1) k = 2; if (k == 3) k = 0; return k; }
 
 /* monomer-monomer translation block, mob.cpp:122-147 (reference-specific formula) */
-void or_tensor_aa(double r, double rinv, const double e[3], double beta, double a9[9])
+void or_tensor_aa(double r, double rinv, const double e[3], double beta, int mode, double a9[9])
 {
     double x, y;
     double ri3 = rinv * rinv * rinv;
-    if (r > 2.0 * beta) { x = (3. / 8.) * rinv - 2.0 * ri3; y = (3. / 4.) * rinv - (1. / 2.) * ri3; }
+    if (mode == OR_AA_RPY) {
+        double b2 = beta * beta;
+        if (r > 2.0 * beta) { x = 1.5 * rinv - b2 * ri3; y = 0.75 * rinv + 0.5 * b2 * ri3; }
+        else { x = (1.0 - 3.0 * r / (16.0 * beta)) / beta; y = (1.0 - 9.0 * r / (32.0 * beta)) / beta; }
+    } else if (r > 2.0 * beta) { x = (3. / 8.) * rinv - 2.0 * ri3; y = (3. / 4.) * rinv - (1. / 2.) * ri3; }
     else { x = (3. / 8.) * r - 1.0; y = 1.0 - (9. / 32.) * r; }
     for (int i = 0; i < 3; i++) {
         ld ee = (ld)(e[i] * e[i]);
@@ -609,7 +613,7 @@ void or_mob(or_sim *s)
                 if (!(s->p.chain_HI && s->chain[i] == s->chain[j])) { li = i; lj = j; have = 1; break; }
         if (have) {
             const double *pd = pdk(s, li, lj, NULL);
-            or_tensor_aa(pd[3], pd[4], pd, s->p.beta, s->stale);
+            or_tensor_aa(pd[3], pd[4], pd, s->p.beta, s->p.aa_mode, s->stale);
         }
         memcpy(s->tab, s->stale, sizeof(double) * 9);
     } else if (s->p.ab_mode == OR_AB_REFERENCE) {
@@ -806,7 +810,7 @@ void or_mobility_apply(const or_sim *s, const double *u, double *y)
         for (int j = i + 1; j < Nm; j++) {
             if (s->p.chain_HI && s->chain[i] == s->chain[j]) continue;
             const double *pd = pdk(s, i, j, NULL);
-            double A[9]; or_tensor_aa(pd[3], pd[4], pd, s->p.beta, A);
+            double A[9]; or_tensor_aa(pd[3], pd[4], pd, s->p.beta, s->p.aa_mode, A);
             for (int a = 0; a < 3; a++)
                 for (int b = 0; b < 3; b++) {
                     y[3 * i + a] += A[a * 3 + b] * u[3 * j + b];

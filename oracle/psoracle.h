@@ -31,6 +31,13 @@ extern "C" {
  *                    computes but never uses (mob.cpp:410-411).               */
 enum { OR_AB_REFERENCE = 0, OR_AB_RPY = 1 };
 
+/* Monomer-monomer translation scalars.  OR_AA_REFERENCE: mob.cpp:122-131
+ * (x = 3/(8r) - 2/r^3, y = 3/(4r) - 1/(2r^3); overlap x = 3r/8 - 1, y = 1 - 9r/32).
+ * OR_AA_RPY: equal-sphere Rotne-Prager-Yamakawa of radius beta in the units of
+ * the reference (6 pi eta = 1): x = 3/(2r) - b^2/r^3, y = 3/(4r) + b^2/(2r^3) for
+ * r > 2b; overlap x = (1 - 3r/(16b))/b, y = (1 - 9r/(32b))/b. */
+enum { OR_AA_REFERENCE = 0, OR_AA_RPY = 1 };
+
 typedef struct or_params {
     int    Nm, Nc, Npoly, Nmono_per_chain;
     double beta, kT, epsilon, kbond, r0, Lmax, tau;
@@ -49,6 +56,7 @@ typedef struct or_params {
     int    lub_on;
     double lub_gap;         /* pairs with gap < lub_gap * a get a resistance block */
     int    noise_lanczos;   /* mm_HI noise: 0 exact eigen square root, 1 Lanczos (kmax 40, tol 1e-6) */
+    int    aa_mode;         /* OR_AA_REFERENCE or OR_AA_RPY */
 } or_params;
 
 typedef struct or_sim or_sim;
@@ -64,7 +72,7 @@ int     or_sizes(const or_sim *s, int *out8);   /* nm3,nc11,nm3nc6,nm3nc11,n,Np,
 void    or_set_lub_tables(or_sim *s, const double *tab, int nrow, int ncol);
 
 /* pair tensors (mob.cpp:30-537), outputs as the double the reference stores */
-void or_tensor_aa(double r, double rinv, const double e[3], double beta, double a[9]);
+void or_tensor_aa(double r, double rinv, const double e[3], double beta, int mode, double a[9]);
 void or_tensor_ab(double r, double rinv, const double e[3], double beta,
                   double b[9], double gt[15]);
 void or_tensor_ab_rpy(double r, double rinv, const double e[3], double beta, double a[9]);

@@ -33,7 +33,7 @@ class OrParams(C.Structure):
         ("ktrap", C.c_double), ("tstart", C.c_double), ("trun", C.c_double), ("weaken_trap", C.c_double),
         ("t0", C.c_double), ("restart", C.c_int), ("ab_mode", C.c_int),
         ("hs_kpref", C.c_double), ("hs_kmode", C.c_int), ("lanczos_nc", C.c_int),
-        ("lub_on", C.c_int), ("lub_gap", C.c_double), ("noise_lanczos", C.c_int),
+        ("lub_on", C.c_int), ("lub_gap", C.c_double), ("noise_lanczos", C.c_int), ("aa_mode", C.c_int),
     ]
 
 
@@ -67,8 +67,8 @@ def lib():
         L.or_get_time.argtypes = [C.c_void_p]
         L.or_sizes.argtypes = [C.c_void_p, I]
         L.or_set_lub_tables.argtypes = [C.c_void_p, P, C.c_int, C.c_int]
-        for f in ("or_tensor_aa", "or_tensor_ab_rpy"):
-            getattr(L, f).argtypes = [C.c_double, C.c_double, P, C.c_double, P]
+        L.or_tensor_aa.argtypes = [C.c_double, C.c_double, P, C.c_double, C.c_int, P]
+        L.or_tensor_ab_rpy.argtypes = [C.c_double, C.c_double, P, C.c_double, P]
         L.or_tensor_ab.argtypes = [C.c_double, C.c_double, P, C.c_double, P, P]
         L.or_tensor_bb.argtypes = [C.c_double, C.c_double, P, P, P, P, P, P, P]
         for f in ("or_check_dist", "or_mob", "or_schur_sync"):
@@ -109,7 +109,7 @@ def default_params(**kw) -> OrParams:
              r0=1.0, Lmax=10.0, tau=1000.0, dt=1e-3, mm_HI=1, chain_HI=0, fene=0, tether=0,
              mono_ev=0, record_forces=1, box_on=0, ktrap=0.0, tstart=0.0, trun=0.0,
              weaken_trap=-1.0, t0=0.0, restart=0, ab_mode=AB_REFERENCE, hs_kpref=1.0,
-             hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5, noise_lanczos=0)
+             hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5, noise_lanczos=0, aa_mode=0)
     box = kw.pop("box", None)
     d.update({k: v for k, v in kw.items() if k in d})
     for k, v in d.items():
@@ -312,10 +312,10 @@ def tensor_ab(e, r, beta):
     return b, g
 
 
-def tensor_aa(e, r, beta):
+def tensor_aa(e, r, beta, mode=0):
     e = np.ascontiguousarray(e, dtype=np.float64)
     a = np.zeros(9)
-    lib().or_tensor_aa(r, 1.0 / r, _p(e), beta, _p(a))
+    lib().or_tensor_aa(r, 1.0 / r, _p(e), beta, mode, _p(a))
     return a
 
 

@@ -17,6 +17,8 @@ HEADER = os.path.join(HERE, "..", "include", "polystokes_b200.h")
 PS_OK = 0
 PS_AB_REFERENCE = 0
 PS_AB_RPY = 1
+PS_AA_REFERENCE = 0
+PS_AA_RPY = 1
 PS_PREC_FP64 = 0
 PS_PREC_MIXED = 1
 
@@ -33,7 +35,7 @@ class PsDesc(C.Structure):
         ("ktrap", C.c_double), ("tstart", C.c_double), ("trun", C.c_double), ("weaken_trap", C.c_double),
         ("t0", C.c_double), ("restart", C.c_int32), ("ab_mode", C.c_int32),
         ("hs_kpref", C.c_double), ("hs_kmode", C.c_int32), ("lanczos_nc", C.c_int32),
-        ("lub_on", C.c_int32), ("lub_gap", C.c_double),
+        ("lub_on", C.c_int32), ("lub_gap", C.c_double), ("aa_mode", C.c_int32),
     ]
 
 

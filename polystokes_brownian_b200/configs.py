@@ -36,7 +36,8 @@ class System:
 DEFAULTS = dict(Nm=0, Nc=0, Npoly=0, Nmono_per_chain=1, beta=1.0, kT=1.0, epsilon=1.0, kbond=1.0,
                 r0=1.0, Lmax=10.0, tau=1000.0, dt=1e-3, mm_HI=1, chain_HI=0, fene=0, tether=0,
                 mono_ev=0, record_forces=1, box_on=0, ktrap=0.0, tstart=0.0, trun=0.0, weaken_trap=-1.0,
-                t0=0.0, restart=0, ab_mode=0, hs_kpref=1.0, hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5)
+                t0=0.0, restart=0, ab_mode=0, hs_kpref=1.0, hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5,
+                aa_mode=0)
 
 
 def make_params(**kw) -> dict:
@@ -155,7 +156,7 @@ def suspension(n: int = 1024, phi: float = 0.2, seed: int = 0, gap: float = 0.01
     return System("suspension", params, np.array(pts))
 
 
-def brush(nchain: int = 128, nper: int = 32, seed: int = 0) -> System:
+def brush(nchain: int = 128, nper: int = 32, seed: int = 0, dt: float = 1e-4, pair_mode: int = 1) -> System:
     """1 colloid (a_c = 5) with nchain chains of nper beads grown outward from its surface.
 
     The chains are free (tether=0): the reference tethers with the chain's own
@@ -174,12 +175,19 @@ def brush(nchain: int = 128, nper: int = 32, seed: int = 0) -> System:
 
     xm = _chains(rng, nchain, nper, beta, step, None, start, grid)
     params = make_params(Nm=nchain * nper, Nc=1, Npoly=nchain, Nmono_per_chain=nper, beta=beta, kT=1.0,
-                         kbond=30 * ac * ac, r0=step, Lmax=3.0 / ac, fene=1, dt=1e-3, mm_HI=1, chain_HI=0)
+                         kbond=30 * ac * ac, r0=step, Lmax=3.0 / ac, fene=1, dt=dt, mm_HI=1, chain_HI=0,
+                         aa_mode=pair_mode, ab_mode=pair_mode)
     return System("brush", params, np.vstack([xm, np.zeros((1, 3))]))
 
 
-def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0) -> System:
-    """One batched-ensemble replica: harmonic chains + 0..2 trapped probes."""
+def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0, dt: float = 1e-4, pair_mode: int = 1) -> System:
+    """One batched-ensemble replica: harmonic chains + 0..2 trapped probes.
+
+    pair_mode 1 (default) uses the RPY monomer-monomer and monomer-colloid
+    scalars; with the reference's own scalars (pair_mode 0) the grand mobility is
+    indefinite and the explicit predictor-corrector diverges within a few steps.
+    dt defaults to 1e-4: at 1e-3 the stated spring constants (kbond = 900,
+    mobility up to ~40) exceed the explicit integrator's stability limit."""
     nprobe = int(rng.integers(0, 3))
     L = int(rng.integers(16, 65))
     npoly = max(1, int(round((N - nprobe) / L)))
@@ -207,15 +215,16 @@ def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0) -> System:
     xm = _chains(rng, npoly, L, beta, step, None, start, grid, bound=R * 1.5)
     x = np.vstack([xm] + ([np.array(colloids)] if colloids else []))
     params = make_params(Nm=Nm, Nc=nprobe, Npoly=npoly, Nmono_per_chain=L, beta=beta, kT=1.0,
-                         kbond=900.0, r0=step, Lmax=10 * step, dt=1e-3, mm_HI=1, chain_HI=0, fene=0,
-                         ktrap=4500.0 if nprobe else 0.0, tstart=0.0, trun=1e9)
+                         kbond=900.0, r0=step, Lmax=10 * step, dt=dt, mm_HI=1, chain_HI=0, fene=0,
+                         ktrap=4500.0 if nprobe else 0.0, tstart=0.0, trun=1e9, aa_mode=pair_mode,
+                         ab_mode=pair_mode)
     return System(f"ensemble_{N}", params, x)
 
 
-def ensemble(n_rep: int = 256, seed: int = 0, nmin: int = 64, nmax: int = 4096) -> list[System]:
+def ensemble(n_rep: int = 256, seed: int = 0, nmin: int = 64, nmax: int = 4096, **kw) -> list[System]:
     rng = np.random.default_rng(seed)
     Ns = np.rint(np.exp(rng.uniform(math.log(nmin), math.log(nmax), size=n_rep))).astype(int)
-    return [ensemble_member(np.random.default_rng([seed, i]), int(N)) for i, N in enumerate(Ns)]
+    return [ensemble_member(np.random.default_rng([seed, i]), int(N), **kw) for i, N in enumerate(Ns)]
 
 
 def small_mixed(seed: int = 0, Nm_chain=(3, 4), Nc: int = 3, mm_HI: int = 1, beta: float = 0.3,

@@ -103,7 +103,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         s.nm3nc3 = s.nm3 + s.nc3; s.nm3nc6 = s.nm3 + s.nc6; s.nm3nc11 = s.nm3 + s.nc11;
         s.n = s.nm3nc11 + s.nm3nc6;
         s.mm_HI = d.mm_HI; s.chain_HI = d.chain_HI; s.ab_mode = d.ab_mode; s.box_on = d.box_on;
-        s.fene = d.fene; s.mono_ev = d.mono_ev; s.lub_on = d.lub_on; s.tether = d.tether;
+        s.fene = d.fene; s.mono_ev = d.mono_ev; s.lub_on = d.lub_on; s.tether = d.tether; s.aa_mode = d.aa_mode;
         s.beta = d.beta; s.beta_inv = 1.0 / d.beta; s.kT = d.kT; s.dt = d.dt; s.epsilon = d.epsilon;
         s.kbond = d.kbond; s.r0 = d.r0; s.Lmax = d.Lmax;
         for (int k = 0; k < 3; k++) s.L[k] = d.box_on ? d.box[k] : 0.0;

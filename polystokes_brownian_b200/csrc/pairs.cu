@@ -29,12 +29,13 @@ __device__ __forceinline__ void mimg(const Seg &s, double &dx, double &dy, doubl
     dz -= s.L[2] * nearbyint(dz * (1.0 / s.L[2]));
 }
 
+// clamp in double before converting: NaN and out-of-range values map into [0, nc)
 __device__ __forceinline__ int ccoord(double v, double org, double size, int nc)
 {
-    int c = (int)floor((v - org) / size);
-    if (c < 0) c = 0;
-    if (c >= nc) c = nc - 1;
-    return c;
+    double f = floor((v - org) / size);
+    if (!(f >= 0.0)) return 0;
+    if (f >= (double)nc) return nc - 1;
+    return (int)f;
 }
 
 // does pair (b, j), b < j (global indices, same replica) belong to list `which`?

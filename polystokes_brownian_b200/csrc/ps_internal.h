@@ -26,7 +26,7 @@ struct Seg {
     int top_off;       // offset in the concatenated mobility (nm3nc11) space
     int vel_off;       // offset in the concatenated velocity (nm3nc6) space
     int n, nm3, nc3, nc5, nc6, nc11, nm3nc3, nm3nc6, nm3nc11;
-    int mm_HI, chain_HI, ab_mode, box_on, fene, mono_ev, lub_on, tether;
+    int mm_HI, chain_HI, ab_mode, box_on, fene, mono_ev, lub_on, tether, aa_mode;
     int shell_schur;   // shell path with the dense Schur floor (nc11 <= lanczos_nc)
     int schur_off;     // offset into the per-replica nc11^2 buffers
     int ba_off;        // offset (in 11-vectors) of this replica's BA partials
@@ -64,6 +64,23 @@ __device__ __forceinline__ void aa_scalars(T r, T rinv, T two_beta, T &x, T &y)
     } else {
         x = T(0.375) * r - T(1.0);
         y = T(1.0) - T(0.28125) * r;
+    }
+}
+
+// Equal-sphere RPY of radius b = two_beta/2 in units 6 pi eta = 1, with the
+// overlap form for r <= 2b (PS_AA_RPY).
+template <class T>
+__device__ __forceinline__ void aa_scalars_rpy(T r, T rinv, T two_beta, T &x, T &y)
+{
+    T b = T(0.5) * two_beta;
+    if (r > two_beta) {
+        T ri3 = rinv * rinv * rinv, b2 = b * b;
+        x = T(1.5) * rinv - b2 * ri3;
+        y = T(0.75) * rinv + T(0.5) * b2 * ri3;
+    } else {
+        T bi = T(1) / b;
+        x = (T(1) - T(0.1875) * r * bi) * bi;
+        y = (T(1) - T(0.28125) * r * bi) * bi;
     }
 }
 

@@ -57,6 +57,7 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     P4 pi = active ? pos[sg.bead_off + i] : pos[sg.bead_off + tl.row0];
     const T two_beta = T(2.0 * sg.beta);
     const bool chain_hi = sg.chain_HI != 0;
+    const bool rpy = sg.aa_mode == PS_AA_RPY;
     Acc<T> a0, a1, a2;
     a0.zero(); a1.zero(); a2.zero();
     for (int jt = j0; jt < j1; jt += RPY_THREADS) {
@@ -80,7 +81,8 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             T rinv = rsqrt_t<T>(r2);
             T r = r2 * rinv;
             T x, y;
-            aa_scalars<T>(r, rinv, two_beta, x, y);
+            if (rpy) aa_scalars_rpy<T>(r, rinv, two_beta, x, y);
+            else aa_scalars<T>(r, rinv, two_beta, x, y);
             T u0 = su[3 * k], u1 = su[3 * k + 1], u2 = su[3 * k + 2];
             // mob_a u = y u + (x - y)(e.u) e,  e = d / r
             T f = (x - y) * (dx * u0 + dy * u1 + dz * u2) * rinv * rinv;

@@ -61,6 +61,15 @@ int stage_pack(Engine &E, cudaStream_t st)
     return PS_OK;
 }
 
+// clamp in double before converting: NaN and out-of-range values map into [0, nc)
+__device__ __forceinline__ int cell_coord(double v, double org, double size, int nc)
+{
+    double f = floor((v - org) / size);
+    if (!(f >= 0.0)) return 0;
+    if (f >= (double)nc) return nc - 1;
+    return (int)f;
+}
+
 // ---------------------------------------------------------------------------
 // monomer cell list (search structure only: its pair sets equal the
 // reference's because membership is decided by the same `dr < cutoff` test).
@@ -102,22 +111,30 @@ __global__ void k_cell_geo(const Seg *__restrict__ segs, const double *__restric
             rc = fmax(rc, (double)s.rcut[0]);
             if (s.lub_on) rc = fmax(rc, (2.0 + s.lub_gap) * s.beta);
         }
-        long cap = pass == 0 ? 2L * s.Nm + 8 : (1L << 62);
+        // cell counts are computed in double and clamped to [1, 2^20] before any
+        // integer conversion, so non-finite or huge coordinates cannot overflow
+        double cap = pass == 0 ? 2.0 * s.Nm + 8.0 : 1e18;
         int nc[3];
         double org[3], size[3], ext[3];
         int periodic = 0;
+        auto count = [&](double len) {
+            double n = floor(len / rc);
+            if (!(n >= 1.0)) n = 1.0;
+            if (n > 1048576.0) n = 1048576.0;
+            return (int)n;
+        };
         if (s.box_on) {
-            for (int d = 0; d < 3; d++) { nc[d] = (int)floor(s.L[d] / rc); ext[d] = s.L[d]; org[d] = -0.5 * s.L[d]; }
+            for (int d = 0; d < 3; d++) { nc[d] = count(s.L[d]); ext[d] = s.L[d]; org[d] = -0.5 * s.L[d]; }
             periodic = (nc[0] >= 3 && nc[1] >= 3 && nc[2] >= 3);
         } else {
             for (int d = 0; d < 3; d++) {
                 double a = s.Nm ? lo[d][0] : 0.0, b = s.Nm ? hi[d][0] : 0.0;
+                if (!isfinite(a) || !isfinite(b)) { a = 0.0; b = 0.0; }
                 ext[d] = b - a; org[d] = a;
-                int n = (int)floor(ext[d] / rc);
-                nc[d] = n > 1 ? n : 1;
+                nc[d] = count(ext[d]);
             }
         }
-        while ((long)nc[0] * nc[1] * nc[2] > cap) {
+        while ((double)nc[0] * (double)nc[1] * (double)nc[2] > cap) {
             int m = 0;
             for (int d = 1; d < 3; d++) if (nc[d] > nc[m]) m = d;
             nc[m] = (nc[m] + 1) / 2;
@@ -127,6 +144,7 @@ __global__ void k_cell_geo(const Seg *__restrict__ segs, const double *__restric
         for (int d = 0; d < 3; d++) {
             if (s.box_on) size[d] = s.L[d] / nc[d];
             else size[d] = ext[d] > 0.0 ? ext[d] / nc[d] : rc;
+            if (!(size[d] > 0.0) || !isfinite(size[d])) size[d] = rc;
         }
         if (s.box_on && !periodic)
             for (int d = 0; d < 3; d++) size[d] = s.L[d] > 0.0 ? s.L[d] : 1.0;
@@ -144,10 +162,8 @@ __device__ __forceinline__ bool ref_cells_adjacent(const double *__restrict__ gr
 {
     for (int d = 0; d < 3; d++) {
         int nc = (int)gref[6 + d];
-        int ci = (int)floor((x[3 * i + d] - gref[d]) / gref[3 + d]);
-        int cj = (int)floor((x[3 * j + d] - gref[d]) / gref[3 + d]);
-        ci = ci < 0 ? 0 : (ci >= nc ? nc - 1 : ci);
-        cj = cj < 0 ? 0 : (cj >= nc ? nc - 1 : cj);
+        int ci = cell_coord(x[3 * i + d], gref[d], gref[3 + d], nc);
+        int cj = cell_coord(x[3 * j + d], gref[d], gref[3 + d], nc);
         int dc = ci - cj;
         if (gref[9] != 0.0) {
             dc = ((dc % nc) + nc) % nc;
@@ -157,13 +173,6 @@ __device__ __forceinline__ bool ref_cells_adjacent(const double *__restrict__ gr
     return true;
 }
 
-__device__ __forceinline__ int cell_coord(double v, double org, double size, int nc)
-{
-    int c = (int)floor((v - org) / size);
-    if (c < 0) c = 0;
-    if (c >= nc) c = nc - 1;
-    return c;
-}
 
 __global__ void k_cell_assign(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                               const double *__restrict__ x, const double *__restrict__ geo,
@@ -484,7 +493,8 @@ __global__ void k_assemble(int R, const Seg *__restrict__ segs, const double *__
             double dr = pair_geom(s, x, (long)s.bead_off + li, (long)s.bead_off + lj, e);
             double ri = 1 / dr;
             double xx, yy;
-            aa_scalars<double>(dr, ri, 2.0 * s.beta, xx, yy);
+            if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(dr, ri, 2.0 * s.beta, xx, yy);
+            else aa_scalars<double>(dr, ri, 2.0 * s.beta, xx, yy);
             for (int a = 0; a < 3; a++)
                 for (int c = 0; c < 3; c++) sa[3 * a + c] = (a == c) ? xx * e[a] * e[a] + yy * (1. - e[a] * e[a])
                                                                    : xx * (e[a] * e[c]) - yy * (e[a] * e[c]);

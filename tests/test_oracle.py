@@ -72,7 +72,7 @@ def test_stale_ab_block_is_last_aa_pair():
     Nm = sysm.params["Nm"]
     d = sysm.x[Nm - 2] - sysm.x[Nm - 1]
     r = np.linalg.norm(d)
-    T = po.tensor_aa(d / r, r, sysm.params["beta"]).reshape(3, 3)
+    T = po.tensor_aa(d / r, r, sysm.params["beta"], 0).reshape(3, 3)
     assert np.allclose(s.stale_a(), T, rtol=0, atol=1e-15)
 
 
