@@ -156,6 +156,24 @@ int ps_sqrtm_apply(ps_ctx *ctx, const double *z, double *w, const ps_sqrt_opts *
 int ps_step(ps_ctx *ctx, const ps_step_inputs *in, ps_step_result *res, void *stream);
 int ps_step_outputs(ps_ctx *ctx, double *up, double *udiff, double *sb, double *fext, void *stream);
 
+/* allocation-free entry point ----------------------------------------------
+ * ps_mobility_apply_noalloc: y = M u for ONE system of N monomers (the
+ * monomer-monomer far-field mobility with full HI and the reference's pair
+ * scalars, PS_AA_REFERENCE: beta^{-1} u plus the pair blocks, skipping
+ * same-chain pairs when chain_HI; chains are contiguous runs of
+ * Nmono_per_chain monomers).  x: 3N positions, u: 3N forces, y: 3N velocities,
+ * all device pointers.  It has no counterpart in the reference: it exists for
+ * callers that must not allocate device memory (an operator callback run inside
+ * a host solver that owns the device memory pool, or a latency-critical loop
+ * where cudaMalloc's implicit synchronisation or failure is not acceptable).
+ * It allocates nothing: its scratch is a fixed 3.4 MB __device__ array held by
+ * every GPU that loads this library until exit, so N is limited to 8192
+ * (larger N returns PS_ERR_TOO_LARGE).  The first call on a device looks up the
+ * array's device address and should come before any stream capture.  Calls
+ * share the array, so calls that overlap on the GPU race; serialise them. */
+int ps_mobility_apply_noalloc(const double *x, const double *u, double *y, int32_t N, double beta,
+                              int32_t chain_HI, int32_t Nmono_per_chain, void *stream);
+
 /* diagnostics ---------------------------------------------------------------
  * ps_time_kernel: average device time (ms, CUDA events on `stream`) of `reps`
  * launches of one far-field kernel on mobility-layout input u; which: 0 the

@@ -109,6 +109,7 @@ def lib():
     L.ps_time_kernel.argtypes = [vp, C.c_int32, C.c_int32, P, C.POINTER(C.c_double), vp]
     L.ps_fma_peak.argtypes = [C.c_int32, C.POINTER(C.c_double), vp]
     L.ps_kernel_launches.restype = C.c_uint64
+    L.ps_mobility_apply_noalloc.argtypes = [P, P, P, C.c_int32, C.c_double, C.c_int32, C.c_int32, vp]
     _lib = L
     return L
 
