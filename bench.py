@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--rtol", type=float, default=1e-6)
+    ap.add_argument("--solver", default="structured", choices=["minres", "structured"])
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
@@ -197,8 +198,9 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
     for _ in range(args.warmup):
-        b.step(rtol=args.rtol)
+        b.step(rtol=args.rtol, solver=solver)
     barrier()
     L = _capi.lib()
     launches0 = L.ps_kernel_launches()
@@ -211,7 +213,7 @@ def run_b200(args):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        r = b.step(rtol=args.rtol)
+        r = b.step(rtol=args.rtol, solver=solver)
         e1.record(st)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
@@ -240,7 +242,7 @@ def run_b200(args):
     e2e_iters = []
     for _ in range(args.steps):
         _capi.check(L.ps_set_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_set_state")
-        r = b.step(rtol=args.rtol)
+        r = b.step(rtol=args.rtol, solver=solver)
         e2e_iters.append(list(r.iters))
         _capi.check(L.ps_get_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_get_state")
     e1.record(st)
@@ -274,7 +276,8 @@ def run_b200(args):
                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == _capi.PS_PREC_FP64 else "f32+f64",
                "data": "synthetic",
                "config": {"workload": name, "replicas": len(systems), "beads": beads, "rtol": args.rtol,
-                          "precision": args.precision, "l2": "flushed (256 MB write) before every timed step",
+                          "precision": args.precision, "solver": args.solver,
+                          "l2": "flushed (256 MB write) before every timed step",
                           "parallelism": f"replicas x{world}"},
                "latency_ms": {"p50": lat_sorted[len(lat) // 2], "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
                "minres_iters": iters, "minres_reason": reasons, "e2e_minres_iters": e2e_iters,

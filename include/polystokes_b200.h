@@ -52,6 +52,15 @@ extern "C" {
 #define PS_AA_REFERENCE 0
 #define PS_AA_RPY 1
 
+/* Saddle solver.  PS_SOLVE_MINRES: preconditioned MINRES with Jacobi, as the
+ * reference's KSPSolve.  PS_SOLVE_STRUCTURED: exact elimination of the
+ * constraint block -- F_t = -b_bot, one dense colloid-stresslet solve
+ * M_SS F_S = b_S - (M F)_S, then U = (M F)_t - b_t (two operator applies) --
+ * followed by warm-started MINRES only where the elimination is not exact
+ * (lubrication, or more than 12 colloids in a replica). */
+#define PS_SOLVE_MINRES 0
+#define PS_SOLVE_STRUCTURED 1
+
 /* precision of the far-field matvec and Krylov vectors */
 #define PS_PREC_FP64 0
 #define PS_PREC_MIXED 1
@@ -82,6 +91,7 @@ typedef struct ps_ksp_opts {
     int32_t maxit;      /* iteration cap (PETSc default 10000) */
     int32_t warm;       /* nonzero: x holds the initial guess */
     int32_t check_every;/* host convergence poll period in iterations (0 = 8) */
+    int32_t method;     /* PS_SOLVE_MINRES (the reference's MINRES + Jacobi) or PS_SOLVE_STRUCTURED */
 } ps_ksp_opts;
 
 typedef struct ps_ksp_result {
@@ -111,6 +121,7 @@ typedef struct ps_step_inputs {
     int32_t maxit;
     int32_t sqrt_kmax;  /* Lanczos subspace cap of the noise (0: 40) */
     double sqrt_tol;    /* Lanczos relative tolerance of the noise (0: 1e-6) */
+    int32_t solver;     /* PS_SOLVE_MINRES (default) or PS_SOLVE_STRUCTURED */
 } ps_step_inputs;
 
 typedef struct ps_step_result {

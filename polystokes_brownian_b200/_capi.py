@@ -21,6 +21,8 @@ PS_AA_REFERENCE = 0
 PS_AA_RPY = 1
 PS_PREC_FP64 = 0
 PS_PREC_MIXED = 1
+PS_SOLVE_MINRES = 0
+PS_SOLVE_STRUCTURED = 1
 
 
 class PsDesc(C.Structure):
@@ -40,7 +42,8 @@ class PsDesc(C.Structure):
 
 
 class PsKspOpts(C.Structure):
-    _fields_ = [("rtol", C.c_double), ("maxit", C.c_int32), ("warm", C.c_int32), ("check_every", C.c_int32)]
+    _fields_ = [("rtol", C.c_double), ("maxit", C.c_int32), ("warm", C.c_int32), ("check_every", C.c_int32),
+                ("method", C.c_int32)]
 
 
 class PsKspResult(C.Structure):
@@ -58,7 +61,8 @@ class PsSqrtResult(C.Structure):
 
 class PsStepInputs(C.Structure):
     _fields_ = [("fb", C.c_void_p), ("wrfd", C.c_void_p), ("zlub", C.c_void_p),
-                ("rtol", C.c_double), ("maxit", C.c_int32), ("sqrt_kmax", C.c_int32), ("sqrt_tol", C.c_double)]
+                ("rtol", C.c_double), ("maxit", C.c_int32), ("sqrt_kmax", C.c_int32), ("sqrt_tol", C.c_double),
+                ("solver", C.c_int32)]
 
 
 class PsStepResult(C.Structure):

@@ -53,7 +53,7 @@ static void free_engine(Engine &E)
     void *ptrs[] = {E.d_segs, E.d_vec_offs, E.d_top_offs, E.d_vel_offs, E.d_bead_offs, E.d_x, E.d_q, E.d_xpos0,
                     E.d_xn, E.d_pos64, E.d_pos32, E.d_chain, E.d_coll_rep, E.d_time, E.d_ktrap, E.d_trapinfo,
                     E.d_aa_tiles, E.d_ab_tiles, E.d_bb_tiles, E.d_partAA, E.d_partAB, E.d_partBB, E.d_partBA,
-                    E.d_tab, E.d_stale, E.d_aa_last, E.d_delta, E.d_schurQ, E.d_schurL, E.d_schur_reps,
+                    E.d_tab, E.d_stale, E.d_aa_last, E.d_delta, E.d_schurQ, E.d_schurL, E.d_schur_reps, E.d_ss_reps,
                     E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_cell, E.d_cell_start, E.d_cell_sorted,
                     E.d_cell_count, E.d_cellgeo, E.d_cell_offs, E.d_nbr_ptr, E.d_nbr, E.d_nbr_count, E.d_lubtab,
                     E.d_luby, E.d_lub_diag, E.d_lub_ptr, E.d_lub_nbr, E.d_D, E.d_z, E.d_v, E.d_xw, E.d_Rr[0],
@@ -78,7 +78,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     std::vector<int> bead_offs(R + 1), vec_offs(R + 1), top_offs(R + 1), vel_offs(R + 1);
     std::vector<long> cell_offs(R + 1);
     std::vector<Tile> aa, ab, bb;
-    std::vector<int> schur_reps;
+    std::vector<int> schur_reps, ss_reps;
+    int ss_polish = 0;
     const int TR = 128;
     int kTpos = 0, kTzero = 0;
     for (int r = 0; r < R; r++) {
@@ -124,6 +125,10 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
             return PS_ERR_UNSUPPORTED;
         }
         if (s.shell_schur) { s.schur_off = (int)schur; schur += (long)s.nc11 * s.nc11; schur_reps.push_back(r); }
+        if (d.Nc > 0) {
+            if (s.nc5 <= 64) ss_reps.push_back(r);
+            else ss_polish++;
+        }
         // tiles
         s.n_mtiles = (d.Nm + TR - 1) / TR;
         s.ba_off = (int)ba;
@@ -182,6 +187,9 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     if ((rc = upload(E.d_ab_tiles, ab))) return rc;
     if ((rc = upload(E.d_bb_tiles, bb))) return rc;
     if ((rc = upload(E.d_schur_reps, schur_reps))) return rc;
+    if ((rc = upload(E.d_ss_reps, ss_reps))) return rc;
+    E.n_ss_reps = (int)ss_reps.size();
+    E.n_ss_polish = ss_polish;
     // per-bead chain ids, colloid -> replica, bonds
     std::vector<double> chain(bead);
     std::vector<int> coll_rep(std::max<long>(coll, 1));
@@ -453,6 +461,7 @@ int ps_get_diagonal(ps_ctx *ctx, double *d, void *stream)
 int ps_ksp_solve(ps_ctx *ctx, const double *b, double *x, const ps_ksp_opts *opts, ps_ksp_result *res, void *stream)
 {
     if (!ctx || !b || !x) return PS_ERR_ARG;
+    if (opts && opts->method == PS_SOLVE_STRUCTURED) return ps::structured_solve(ctx->E, b, x, opts, res, S(stream));
     return ps::minres_solve(ctx->E, b, x, opts, res, S(stream));
 }
 

@@ -290,7 +290,7 @@ __global__ void k_mr_flush(RedTable T, const double *__restrict__ v, double *__r
 
 int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res, cudaStream_t st)
 {
-    ps_ksp_opts opt = {1e-6, 10000, 0, 8};
+    ps_ksp_opts opt = {1e-6, 10000, 0, 8, PS_SOLVE_MINRES};
     if (o) opt = *o;
     if (opt.check_every <= 0) opt.check_every = 8;
     if (opt.maxit <= 0) opt.maxit = 10000;

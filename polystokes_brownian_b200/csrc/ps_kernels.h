@@ -66,6 +66,8 @@ struct Engine {
     long nschur = 0;
     double *d_delta = nullptr, *d_schurQ = nullptr, *d_schurL = nullptr;
     int *d_schur_reps = nullptr; int n_schur_reps = 0;
+    int *d_ss_reps = nullptr; int n_ss_reps = 0;   // replicas whose stresslet block is solved densely
+    int n_ss_polish = 0;                           // replicas with colloids beyond the dense limit
 
     // bonds (per-bead CSR: partner, sign)
     int *d_bond_ptr = nullptr, *d_bond_nbr = nullptr;
@@ -129,6 +131,9 @@ int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps
 int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStream_t st);
 // krylov.cu
 int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res, cudaStream_t st);
+// solve.cu
+int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
+                     cudaStream_t st);
 int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
 int build_red_table(Engine &E, RedTable &T, bool top);
 void free_red_table(RedTable &T);

@@ -249,10 +249,12 @@ static int stage(Engine &E, double *rhs, cudaStream_t st)
 static int solve(Engine &E, const double *b, double *x, int warm, const ps_step_inputs *in, ps_step_result *res,
                  int slot, cudaStream_t st)
 {
-    ps_ksp_opts o = {in ? in->rtol : 1e-6, in && in->maxit > 0 ? in->maxit : 10000, warm, 8};
+    ps_ksp_opts o = {in ? in->rtol : 1e-6, in && in->maxit > 0 ? in->maxit : 10000, warm, 8,
+                     in ? in->solver : PS_SOLVE_MINRES};
     if (o.rtol <= 0) o.rtol = 1e-6;
     ps_ksp_result kr;
-    int reason = minres_solve(E, b, x, &o, &kr, st);
+    int reason = (o.method == PS_SOLVE_STRUCTURED) ? structured_solve(E, b, x, &o, &kr, st)
+                                                   : minres_solve(E, b, x, &o, &kr, st);
     if (reason == PS_ERR_CUDA) return reason;
     if (res) {
         res->iters[slot] = kr.iters_max;

@@ -127,9 +127,10 @@ class Batch:
         check(lib().ps_get_diagonal(self.h, _ptr(d), self.stream), "ps_get_diagonal")
         return d
 
-    def solve(self, b: torch.Tensor, x0: torch.Tensor | None = None, rtol: float = 1e-8, maxit: int = 10000):
+    def solve(self, b: torch.Tensor, x0: torch.Tensor | None = None, rtol: float = 1e-8, maxit: int = 10000,
+              method: int = _capi.PS_SOLVE_MINRES):
         x = self.zeros(self.nvec) if x0 is None else x0.clone()
-        o = _capi.PsKspOpts(rtol, maxit, int(x0 is not None), 8)
+        o = _capi.PsKspOpts(rtol, maxit, int(x0 is not None), 8, method)
         r = _capi.PsKspResult()
         rc = lib().ps_ksp_solve(self.h, _ptr(b), _ptr(x), C.byref(o), C.byref(r), self.stream)
         if rc == _capi.PS_OK - 2:
@@ -144,9 +145,9 @@ class Batch:
         return w, r
 
     def step(self, fb: torch.Tensor | None = None, wrfd: torch.Tensor | None = None, rtol: float = 1e-8,
-             maxit: int = 10000, sqrt_kmax: int = 0, sqrt_tol: float = 0.0):
+             maxit: int = 10000, sqrt_kmax: int = 0, sqrt_tol: float = 0.0, solver: int = 0):
         inp = _capi.PsStepInputs(None if fb is None else fb.data_ptr(), None if wrfd is None else wrfd.data_ptr(),
-                                 None, rtol, maxit, sqrt_kmax, sqrt_tol)
+                                 None, rtol, maxit, sqrt_kmax, sqrt_tol, solver)
         res = _capi.PsStepResult()
         check(lib().ps_step(self.h, C.byref(inp), C.byref(res), self.stream), "ps_step")
         return res
