@@ -41,10 +41,15 @@ template <> struct Acc<float> {
 template <class T>
 __global__ void __launch_bounds__(RPY_THREADS)
 k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
-         const double *__restrict__ u, int in_top, double *__restrict__ part, long part_stride, int nchunk)
+         const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
+         long part_stride, int nchunk)
 {
+    // FP32: positions are split hi + lo (both float) so that pair separations
+    // keep FP64-level accuracy: d = (hi_i - hi_j) + (lo_i - lo_j).
     typedef typename V4<T>::t P4;
+    constexpr bool F32 = sizeof(T) == 4;
     __shared__ P4 sp[RPY_THREADS];
+    __shared__ float4 sl[F32 ? RPY_THREADS : 1];
     __shared__ T su[RPY_THREADS * 3];
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
@@ -55,6 +60,8 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     const bool active = threadIdx.x < tl.nrow;
     const int uoff = in_top ? sg.top_off : sg.vec_off;
     P4 pi = active ? pos[sg.bead_off + i] : pos[sg.bead_off + tl.row0];
+    float4 li = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (F32) li = plo[sg.bead_off + (active ? i : tl.row0)];
     const T two_beta = T(2.0 * sg.beta);
     const bool chain_hi = sg.chain_HI != 0;
     const bool rpy = sg.aa_mode == PS_AA_RPY;
@@ -66,6 +73,7 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
         if (threadIdx.x < nj) {
             int j = jt + threadIdx.x;
             sp[threadIdx.x] = pos[sg.bead_off + j];
+            if constexpr (F32) sl[threadIdx.x] = plo[sg.bead_off + j];
             su[3 * threadIdx.x + 0] = (T)u[uoff + 3 * j + 0];
             su[3 * threadIdx.x + 1] = (T)u[uoff + 3 * j + 1];
             su[3 * threadIdx.x + 2] = (T)u[uoff + 3 * j + 2];
@@ -75,6 +83,10 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
         for (int k = 0; k < nj; k++) {
             P4 pj = sp[k];
             T dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            if constexpr (F32) {
+                float4 lj = sl[k];
+                dx += li.x - lj.x; dy += li.y - lj.y; dz += li.z - lj.z;
+            }
             T r2 = dx * dx + dy * dy + dz * dz;
             bool skip = (jt + k == i) || (chain_hi && pi.w == pj.w);
             if (skip) continue;
@@ -107,10 +119,11 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
 template <class T>
 __global__ void __launch_bounds__(RPY_THREADS)
 k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
-         const double *__restrict__ u, int in_top, const double *__restrict__ tab, double *__restrict__ part_m,
-         double *__restrict__ part_ba)
+         const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, const double *__restrict__ tab,
+         double *__restrict__ part_m, double *__restrict__ part_ba)
 {
     typedef typename V4<T>::t P4;
+    constexpr bool F32 = sizeof(T) == 4;
     __shared__ T red[RPY_THREADS / 32][12];
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
@@ -137,6 +150,10 @@ k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
         }
         for (int q = 0; q < 5; q++) Sc[q] = (T)u[uoff + sg.nm3nc6 + 5 * cc + q];
         T dx = pm.x - pc.x, dy = pm.y - pc.y, dz = pm.z - pc.z;
+        if constexpr (F32) {
+            float4 lm = plo[sg.bead_off + (active ? i : tl.row0)], lc = plo[sg.bead_off + Nm + cc];
+            dx += lm.x - lc.x; dy += lm.y - lc.y; dz += lm.z - lc.z;
+        }
         T r2 = dx * dx + dy * dy + dz * dz;
         T rinv = rsqrt_t<T>(r2);
         T e[3] = {dx * rinv, dy * rinv, dz * rinv};
@@ -203,11 +220,14 @@ k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
 template <class T>
 __global__ void __launch_bounds__(RPY_THREADS)
 k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
-         const double *__restrict__ u, int in_top, double *__restrict__ part, long part_stride, int nchunk)
+         const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
+         long part_stride, int nchunk)
 {
     typedef typename V4<T>::t P4;
+    constexpr bool F32 = sizeof(T) == 4;
     constexpr int CT = 64;
     __shared__ P4 sp[CT];
+    __shared__ float4 sl[F32 ? CT : 1];
     __shared__ T su[CT * 11];
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
@@ -218,6 +238,8 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     const bool active = threadIdx.x < tl.nrow;
     const int uoff = in_top ? sg.top_off : sg.vec_off;
     P4 pi = pos[sg.bead_off + Nm + (active ? i : tl.row0)];
+    float4 li = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (F32) li = plo[sg.bead_off + Nm + (active ? i : tl.row0)];
     Acc<T> acc[11];
     for (int q = 0; q < 11; q++) acc[q].zero();
     for (int jt = j0; jt < j1; jt += CT) {
@@ -228,7 +250,10 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             int idx = q < 3 ? sg.nm3 + 3 * j + q : (q < 6 ? sg.nm3 + sg.nc3 + 3 * j + (q - 3) : sg.nm3nc6 + 5 * j + (q - 6));
             su[t] = (T)u[uoff + idx];
         }
-        if (threadIdx.x < nj) sp[threadIdx.x] = pos[sg.bead_off + Nm + jt + threadIdx.x];
+        if (threadIdx.x < nj) {
+            sp[threadIdx.x] = pos[sg.bead_off + Nm + jt + threadIdx.x];
+            if constexpr (F32) sl[threadIdx.x] = plo[sg.bead_off + Nm + jt + threadIdx.x];
+        }
         __syncthreads();
         T out[11];
         for (int q = 0; q < 11; q++) out[q] = T(0);
@@ -237,9 +262,12 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             if (j == i) continue;
             P4 pj = sp[k];
             bool lo = i < j;
-            T dx = lo ? pi.x - pj.x : pj.x - pi.x;
-            T dy = lo ? pi.y - pj.y : pj.y - pi.y;
-            T dz = lo ? pi.z - pj.z : pj.z - pi.z;
+            T dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            if constexpr (F32) {
+                float4 lj = sl[k];
+                dx += li.x - lj.x; dy += li.y - lj.y; dz += li.z - lj.z;
+            }
+            if (!lo) { dx = -dx; dy = -dy; dz = -dz; }
             T r2 = dx * dx + dy * dy + dz * dz;
             T rinv = rsqrt_t<T>(r2);
             T e[3] = {dx * rinv, dy * rinv, dz * rinv};
@@ -333,13 +361,13 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st)
 {
     const typename V4<T>::t *pos = (const typename V4<T>::t *)(sizeof(T) == 8 ? (const void *)E.d_pos64 : (const void *)E.d_pos32);
     if (E.n_aa_tiles)
-        ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, pos, u, in_top,
+        ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top,
                                                                          E.d_partAA, E.part_stride, E.nch_aa);
     if (E.n_ab_tiles)
-        ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, u, in_top, E.d_tab, E.d_partAB,
+        ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
                                                          E.d_partBA);
     if (E.n_bb_tiles)
-        ::ps_launch_count++, k_rpy_bb<T><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, pos, u, in_top,
+        ::ps_launch_count++, k_rpy_bb<T><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, pos, E.d_pos32lo, u, in_top,
                                                                          E.d_partBB, E.part_stride, E.nch_bb);
 }
 
@@ -374,14 +402,14 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     cudaEventCreate(&b);
     auto launch = [&]() {
         if (which == 0 && E.n_aa_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_aa<float><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
-            else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
+            if (fp32) ::ps_launch_count++, k_rpy_aa<float><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
+            else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
         } else if (which == 1 && E.n_ab_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
-            else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
+            if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
+            else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
         } else if (which == 2 && E.n_bb_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_bb<float><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const float4 *)pos, u, 1, E.d_partBB, E.part_stride, E.nch_bb);
-            else ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const double4 *)pos, u, 1, E.d_partBB, E.part_stride, E.nch_bb);
+            if (fp32) ::ps_launch_count++, k_rpy_bb<float><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb);
+            else ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb);
         } else if (which == 3) {
             apply_operator(E, 1, u, E.d_tmp_top2, nullptr, fp32, st);
         }

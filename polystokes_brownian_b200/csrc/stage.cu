@@ -44,19 +44,21 @@ __device__ __forceinline__ int rep_of(const int *__restrict__ offs, int R, long 
 // ---------------------------------------------------------------------------
 // packing: x (AoS doubles) -> (x,y,z,chain) in FP64 and FP32
 __global__ void k_pack(long ntot, const double *__restrict__ x, const double *__restrict__ chain,
-                       double4 *__restrict__ p64, float4 *__restrict__ p32)
+                       double4 *__restrict__ p64, float4 *__restrict__ p32, float4 *__restrict__ p32lo)
 {
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     double cx = x[3 * b], cy = x[3 * b + 1], cz = x[3 * b + 2], ch = chain[b];
     p64[b] = make_double4(cx, cy, cz, ch);
-    p32[b] = make_float4((float)cx, (float)cy, (float)cz, (float)ch);
+    float hx = (float)cx, hy = (float)cy, hz = (float)cz;
+    p32[b] = make_float4(hx, hy, hz, (float)ch);
+    p32lo[b] = make_float4((float)(cx - (double)hx), (float)(cy - (double)hy), (float)(cz - (double)hz), 0.f);
 }
 
 int stage_pack(Engine &E, cudaStream_t st)
 {
     int thr = 256;
-    ::ps_launch_count++, k_pack<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_x, E.d_chain, E.d_pos64, E.d_pos32);
+    ::ps_launch_count++, k_pack<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_x, E.d_chain, E.d_pos64, E.d_pos32, E.d_pos32lo);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
