@@ -118,6 +118,14 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         s.sig[0] = (float)(2. * d.beta); s.sig[1] = (float)(1. + d.beta); s.sig[2] = 2.0f;
         for (int k = 0; k < 3; k++) s.rcut[k] = (float)(pref * (double)s.sig[k]);
         s.lub_gap = d.lub_gap;
+        if (d.aa_mode == PS_AA_RPY) {
+            double b = d.beta, b2 = b * b;
+            const double c[8] = {1.5, -b2, 0.75, 0.5 * b2, 1.0 / b, -0.1875 / b2, 1.0 / b, -0.28125 / b2};
+            for (int k = 0; k < 8; k++) s.aa_c[k] = (float)c[k];
+        } else {
+            const double c[8] = {0.375, -2.0, 0.75, -0.5, -1.0, 0.375, 1.0, -0.28125};
+            for (int k = 0; k < 8; k++) s.aa_c[k] = (float)c[k];
+        }
         int lnc = d.lanczos_nc > 0 ? d.lanczos_nc : 64;
         s.shell_schur = (!d.mm_HI && d.Nc > 0 && s.nc11 <= lnc && s.nc11 <= PS_MAX_NC11_SCHUR);
         if (!d.mm_HI && d.Nc > 0 && !s.shell_schur && d.kT > 0) {

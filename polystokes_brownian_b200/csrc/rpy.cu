@@ -39,7 +39,7 @@ template <> struct Acc<float> {
 // AA: monomer rows x monomer columns (mm_HI only), 3 -> 3.
 // pos: (x,y,z,chain) per bead.  u: input vector, monomer F at off + 3 m.
 template <class T>
-__global__ void __launch_bounds__(RPY_THREADS)
+__global__ void __launch_bounds__(RPY_THREADS, 4)
 k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
          long part_stride, int nchunk)
@@ -64,7 +64,16 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     if constexpr (F32) li = plo[sg.bead_off + (active ? i : tl.row0)];
     const T two_beta = T(2.0 * sg.beta);
     const bool chain_hi = sg.chain_HI != 0;
-    const bool rpy = sg.aa_mode == PS_AA_RPY;
+    // scalars in FP64 from the mode (x = c0/r + c1/r^3, ... as in Seg::aa_c)
+    T c0, c1, c2, c3, c4, c5, c6, c7;
+    if (sg.aa_mode == PS_AA_RPY) {
+        T b = T(sg.beta), b2 = b * b;
+        c0 = T(1.5); c1 = -b2; c2 = T(0.75); c3 = T(0.5) * b2;
+        c4 = T(1) / b; c5 = T(-0.1875) / b2; c6 = T(1) / b; c7 = T(-0.28125) / b2;
+    } else {
+        c0 = T(0.375); c1 = T(-2.0); c2 = T(0.75); c3 = T(-0.5);
+        c4 = T(-1.0); c5 = T(0.375); c6 = T(1.0); c7 = T(-0.28125);
+    }
     Acc<T> a0, a1, a2;
     a0.zero(); a1.zero(); a2.zero();
     for (int jt = j0; jt < j1; jt += RPY_THREADS) {
@@ -93,8 +102,14 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             T rinv = rsqrt_t<T>(r2);
             T r = r2 * rinv;
             T x, y;
-            if (rpy) aa_scalars_rpy<T>(r, rinv, two_beta, x, y);
-            else aa_scalars<T>(r, rinv, two_beta, x, y);
+            if (r > two_beta) {
+                T ri3 = rinv * rinv * rinv;
+                x = c0 * rinv + c1 * ri3;
+                y = c2 * rinv + c3 * ri3;
+            } else {
+                x = c4 + c5 * r;
+                y = c6 + c7 * r;
+            }
             T u0 = su[3 * k], u1 = su[3 * k + 1], u2 = su[3 * k + 2];
             // mob_a u = y u + (x - y)(e.u) e,  e = d / r
             T f = (x - y) * (dx * u0 + dy * u1 + dz * u2) * rinv * rinv;
@@ -108,6 +123,98 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
         double *o = part + (long)c * part_stride + sg.top_off + 3 * i;
         o[0] = (double)a0.get(); o[1] = (double)a1.get(); o[2] = (double)a2.get();
     }
+}
+
+// ---------------------------------------------------------------------------
+// AA in FP32 with packed FP32x2 arithmetic (sm_100 FFMA2/FADD2/FMUL2): each
+// thread owns two rows (i and i + 64 of a 128-row tile) held in the two lanes of
+// float2 registers, so one packed instruction advances two pairs against the
+// same shared-memory column.  Positions are hi + lo floats, separations
+// d = (hi_i - hi_j) + (lo_i - lo_j).  Self pairs and skipped same-chain pairs
+// get rinv = 0, which zeroes their contribution without a branch; the near-
+// overlap form (r <= 2 beta) is applied only when some lane of the warp needs it.
+constexpr int AAF_THREADS = 64;
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+__global__ void __launch_bounds__(AAF_THREADS)
+k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const float4 *__restrict__ pos,
+            const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
+            long part_stride, int nchunk)
+{
+    __shared__ float4 sA[128];   // hi x, y, z, chain
+    __shared__ float4 sB[128];   // lo x, y, z, u0
+    __shared__ float2 sC[128];   // u1, u2
+    const Tile tl = tiles[blockIdx.x];
+    const Seg &sg = segs[tl.rep];
+    const int c = blockIdx.y;
+    const int Nm = sg.Nm;
+    const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
+    const int i0 = tl.row0 + threadIdx.x, i1 = i0 + AAF_THREADS;
+    const bool a0 = threadIdx.x < tl.nrow, a1 = threadIdx.x + AAF_THREADS < tl.nrow;
+    const int uoff = in_top ? sg.top_off : sg.vec_off;
+    const float4 P0 = pos[sg.bead_off + (a0 ? i0 : tl.row0)], P1 = pos[sg.bead_off + (a1 ? i1 : tl.row0)];
+    const float4 L0 = plo[sg.bead_off + (a0 ? i0 : tl.row0)], L1 = plo[sg.bead_off + (a1 ? i1 : tl.row0)];
+    const float2 px = make_float2(P0.x, P1.x), py = make_float2(P0.y, P1.y), pz = make_float2(P0.z, P1.z);
+    const float2 lx = make_float2(L0.x, L1.x), ly = make_float2(L0.y, L1.y), lz = make_float2(L0.z, L1.z);
+    const bool chain_hi = sg.chain_HI != 0;
+    const float2 cx1 = f2(sg.aa_c[0]), cx3 = f2(sg.aa_c[1]), cy1 = f2(sg.aa_c[2]), cy3 = f2(sg.aa_c[3]);
+    const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
+    const float two_beta = (float)(2.0 * sg.beta);
+    float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), kx = f2(0.f), ky = f2(0.f), kz = f2(0.f);
+    for (int jt = j0; jt < j1; jt += 128) {
+        const int nj = min(128, j1 - jt);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nj; t += AAF_THREADS) {
+            const int j = jt + t;
+            const float4 A = pos[sg.bead_off + j], B = plo[sg.bead_off + j];
+            sA[t] = A;
+            sB[t] = make_float4(B.x, B.y, B.z, (float)u[uoff + 3 * j]);
+            sC[t] = make_float2((float)u[uoff + 3 * j + 1], (float)u[uoff + 3 * j + 2]);
+        }
+        __syncthreads();
+        float2 tx = f2(0.f), ty = f2(0.f), tz = f2(0.f);
+#pragma unroll 4
+        for (int k = 0; k < nj; k++) {
+            const float4 A = sA[k], B = sB[k];
+            const float2 C = sC[k];
+            const int j = jt + k;
+            float2 dx = __fadd2_rn(__fadd2_rn(px, f2(-A.x)), __fadd2_rn(lx, f2(-B.x)));
+            float2 dy = __fadd2_rn(__fadd2_rn(py, f2(-A.y)), __fadd2_rn(ly, f2(-B.y)));
+            float2 dz = __fadd2_rn(__fadd2_rn(pz, f2(-A.z)), __fadd2_rn(lz, f2(-B.z)));
+            float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+            const bool e0 = (j == i0) || (chain_hi && P0.w == A.w);
+            const bool e1 = (j == i1) || (chain_hi && P1.w == A.w);
+            float2 ri = make_float2(e0 ? 0.f : rsqrtf(r2.x), e1 ? 0.f : rsqrtf(r2.y));
+            float2 ri2 = __fmul2_rn(ri, ri);
+            float2 ri3 = __fmul2_rn(ri2, ri);
+            float2 x = __ffma2_rn(cx3, ri3, __fmul2_rn(cx1, ri));
+            float2 y = __ffma2_rn(cy3, ri3, __fmul2_rn(cy1, ri));
+            float2 r = __fmul2_rn(r2, ri);
+            const bool n0 = !e0 && r.x <= two_beta, n1 = !e1 && r.y <= two_beta;
+            if (__any_sync(0xffffffffu, n0 || n1)) {
+                if (n0) { x.x = nx0 + nx1 * r.x; y.x = ny0 + ny1 * r.x; }
+                if (n1) { x.y = nx0 + nx1 * r.y; y.y = ny0 + ny1 * r.y; }
+            }
+            // mob_a u = y u + (x - y)(d.u) d / r^2
+            float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(B.w))));
+            float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(x, make_float2(-y.x, -y.y)), du), ri2);
+            tx = __ffma2_rn(f, dx, __ffma2_rn(y, f2(B.w), tx));
+            ty = __ffma2_rn(f, dy, __ffma2_rn(y, f2(C.x), ty));
+            tz = __ffma2_rn(f, dz, __ffma2_rn(y, f2(C.y), tz));
+        }
+        // Kahan across column tiles
+        float2 yy, tt;
+        yy = __fadd2_rn(tx, make_float2(-kx.x, -kx.y)); tt = __fadd2_rn(sx, yy);
+        kx = __fadd2_rn(__fadd2_rn(tt, make_float2(-sx.x, -sx.y)), make_float2(-yy.x, -yy.y)); sx = tt;
+        yy = __fadd2_rn(ty, make_float2(-ky.x, -ky.y)); tt = __fadd2_rn(sy, yy);
+        ky = __fadd2_rn(__fadd2_rn(tt, make_float2(-sy.x, -sy.y)), make_float2(-yy.x, -yy.y)); sy = tt;
+        yy = __fadd2_rn(tz, make_float2(-kz.x, -kz.y)); tt = __fadd2_rn(sz, yy);
+        kz = __fadd2_rn(__fadd2_rn(tt, make_float2(-sz.x, -sz.y)), make_float2(-yy.x, -yy.y)); sz = tt;
+    }
+    double *o = part + (long)c * part_stride + sg.top_off;
+    if (a0) { o[3 * i0] = sx.x; o[3 * i0 + 1] = sy.x; o[3 * i0 + 2] = sz.x; }
+    if (a1) { o[3 * i1] = sx.y; o[3 * i1 + 1] = sy.y; o[3 * i1 + 2] = sz.y; }
 }
 
 // ---------------------------------------------------------------------------
@@ -360,9 +467,14 @@ template <class T>
 void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st)
 {
     const typename V4<T>::t *pos = (const typename V4<T>::t *)(sizeof(T) == 8 ? (const void *)E.d_pos64 : (const void *)E.d_pos32);
-    if (E.n_aa_tiles)
-        ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top,
-                                                                         E.d_partAA, E.part_stride, E.nch_aa);
+    if (E.n_aa_tiles) {
+        if constexpr (sizeof(T) == 4)
+            ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
+                E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa);
+        else
+            ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(
+                E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa);
+    }
     if (E.n_ab_tiles)
         ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
                                                          E.d_partBA);
@@ -402,7 +514,7 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     cudaEventCreate(&b);
     auto launch = [&]() {
         if (which == 0 && E.n_aa_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_aa<float><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
+            if (fp32) ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
             else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
         } else if (which == 1 && E.n_ab_tiles) {
             if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
