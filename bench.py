@@ -219,7 +219,7 @@ def run_b200(args):
         ms = e0.elapsed_time(e1)
         lat.append(ms)
         t_total += ms
-        iters.append(list(r.iters))
+        iters.append(list(r.iters) + [r.lanczos_iters])
         reasons.append(r.reason)
     barrier()
     xs, _ = b.state()
@@ -280,7 +280,7 @@ def run_b200(args):
                           "l2": "flushed (256 MB write) before every timed step",
                           "parallelism": f"replicas x{world}"},
                "latency_ms": {"p50": lat_sorted[len(lat) // 2], "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
-               "minres_iters": iters, "minres_reason": reasons, "e2e_minres_iters": e2e_iters,
+               "minres_iters": iters, "minres_iters_note": "per step: max MINRES iterations of the 5 solves, then the Lanczos subspace size", "minres_reason": reasons, "e2e_minres_iters": e2e_iters,
                "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * 3 * b.ntot,
                        "d2h_bytes_per_step": 8 * 3 * b.ntot},
                "gpu_launches": launches, "roofline": roof, "clocks": clocks, "state_finite": finite}

@@ -127,6 +127,8 @@ typedef struct ps_step_inputs {
 typedef struct ps_step_result {
     int32_t iters[5];   /* max over replicas, per solve */
     int32_t reason;     /* worst KSP reason over the five solves */
+    int32_t lanczos_iters;  /* Lanczos subspace size of the noise (max over replicas) */
+    int32_t lanczos_nneg;   /* negative projected eigenvalues floored (sum over replicas) */
 } ps_step_result;
 
 typedef struct ps_ctx ps_ctx;

@@ -66,7 +66,8 @@ class PsStepInputs(C.Structure):
 
 
 class PsStepResult(C.Structure):
-    _fields_ = [("iters", C.c_int32 * 5), ("reason", C.c_int32)]
+    _fields_ = [("iters", C.c_int32 * 5), ("reason", C.c_int32), ("lanczos_iters", C.c_int32),
+                ("lanczos_nneg", C.c_int32)]
 
 
 def declared_symbols(header: str = HEADER) -> list[str]:

@@ -327,7 +327,8 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
             const double *w1 = E.d_W[(k + 0) % 3];   // w_{k-3}
             const double *w2 = E.d_W[(k + 1) % 3];   // w_{k-2}
             // A v_k = (1/beta_k) A z_k: the operator applies the per-replica scale
-            apply_operator(E, 0, E.d_z, Av, E.d_sinv, E.precision == PS_PREC_MIXED, st);
+            apply_operator(E, 0, E.d_z, Av, E.d_sinv, E.precision == PS_PREC_MIXED, st, &E.d_mr[0].done,
+                           (int)sizeof(MinresScal));
             ::ps_launch_count++, k_mr_alpha<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_z, E.d_v, Av, rkm1, wnew, w1, w2, x, E.d_mr, k);
             ::ps_launch_count++, k_mr_beta<<<T.nblk, RB_THREADS, 0, st>>>(T, Av, rk, E.d_D, E.d_z, E.d_mr, opt.maxit, E.d_nactive,
                                                     E.d_sinv);
@@ -612,7 +613,8 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     std::vector<LzScal> hl(E.R);
     int j = 0;
     for (j = 0; j < kmax; j++) {
-        apply_operator(E, 1, V + (long)j * ldv, q, nullptr, E.precision == PS_PREC_MIXED, st);
+        apply_operator(E, 1, V + (long)j * ldv, q, nullptr, E.precision == PS_PREC_MIXED, st, &lz[0].done,
+                       (int)sizeof(LzScal));
         for (int pass = 0; pass < 2; pass++) {
             ::ps_launch_count++, k_lz_dots<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h);
             ::ps_launch_count++, k_lz_sub<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h, alpha, pass == 0);

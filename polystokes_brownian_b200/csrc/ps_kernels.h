@@ -115,7 +115,10 @@ struct Engine {
 };
 
 // rpy.cu
-void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st);
+// done: optional per-replica int flags (base pointer + byte stride); replicas
+// whose flag is nonzero are skipped by every kernel of the apply
+void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st,
+                    const void *done = nullptr, int done_stride = 0);
 int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cudaStream_t st);
 int fma_peak(int fp64, double *tflops, cudaStream_t st);
 // stage.cu

@@ -42,8 +42,9 @@ template <class T>
 __global__ void __launch_bounds__(RPY_THREADS, 4)
 k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
-         long part_stride, int nchunk)
+         long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
 {
+    if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     // FP32: positions are split hi + lo (both float) so that pair separations
     // keep FP64-level accuracy: d = (hi_i - hi_j) + (lo_i - lo_j).
     typedef typename V4<T>::t P4;
@@ -140,8 +141,9 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __global__ void __launch_bounds__(AAF_THREADS)
 k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const float4 *__restrict__ pos,
             const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
-            long part_stride, int nchunk)
+            long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
 {
+    if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     __shared__ float4 sA[128];   // hi x, y, z, chain
     __shared__ float4 sB[128];   // lo x, y, z, u0
     __shared__ float2 sC[128];   // u1, u2
@@ -227,8 +229,9 @@ template <class T>
 __global__ void __launch_bounds__(RPY_THREADS)
 k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, const double *__restrict__ tab,
-         double *__restrict__ part_m, double *__restrict__ part_ba)
+         double *__restrict__ part_m, double *__restrict__ part_ba, const char *__restrict__ done, int done_stride)
 {
+    if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     typedef typename V4<T>::t P4;
     constexpr bool F32 = sizeof(T) == 4;
     __shared__ T red[RPY_THREADS / 32][12];
@@ -328,8 +331,9 @@ template <class T>
 __global__ void __launch_bounds__(RPY_THREADS)
 k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
-         long part_stride, int nchunk)
+         long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
 {
+    if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     typedef typename V4<T>::t P4;
     constexpr bool F32 = sizeof(T) == 4;
     constexpr int CT = 64;
@@ -411,11 +415,12 @@ __global__ void k_combine(const Seg *__restrict__ segs, const int *__restrict__ 
                           const double *__restrict__ partAA, int nchAA, const double *__restrict__ partAB,
                           const double *__restrict__ partBB, int nchBB, const double *__restrict__ partBA,
                           const double *__restrict__ delta, const double *__restrict__ lub_y,
-                          long part_stride, double *__restrict__ y)
+                          long part_stride, double *__restrict__ y, const char *__restrict__ done, int done_stride)
 {
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= total) return;
     int r = find_rep(offs, R, k);
+    if (done && *(const int *)(done + (long)r * done_stride)) return;   // converged replica: skip
     const Seg &sg = segs[r];
     int i = (int)(k - offs[r]);
     const int xo = mode == 0 ? sg.vec_off : sg.top_off;
@@ -464,30 +469,32 @@ __global__ void k_combine(const Seg *__restrict__ segs, const int *__restrict__ 
 // ---------------------------------------------------------------------------
 // host launchers
 template <class T>
-void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st)
+void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const char *done, int dstride)
 {
     const typename V4<T>::t *pos = (const typename V4<T>::t *)(sizeof(T) == 8 ? (const void *)E.d_pos64 : (const void *)E.d_pos32);
     if (E.n_aa_tiles) {
         if constexpr (sizeof(T) == 4)
             ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
-                E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa);
+                E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
         else
             ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(
-                E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa);
+                E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
     }
     if (E.n_ab_tiles)
         ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
-                                                         E.d_partBA);
+                                                         E.d_partBA, done, dstride);
     if (E.n_bb_tiles)
         ::ps_launch_count++, k_rpy_bb<T><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, pos, E.d_pos32lo, u, in_top,
-                                                                         E.d_partBB, E.part_stride, E.nch_bb);
+                                                                         E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
 }
 
-void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st)
+void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st,
+                    const void *done, int done_stride)
 {
     int in_top = mode == 1;
-    if (fp32) launch_pairs<float>(E, x, in_top, st);
-    else launch_pairs<double>(E, x, in_top, st);
+    const char *dn = (const char *)done;
+    if (fp32) launch_pairs<float>(E, x, in_top, st, dn, done_stride);
+    else launch_pairs<double>(E, x, in_top, st, dn, done_stride);
     const double *lub_y = nullptr;
     if (mode == 0 && E.any_lub) {
         lub_apply(E, x, E.d_luby, st);
@@ -498,7 +505,7 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
     int thr = 256;
     ::ps_launch_count++, k_combine<<<(unsigned)((total + thr - 1) / thr), thr, 0, st>>>(
         E.d_segs, offs, E.R, total, mode, x, scale, E.d_partAA, E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
-        E.d_partBA, E.d_delta, lub_y, E.part_stride, y);
+        E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
 }
 
 
@@ -514,14 +521,14 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     cudaEventCreate(&b);
     auto launch = [&]() {
         if (which == 0 && E.n_aa_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
-            else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa);
+            if (fp32) ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+            else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
         } else if (which == 1 && E.n_ab_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
-            else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA);
+            if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
+            else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
         } else if (which == 2 && E.n_bb_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_bb<float><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb);
-            else ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb);
+            if (fp32) ::ps_launch_count++, k_rpy_bb<float><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
+            else ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
         } else if (which == 3) {
             apply_operator(E, 1, u, E.d_tmp_top2, nullptr, fp32, st);
         }

@@ -267,7 +267,7 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
 {
     const int thr = 256;
     int rc;
-    if (res) { for (int k = 0; k < 5; k++) res->iters[k] = 0; res->reason = 1000; }
+    if (res) { for (int k = 0; k < 5; k++) res->iters[k] = 0; res->reason = 1000; res->lanczos_iters = 0; res->lanczos_nneg = 0; }
     ::ps_launch_count++, k_time<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_segs, E.d_time);
     PS_CK(cudaMemcpyAsync(E.d_xn, E.d_x, sizeof(double) * 3 * E.ntot, cudaMemcpyDeviceToDevice, st));
     // predictor stage at x_n
@@ -286,7 +286,9 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
             wr = E.d_wr;
         }
         ps_sqrt_opts so = {in && in->sqrt_kmax > 0 ? in->sqrt_kmax : 40, in && in->sqrt_tol > 0 ? in->sqrt_tol : 1e-6};
-        if ((rc = slip_noise(E, fb, E.d_Wn, &so, nullptr, st))) return rc;
+        ps_sqrt_result sr = {0, 0};
+        if ((rc = slip_noise(E, fb, E.d_Wn, &so, &sr, st))) return rc;
+        if (res) { res->lanczos_iters = sr.iters_max; res->lanczos_nneg = sr.nneg; }
         ::ps_launch_count++, k_add_noise<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
         ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
