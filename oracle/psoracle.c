@@ -1018,13 +1018,12 @@ static void lub_noise(const or_sim *s, const double *z, double scale, double *yb
     int np = or_lub_pairs(s, NULL, NULL, 0);
     int *pi = (int *)malloc(sizeof(int) * (np + 1)), *pj = (int *)malloc(sizeof(int) * (np + 1));
     or_lub_pairs(s, pi, pj, np);
-    double R[144], Q[144], lam[12], w[12]; int dof[12]; long off = 0;
+    double R[144], w[12]; int dof[12];
     for (int k = 0; k < np; k++) {
+        /* 12 normals per pair (monomer pairs use the first 6) */
         int nd = lub_block(s, pi[k], pj[k], R, dof);
-        or_sqrtm_eig(R, nd, z + off, w);
-        (void)Q; (void)lam;
+        or_sqrtm_eig(R, nd, z + 12L * k, w);
         for (int a = 0; a < nd; a++) ybot[dof[a]] += scale * w[a];
-        off += nd;
     }
     free(pi); free(pj);
 }

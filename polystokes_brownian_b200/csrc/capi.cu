@@ -56,7 +56,7 @@ static void free_engine(Engine &E)
                     E.d_tab, E.d_stale, E.d_aa_last, E.d_delta, E.d_schurQ, E.d_schurL, E.d_schur_reps, E.d_ss_reps,
                     E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_cell, E.d_cell_start, E.d_cell_sorted,
                     E.d_cell_count, E.d_cellgeo, E.d_cell_offs, E.d_nbr_ptr, E.d_nbr, E.d_nbr_count, E.d_lubtab,
-                    E.d_luby, E.d_lub_diag, E.d_lub_ptr, E.d_lub_nbr, E.d_D, E.d_z, E.d_v, E.d_xw, E.d_Rr[0],
+                    E.d_luby, E.d_lub_diag, E.d_lub_ptr, E.d_lub_nbr, E.d_tmp_vel, E.d_tmp_vel2, E.d_zlub, E.d_D, E.d_z, E.d_v, E.d_xw, E.d_Rr[0],
                     E.d_Rr[1], E.d_Rr[2], E.d_W[0], E.d_W[1], E.d_W[2], E.d_mr, E.d_sinv, E.d_nactive,
                     E.d_rhs, E.d_X, E.d_Xd, E.d_Xdet, E.d_Wn, E.d_vdn, E.d_vdc, E.d_vb, E.d_up, E.d_ud,
                     E.d_drift, E.d_sb, E.d_fext, E.d_fb, E.d_wr, E.d_tmp_top, E.d_tmp_top2, E.d_lzV, E.d_lzT,
@@ -92,10 +92,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
             ps::set_error("Npoly * Nmono_per_chain != Nm for replica " + std::to_string(r));
             return PS_ERR_ARG;
         }
-        if (d.lub_on) {
-            ps::set_error("lubrication is not available in this build");
-            return PS_ERR_UNSUPPORTED;
-        }
+        if (d.lub_on) E.any_lub = true;
         Seg s;
         memset(&s, 0, sizeof s);
         s.Nm = d.Nm; s.Nc = d.Nc; s.Np = d.Nm + d.Nc;
@@ -284,6 +281,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_cell_sorted, sizeof(int) * bead);
     TRY_ALLOC(E.d_cellgeo, sizeof(double) * 20 * R);
     TRY_ALLOC(E.d_nbr_ptr, sizeof(int) * (bead + 1));
+    TRY_ALLOC(E.d_lub_ptr, sizeof(int) * (bead + 1));
     TRY_ALLOC(E.d_nbr_count, sizeof(int) * (bead + 1));
     E.nbr_cap = 16 * bead + 1024;
     TRY_ALLOC(E.d_nbr, sizeof(int) * E.nbr_cap);
@@ -307,7 +305,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_fb, sizeof(double) * top);
     TRY_ALLOC(E.d_tmp_top, sizeof(double) * top);
     TRY_ALLOC(E.d_tmp_top2, sizeof(double) * top);
-    double **velbufs[] = {&E.d_vdn, &E.d_vdc, &E.d_vb, &E.d_up, &E.d_ud, &E.d_drift, &E.d_sb, &E.d_fext, &E.d_wr};
+    double **velbufs[] = {&E.d_vdn, &E.d_vdc, &E.d_vb, &E.d_up, &E.d_ud, &E.d_drift, &E.d_sb, &E.d_fext, &E.d_wr,
+                          &E.d_luby, &E.d_lub_diag, &E.d_tmp_vel, &E.d_tmp_vel2};
     for (double **p : velbufs) TRY_ALLOC(*p, sizeof(double) * vel);
     // Lanczos
     if (E.any_mmhi) {
@@ -364,9 +363,20 @@ int ps_ctx_offsets(const ps_ctx *ctx, int32_t rep, int64_t *o)
 
 int ps_set_lub_table(ps_ctx *ctx, const double *tab, int32_t nrow, int32_t ncol)
 {
-    (void)ctx; (void)tab; (void)nrow; (void)ncol;
-    ps::set_error("lubrication is not available in this build");
-    return PS_ERR_UNSUPPORTED;
+    // rows of r2babc.dat: r/a then X11A X12A Y11A Y12A Y11B Y12B X11C X12C Y11C Y12C
+    if (!ctx || !tab || nrow < 2 || ncol < 11) { ps::set_error("ps_set_lub_table: need >= 2 rows of 11 columns"); return PS_ERR_ARG; }
+    for (int i = 1; i < nrow; i++)
+        if (!(tab[i * ncol] > tab[(i - 1) * ncol])) { ps::set_error("ps_set_lub_table: r must increase"); return PS_ERR_ARG; }
+    Engine &E = ctx->E;
+    std::vector<double> t((size_t)nrow * 11);
+    for (int i = 0; i < nrow; i++)
+        for (int c = 0; c < 11; c++) t[(size_t)i * 11 + c] = tab[(size_t)i * ncol + c];
+    if (E.d_lubtab) cudaFree(E.d_lubtab);
+    E.d_lubtab = nullptr;
+    int rc = upload(E.d_lubtab, t);
+    if (rc) return rc;
+    E.lub_nrow = nrow;
+    return PS_OK;
 }
 
 int ps_set_seed(ps_ctx *ctx, uint64_t seed)
@@ -428,6 +438,7 @@ int ps_build_pairs(ps_ctx *ctx, void *stream)
 int ps_pair_list(ps_ctx *ctx, int32_t which, int32_t *pi, int32_t *pj, int64_t maxp, int64_t *count, void *stream)
 {
     if (!ctx || which < 0 || which > 2) return PS_ERR_ARG;
+    if (which == 2 && !ctx->E.any_lub) { ps::set_error("no replica has lubrication on"); return PS_ERR_STATE; }
     return ps::pair_list(ctx->E, which, pi, pj, maxp, count, S(stream));
 }
 

@@ -73,7 +73,7 @@ __device__ __forceinline__ bool in_list(const Seg &s, const double *__restrict__
         double rc = (double)s.rcut[0];
         return d2 < rc * rc && d2 != 0.0 && ref_adjacent(gref, x, b, j);
     }
-    // which == 2
+    // which == 2 or 3 (lubrication)
     if (mi != mk) return false;
     double a = mi ? s.beta : 1.0;
     double dr = sqrt(d2);
@@ -106,16 +106,19 @@ __device__ __forceinline__ void partners(const Seg &s, int r, long b, const doub
                     long cc = cell_off[r] + q[0] + (long)nc[0] * (q[1] + (long)nc[1] * q[2]);
                     for (int k = cstart[cc]; k < cstart[cc + 1]; k++) {
                         long j = csorted[k];
-                        if (j > b && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
+                        bool take = (which == 3) ? (j != b) : (j > b);
+                        if (take && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
                     }
                 }
     }
-    if (which != 1) {
-        // colloid partners (all colloids follow all monomers)
-        int c0 = i < s.Nm ? 0 : i - s.Nm + 1;
+    if (which != 1 && !(which >= 2 && i < s.Nm)) {
+        // colloid partners (all colloids follow all monomers); lubrication pairs
+        // are equal-radius, so monomers have no colloid partners there
+        int c0 = (which == 3) ? 0 : (i < s.Nm ? 0 : i - s.Nm + 1);
         for (int c = c0; c < s.Nc; c++) {
             long j = (long)s.bead_off + s.Nm + c;
-            if (j > b && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
+            bool take = (which == 3) ? (j != b) : (j > b);
+            if (take && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
         }
     }
 }

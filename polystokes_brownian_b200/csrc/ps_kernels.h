@@ -86,7 +86,8 @@ struct Engine {
 
     // lubrication
     double *d_lubtab = nullptr; int lub_nrow = 0;
-    double *d_luby = nullptr, *d_lub_diag = nullptr;
+    double *d_luby = nullptr, *d_lub_diag = nullptr, *d_tmp_vel = nullptr, *d_tmp_vel2 = nullptr;
+    double *d_zlub = nullptr; long zlub_cap = 0;
     int *d_lub_ptr = nullptr, *d_lub_nbr = nullptr; long lub_cap = 0; long lub_npairs = 0;
 
     // Krylov workspace
@@ -121,8 +122,12 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
                     const void *done = nullptr, int done_stride = 0);
 int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cudaStream_t st);
 int fma_peak(int fp64, double *tflops, cudaStream_t st);
-// stage.cu
+// lub.cu
 void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st);
+int lub_build(Engine &E, cudaStream_t st);
+int lub_diag(Engine &E, cudaStream_t st);
+int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st);
+// stage.cu
 int stage_pack(Engine &E, cudaStream_t st);
 int stage_pairs(Engine &E, cudaStream_t st);
 int stage_rhs(Engine &E, int drift, const double *fext, double *rhs, cudaStream_t st);

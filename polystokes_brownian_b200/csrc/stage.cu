@@ -470,7 +470,12 @@ int stage_pairs(Engine &E, cudaStream_t st)
 {
     int rc = stage_pack(E, st);
     if (rc) return rc;
-    if (E.need_cells) return stage_cells(E, st, E.d_cell_offs, E.ncells);
+    if (E.need_cells && (rc = stage_cells(E, st, E.d_cell_offs, E.ncells))) return rc;
+    if (E.any_lub) {
+        if (!E.d_lubtab) { set_error("lubrication requested but no table set (ps_set_lub_table)"); return PS_ERR_STATE; }
+        if ((rc = lub_build(E, st))) return rc;
+        if ((rc = lub_diag(E, st))) return rc;
+    }
     return PS_OK;
 }
 
@@ -727,13 +732,6 @@ int diag_saddle(Engine &E, double *d, cudaStream_t st)
     return PS_OK;
 }
 
-// ---------------------------------------------------------------------------
-// lubrication: not in the first engine build
-void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st)
-{
-    (void)x_saddle;
-    cudaMemsetAsync(y_vel, 0, sizeof(double) * E.nvel, st);
-}
 
 int pair_list(Engine &E, int which, int32_t *pi, int32_t *pj, int64_t maxp, int64_t *count, cudaStream_t st);
 

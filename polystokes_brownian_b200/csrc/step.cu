@@ -290,6 +290,21 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         if ((rc = slip_noise(E, fb, E.d_Wn, &so, &sr, st))) return rc;
         if (res) { res->lanczos_iters = sr.iters_max; res->lanczos_nneg = sr.nneg; }
         ::ps_launch_count++, k_add_noise<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
+        if (E.any_lub && E.lub_npairs > 0) {
+            // Brownian lubrication force: 12 normals per canonical pair
+            const double *zl = in ? in->zlub : nullptr;
+            if (!zl) {
+                long nz = 12 * E.lub_npairs;
+                if (nz > E.zlub_cap) {
+                    cudaFree(E.d_zlub);
+                    E.zlub_cap = nz * 3 / 2 + 1024;
+                    PS_CK(cudaMalloc(&E.d_zlub, sizeof(double) * E.zlub_cap));
+                }
+                ::ps_launch_count++, k_normals<<<nb(nz, thr), thr, 0, st>>>(nz, E.seed ^ 0x5bd1e995ull, 2 * E.step_counter + 1, E.d_zlub);
+                zl = E.d_zlub;
+            }
+            if ((rc = lub_noise(E, zl, E.d_rhs, st))) return rc;
+        }
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
         ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
         ::ps_launch_count++, k_sub<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_up, E.d_vdn, E.d_vb);
@@ -297,14 +312,14 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         PS_CK(cudaMemcpyAsync(E.d_fext, wr, sizeof(double) * E.nvel, cudaMemcpyDeviceToDevice, st));
         long n3 = 3 * E.ntot;
         ::ps_launch_count++, k_probe<<<nb(n3, thr), thr, 0, st>>>(n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, 1.0);
-        if ((rc = stage_pack(E, st))) return rc;
+        if ((rc = E.any_lub ? stage_pairs(E, st) : stage_pack(E, st))) return rc;
         if ((rc = stage_assemble(E, st))) return rc;
         if ((rc = stage_rhs(E, 1, E.d_fext, E.d_rhs, st))) return rc;
         if ((rc = solve(E, E.d_rhs, E.d_Xd, 0, in, res, 2, st))) return rc;
         ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xd, E.d_drift, 0);
         PS_CK(cudaMemcpyAsync(E.d_X, E.d_Xd, sizeof(double) * E.nvec, cudaMemcpyDeviceToDevice, st));  // keep S(+)
         ::ps_launch_count++, k_probe<<<nb(n3, thr), thr, 0, st>>>(n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, -2.0);
-        if ((rc = stage_pack(E, st))) return rc;
+        if ((rc = E.any_lub ? stage_pairs(E, st) : stage_pack(E, st))) return rc;
         if ((rc = stage_assemble(E, st))) return rc;
         if ((rc = stage_rhs(E, 1, E.d_fext, E.d_rhs, st))) return rc;
         if ((rc = solve(E, E.d_rhs, E.d_Xd, 1, in, res, 3, st))) return rc;

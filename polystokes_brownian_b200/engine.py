@@ -36,7 +36,8 @@ def make_desc(params: dict) -> _capi.PsDesc:
 class Batch:
     """A batch of independent systems advanced by the B200 engine."""
 
-    def __init__(self, systems: list[System], precision: int = _capi.PS_PREC_FP64, device: str = "cuda:0"):
+    def __init__(self, systems: list[System], precision: int = _capi.PS_PREC_FP64, device: str = "cuda:0",
+                 lub_table: np.ndarray | None = None):
         self.systems = systems
         self.R = len(systems)
         self.device = torch.device(device)
@@ -54,6 +55,11 @@ class Batch:
             o = (C.c_int64 * 4)()
             lib().ps_ctx_offsets(self.h, r, o)
             self.off.append(dict(bead=int(o[0]), vec=int(o[1]), top=int(o[2]), vel=int(o[3])))
+        if any(s.params.get("lub_on") for s in systems):
+            from .lubdat import load_table
+            tab = np.ascontiguousarray(load_table() if lub_table is None else lub_table, dtype=np.float64)
+            check(lib().ps_set_lub_table(self.h, tab.ctypes.data_as(C.c_void_p), tab.shape[0], tab.shape[1]),
+                  "ps_set_lub_table")
         x = np.concatenate([np.ascontiguousarray(s.x, dtype=np.float64).ravel() for s in systems])
         self.set_state(torch.from_numpy(x).to(self.device))
 
@@ -145,9 +151,10 @@ class Batch:
         return w, r
 
     def step(self, fb: torch.Tensor | None = None, wrfd: torch.Tensor | None = None, rtol: float = 1e-8,
-             maxit: int = 10000, sqrt_kmax: int = 0, sqrt_tol: float = 0.0, solver: int = 0):
+             maxit: int = 10000, sqrt_kmax: int = 0, sqrt_tol: float = 0.0, solver: int = 0,
+             zlub: torch.Tensor | None = None):
         inp = _capi.PsStepInputs(None if fb is None else fb.data_ptr(), None if wrfd is None else wrfd.data_ptr(),
-                                 None, rtol, maxit, sqrt_kmax, sqrt_tol, solver)
+                                 None if zlub is None else zlub.data_ptr(), rtol, maxit, sqrt_kmax, sqrt_tol, solver)
         res = _capi.PsStepResult()
         check(lib().ps_step(self.h, C.byref(inp), C.byref(res), self.stream), "ps_step")
         return res

@@ -54,6 +54,10 @@ def lubdat():
     for name in ("r2babc", "r2babcd", "r2bgh", "r2bghd", "r2bm"):
         tabs[name] = np.loadtxt(os.path.join(REF, "lubdat", name + ".dat"))
     np.savez_compressed(os.path.join(OUT, "lubdat.npz"), **tabs)
+    # the table the lubrication path consumes, shipped with the package
+    pkg = os.path.join(OUT, "..", "..", "polystokes_brownian_b200", "data")
+    os.makedirs(pkg, exist_ok=True)
+    np.save(os.path.join(pkg, "lubdat_r2babc.npy"), tabs["r2babc"])
 
 
 if __name__ == "__main__":
