@@ -84,6 +84,7 @@ typedef struct ps_desc {
     int32_t lub_on;     /* near-field lubrication (not in the reference) */
     double lub_gap;     /* lubricated pairs: gap < lub_gap * radius */
     int32_t aa_mode;    /* PS_AA_REFERENCE | PS_AA_RPY: monomer-monomer scalars */
+    int32_t lub_bonded; /* nonzero: bonded chain neighbours are lubricated too (default 0: skipped) */
 } ps_desc;
 
 typedef struct ps_ksp_opts {

@@ -937,6 +937,8 @@ int or_lub_pairs(const or_sim *s, int *pi, int *pj, int maxp)
         for (int j = i + 1; j < Np; j++) {
             int mi = i < Nm, mj = j < Nm;
             if (mi != mj) continue;
+            /* bonded chain neighbours (init.cpp:205-321 topology) only with lub_bonded */
+            if (mi && !s->p.lub_bonded && i / s->p.Nmono_per_chain == j / s->p.Nmono_per_chain && j == i + 1) continue;
             double a = mi ? s->p.beta : 1.0;
             double dx = s->x[3 * i] - s->x[3 * j], dy = s->x[3 * i + 1] - s->x[3 * j + 1], dz = s->x[3 * i + 2] - s->x[3 * j + 2];
             min_image(s, &dx, &dy, &dz);

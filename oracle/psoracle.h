@@ -57,6 +57,7 @@ typedef struct or_params {
     double lub_gap;         /* pairs with gap < lub_gap * a get a resistance block */
     int    noise_lanczos;   /* mm_HI noise: 0 exact eigen square root, 1 Lanczos (kmax 40, tol 1e-6) */
     int    aa_mode;         /* OR_AA_REFERENCE or OR_AA_RPY */
+    int    lub_bonded;      /* nonzero: bonded chain neighbours are lubricated too */
 } or_params;
 
 typedef struct or_sim or_sim;

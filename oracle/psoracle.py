@@ -34,6 +34,7 @@ class OrParams(C.Structure):
         ("t0", C.c_double), ("restart", C.c_int), ("ab_mode", C.c_int),
         ("hs_kpref", C.c_double), ("hs_kmode", C.c_int), ("lanczos_nc", C.c_int),
         ("lub_on", C.c_int), ("lub_gap", C.c_double), ("noise_lanczos", C.c_int), ("aa_mode", C.c_int),
+        ("lub_bonded", C.c_int),
     ]
 
 
@@ -109,7 +110,8 @@ def default_params(**kw) -> OrParams:
              r0=1.0, Lmax=10.0, tau=1000.0, dt=1e-3, mm_HI=1, chain_HI=0, fene=0, tether=0,
              mono_ev=0, record_forces=1, box_on=0, ktrap=0.0, tstart=0.0, trun=0.0,
              weaken_trap=-1.0, t0=0.0, restart=0, ab_mode=AB_REFERENCE, hs_kpref=1.0,
-             hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5, noise_lanczos=0, aa_mode=0)
+             hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5, noise_lanczos=0, aa_mode=0,
+             lub_bonded=0)
     box = kw.pop("box", None)
     d.update({k: v for k, v in kw.items() if k in d})
     for k, v in d.items():

@@ -37,7 +37,7 @@ class PsDesc(C.Structure):
         ("ktrap", C.c_double), ("tstart", C.c_double), ("trun", C.c_double), ("weaken_trap", C.c_double),
         ("t0", C.c_double), ("restart", C.c_int32), ("ab_mode", C.c_int32),
         ("hs_kpref", C.c_double), ("hs_kmode", C.c_int32), ("lanczos_nc", C.c_int32),
-        ("lub_on", C.c_int32), ("lub_gap", C.c_double), ("aa_mode", C.c_int32),
+        ("lub_on", C.c_int32), ("lub_gap", C.c_double), ("aa_mode", C.c_int32), ("lub_bonded", C.c_int32),
     ]
 
 

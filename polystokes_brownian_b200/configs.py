@@ -37,7 +37,7 @@ DEFAULTS = dict(Nm=0, Nc=0, Npoly=0, Nmono_per_chain=1, beta=1.0, kT=1.0, epsilo
                 r0=1.0, Lmax=10.0, tau=1000.0, dt=1e-3, mm_HI=1, chain_HI=0, fene=0, tether=0,
                 mono_ev=0, record_forces=1, box_on=0, ktrap=0.0, tstart=0.0, trun=0.0, weaken_trap=-1.0,
                 t0=0.0, restart=0, ab_mode=0, hs_kpref=1.0, hs_kmode=0, lanczos_nc=64, lub_on=0, lub_gap=0.5,
-                aa_mode=0)
+                aa_mode=0, lub_bonded=0)
 
 
 def make_params(**kw) -> dict:

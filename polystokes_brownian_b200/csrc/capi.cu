@@ -60,12 +60,14 @@ static void free_engine(Engine &E)
                     E.d_Rr[1], E.d_Rr[2], E.d_W[0], E.d_W[1], E.d_W[2], E.d_mr, E.d_sinv, E.d_nactive,
                     E.d_rhs, E.d_X, E.d_Xd, E.d_Xdet, E.d_Wn, E.d_vdn, E.d_vdc, E.d_vb, E.d_up, E.d_ud,
                     E.d_drift, E.d_sb, E.d_fext, E.d_fb, E.d_wr, E.d_tmp_top, E.d_tmp_top2, E.d_lzV, E.d_lzT,
-                    E.d_lzw, E.d_lzq, E.d_lzs};
+                    E.d_lzw, E.d_lzq, E.d_lzs, E.d_ssinv, E.d_pcg, E.d_pV, E.d_pr, E.d_pz, E.d_pp, E.d_ps,
+                    E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
     ps::free_red_table(E.red);
     ps::free_red_table(E.red_top);
+    ps::free_red_table(E.red_vel);
 }
 
 static int build(Engine &E, const ps_desc *descs, int R, int precision)
@@ -74,7 +76,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     E.precision = precision;
     E.desc.assign(descs, descs + R);
     E.segs.resize(R);
-    long bead = 0, coll = 0, vec = 0, top = 0, vel = 0, schur = 0, ba = 0, cells = 0;
+    long bead = 0, coll = 0, vec = 0, top = 0, vel = 0, schur = 0, ba = 0, cells = 0, ssinv = 0;
     std::vector<int> bead_offs(R + 1), vec_offs(R + 1), top_offs(R + 1), vel_offs(R + 1);
     std::vector<long> cell_offs(R + 1);
     std::vector<Tile> aa, ab, bb;
@@ -115,6 +117,9 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         s.sig[0] = (float)(2. * d.beta); s.sig[1] = (float)(1. + d.beta); s.sig[2] = 2.0f;
         for (int k = 0; k < 3; k++) s.rcut[k] = (float)(pref * (double)s.sig[k]);
         s.lub_gap = d.lub_gap;
+        s.lub_bonded = d.lub_bonded;
+        s.nper = d.Nmono_per_chain > 0 ? d.Nmono_per_chain : 1;
+        s.ss_off = -1;
         if (d.aa_mode == PS_AA_RPY) {
             double b = d.beta, b2 = b * b;
             const double c[8] = {1.5, -b2, 0.75, 0.5 * b2, 1.0 / b, -0.1875 / b2, 1.0 / b, -0.28125 / b2};
@@ -131,7 +136,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         }
         if (s.shell_schur) { s.schur_off = (int)schur; schur += (long)s.nc11 * s.nc11; schur_reps.push_back(r); }
         if (d.Nc > 0) {
-            if (s.nc5 <= 64) ss_reps.push_back(r);
+            if (s.nc5 <= 64) { ss_reps.push_back(r); s.ss_off = (int)ssinv; ssinv += (long)s.nc5 * s.nc5; }
             else ss_polish++;
         }
         // tiles
@@ -294,8 +299,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_sinv, sizeof(double) * R);
     TRY_ALLOC(E.d_nactive, sizeof(int));
     PS_CK(cudaMallocHost(&E.h_nactive, sizeof(int)));
-    if ((rc = ps::build_red_table(E, E.red, false))) return rc;
-    if ((rc = ps::build_red_table(E, E.red_top, true))) return rc;
+    if ((rc = ps::build_red_table(E, E.red, 0))) return rc;
+    if ((rc = ps::build_red_table(E, E.red_top, 1))) return rc;
     // step workspace
     TRY_ALLOC(E.d_rhs, sizeof(double) * vec);
     TRY_ALLOC(E.d_X, sizeof(double) * vec);
@@ -308,6 +313,17 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     double **velbufs[] = {&E.d_vdn, &E.d_vdc, &E.d_vb, &E.d_up, &E.d_ud, &E.d_drift, &E.d_sb, &E.d_fext, &E.d_wr,
                           &E.d_luby, &E.d_lub_diag, &E.d_tmp_vel, &E.d_tmp_vel2};
     for (double **p : velbufs) TRY_ALLOC(*p, sizeof(double) * vel);
+    // lubricated structured solve
+    if (E.any_lub) {
+        E.n_ssinv = ssinv;
+        TRY_ALLOC(E.d_ssinv, sizeof(double) * std::max<long>(ssinv, 1));
+        TRY_ALLOC(E.d_pcg, sizeof(ps::PcgScal) * R);
+        double **pv[] = {&E.d_pV, &E.d_pr, &E.d_pz, &E.d_pp, &E.d_ps, &E.d_pAp, &E.d_pg};
+        for (double **p : pv) TRY_ALLOC(*p, sizeof(double) * vel);
+        double **pt[] = {&E.d_pu, &E.d_py, &E.d_pu2, &E.d_py2};
+        for (double **p : pt) TRY_ALLOC(*p, sizeof(double) * top);
+        if ((rc = ps::build_red_table(E, E.red_vel, 2))) return rc;
+    }
     // Lanczos
     if (E.any_mmhi) {
         const int KM = 64;

@@ -293,6 +293,14 @@ void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st
         y_vel, nullptr);
 }
 
+void lub_apply_vel(Engine &E, const double *u_vel, double *y_vel, cudaStream_t st)
+{
+    int thr = 128;
+    ::ps_launch_count++, k_lub_apply<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
+        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, u_vel, 0,
+        y_vel, nullptr);
+}
+
 int lub_diag(Engine &E, cudaStream_t st)
 {
     int thr = 128;

@@ -75,6 +75,7 @@ __device__ __forceinline__ bool in_list(const Seg &s, const double *__restrict__
     }
     // which == 2 or 3 (lubrication)
     if (mi != mk) return false;
+    if (mi && !s.lub_bonded && i / s.nper == k / s.nper && (k - i == 1 || i - k == 1)) return false;
     double a = mi ? s.beta : 1.0;
     double dr = sqrt(d2);
     return dr - 2 * a < s.lub_gap * a;

@@ -38,6 +38,9 @@ struct Seg {
     double hs_k;       // HS spring constant kpref/dt (or kpref/(dt beta))
     float sig[3], rverl[3], rcut[3];
     double lub_gap;
+    int lub_bonded;    // lubricate bonded chain neighbours too
+    int nper;          // monomers per chain
+    int ss_off;        // offset of the inverse stresslet block (nc5^2 doubles), -1 if none
     // monomer-monomer scalars as x = c0/r + c1/r^3, y = c2/r + c3/r^3 (r > 2 beta)
     // and x = c4 + c5 r, y = c6 + c7 r (r <= 2 beta), for the selected aa_mode
     float aa_c[8];

@@ -29,6 +29,12 @@ struct RedTable {
     double *d_part = nullptr;    // nblk x 4 partial sums
 };
 
+// Per-replica scalars of the lubricated resistance-form PCG.
+struct PcgScal {
+    double rz, alpha, beta, tol, err;
+    int it, done, reason, pad;
+};
+
 struct Engine {
     int R = 0;
     int precision = PS_PREC_FP64;
@@ -93,6 +99,13 @@ struct Engine {
     // Krylov workspace
     RedTable red;                    // over saddle vectors
     RedTable red_top;                // over mobility vectors
+    RedTable red_vel;                // over velocity vectors (lubricated PCG)
+    // lubricated structured solve: inverse stresslet blocks, PCG state (velocity layout)
+    double *d_ssinv = nullptr; long n_ssinv = 0;
+    PcgScal *d_pcg = nullptr;
+    double *d_pV = nullptr, *d_pr = nullptr, *d_pz = nullptr, *d_pp = nullptr, *d_ps = nullptr, *d_pAp = nullptr,
+           *d_pg = nullptr;
+    double *d_pu = nullptr, *d_py = nullptr, *d_pu2 = nullptr, *d_py2 = nullptr;   // mobility layout
     double *d_D = nullptr, *d_z = nullptr, *d_v = nullptr, *d_xw = nullptr;
     double *d_Rr[3] = {nullptr, nullptr, nullptr}, *d_W[3] = {nullptr, nullptr, nullptr};
     MinresScal *d_mr = nullptr;
@@ -117,13 +130,16 @@ struct Engine {
 
 // rpy.cu
 // done: optional per-replica int flags (base pointer + byte stride); replicas
-// whose flag is nonzero are skipped by every kernel of the apply
+// whose flag is nonzero are skipped by every kernel of the apply.
+// skip_aa: leave out the monomer-monomer pairs -- exact for every colloid row,
+// and for the monomer rows when the monomer inputs are zero.
 void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st,
-                    const void *done = nullptr, int done_stride = 0);
+                    const void *done = nullptr, int done_stride = 0, bool skip_aa = false);
 int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cudaStream_t st);
 int fma_peak(int fp64, double *tflops, cudaStream_t st);
 // lub.cu
 void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st);
+void lub_apply_vel(Engine &E, const double *u_vel, double *y_vel, cudaStream_t st);
 int lub_build(Engine &E, cudaStream_t st);
 int lub_diag(Engine &E, cudaStream_t st);
 int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st);
@@ -143,7 +159,7 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
 int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
                      cudaStream_t st);
 int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
-int build_red_table(Engine &E, RedTable &T, bool top);
+int build_red_table(Engine &E, RedTable &T, int layout);   // 0 saddle, 1 top, 2 velocity
 void free_red_table(RedTable &T);
 void seg_dot(Engine &E, RedTable &T, const double *a, const double *b, double *out_per_rep, cudaStream_t st);
 

@@ -469,10 +469,10 @@ __global__ void k_combine(const Seg *__restrict__ segs, const int *__restrict__ 
 // ---------------------------------------------------------------------------
 // host launchers
 template <class T>
-void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const char *done, int dstride)
+void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const char *done, int dstride, bool skip_aa)
 {
     const typename V4<T>::t *pos = (const typename V4<T>::t *)(sizeof(T) == 8 ? (const void *)E.d_pos64 : (const void *)E.d_pos32);
-    if (E.n_aa_tiles) {
+    if (E.n_aa_tiles && !skip_aa) {
         if constexpr (sizeof(T) == 4)
             ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
                 E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
@@ -489,12 +489,12 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
 }
 
 void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st,
-                    const void *done, int done_stride)
+                    const void *done, int done_stride, bool skip_aa)
 {
     int in_top = mode == 1;
     const char *dn = (const char *)done;
-    if (fp32) launch_pairs<float>(E, x, in_top, st, dn, done_stride);
-    else launch_pairs<double>(E, x, in_top, st, dn, done_stride);
+    if (fp32) launch_pairs<float>(E, x, in_top, st, dn, done_stride, skip_aa);
+    else launch_pairs<double>(E, x, in_top, st, dn, done_stride, skip_aa);
     const double *lub_y = nullptr;
     if (mode == 0 && E.any_lub) {
         lub_apply(E, x, E.d_luby, st);
@@ -504,7 +504,7 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
     const int *offs = mode == 0 ? E.d_vec_offs : E.d_top_offs;
     int thr = 256;
     ::ps_launch_count++, k_combine<<<(unsigned)((total + thr - 1) / thr), thr, 0, st>>>(
-        E.d_segs, offs, E.R, total, mode, x, scale, E.d_partAA, E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
+        E.d_segs, offs, E.R, total, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
         E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
 }
 
