@@ -141,6 +141,22 @@ int ps_ctx_sizes(const ps_ctx *ctx, int64_t *out8); /* ntot_beads, nvec, ntop, n
 int ps_ctx_offsets(const ps_ctx *ctx, int32_t rep, int64_t *out4); /* bead, vec, top, vel offsets */
 int ps_set_lub_table(ps_ctx *ctx, const double *host_tab, int32_t nrow, int32_t ncol);
 int ps_set_seed(ps_ctx *ctx, uint64_t seed);
+/* Per-replica noise streams (no reference counterpart; the reference draws from
+ * one std::mt19937_64 per process, Stokes.h:111-112).  Device draws of replica r
+ * at its step k use Philox keyed by seeds[r], subsequence = the DOF's index
+ * within the replica, offset by k: a replica's noise does not depend on the
+ * other replicas of the batch.  ps_set_seed(ctx, s) sets seeds[r] =
+ * splitmix64(s + r) and all step counters to 0.  steps may be NULL (unchanged). */
+int ps_set_replica_seeds(ps_ctx *ctx, const uint64_t *host_seeds, const uint64_t *host_steps);
+int ps_get_replica_steps(ps_ctx *ctx, uint64_t *host_steps);
+/* Per-replica auxiliary state: time (R), trap constant ktrap (R; weaken_trap
+ * changes it, rhs.cpp:46-100), trap centres xpos0 (3 Nc per replica, colloid
+ * order).  Host or device pointers; NULL members are skipped.  With
+ * ps_get_state/ps_set_state and ps_get_replica_steps/ps_set_replica_seeds this
+ * moves a trajectory between contexts (continuous batching) or restarts it;
+ * the reference restarts from its own files instead (Stokes.cpp:19-34). */
+int ps_get_aux(ps_ctx *ctx, double *time, double *ktrap, double *xpos0, void *stream);
+int ps_set_aux(ps_ctx *ctx, const double *time, const double *ktrap, const double *xpos0, void *stream);
 const char *ps_last_error(void);
 
 /* state --------------------------------------------------------------------- */

@@ -97,6 +97,10 @@ def lib():
     L.ps_ctx_offsets.argtypes = [vp, C.c_int32, I64P]
     L.ps_set_lub_table.argtypes = [vp, P, C.c_int32, C.c_int32]
     L.ps_set_seed.argtypes = [vp, C.c_uint64]
+    L.ps_set_replica_seeds.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.ps_get_replica_steps.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.ps_get_aux.argtypes = [vp, P, P, P, vp]
+    L.ps_set_aux.argtypes = [vp, P, P, P, vp]
     L.ps_set_state.argtypes = [vp, P, P, vp]
     L.ps_get_state.argtypes = [vp, P, P, vp]
     L.ps_set_time.argtypes = [vp, C.c_double]

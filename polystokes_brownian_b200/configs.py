@@ -180,8 +180,12 @@ def brush(nchain: int = 128, nper: int = 32, seed: int = 0, dt: float = 1e-4, pa
     return System("brush", params, np.vstack([xm, np.zeros((1, 3))]))
 
 
-def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0, dt: float = 1e-4, pair_mode: int = 1) -> System:
+def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0, dt: float = 1e-4, pair_mode: int = 1,
+                    lub: bool = False, lub_gap: float = 0.5) -> System:
     """One batched-ensemble replica: harmonic chains + 0..2 trapped probes.
+
+    lub: near-field lubrication for equal-radius pairs with gap < lub_gap * a;
+    bonded chain neighbours (held at contact by their springs) are not lubricated.
 
     pair_mode 1 (default) uses the RPY monomer-monomer and monomer-colloid
     scalars; with the reference's own scalars (pair_mode 0) the grand mobility is
@@ -217,7 +221,7 @@ def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0, dt: float = 1e-4, pair
     params = make_params(Nm=Nm, Nc=nprobe, Npoly=npoly, Nmono_per_chain=L, beta=beta, kT=1.0,
                          kbond=900.0, r0=step, Lmax=10 * step, dt=dt, mm_HI=1, chain_HI=0, fene=0,
                          ktrap=4500.0 if nprobe else 0.0, tstart=0.0, trun=1e9, aa_mode=pair_mode,
-                         ab_mode=pair_mode)
+                         ab_mode=pair_mode, lub_on=int(lub), lub_gap=lub_gap)
     return System(f"ensemble_{N}", params, x)
 
 

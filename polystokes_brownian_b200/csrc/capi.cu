@@ -61,7 +61,7 @@ static void free_engine(Engine &E)
                     E.d_rhs, E.d_X, E.d_Xd, E.d_Xdet, E.d_Wn, E.d_vdn, E.d_vdc, E.d_vb, E.d_up, E.d_ud,
                     E.d_drift, E.d_sb, E.d_fext, E.d_fb, E.d_wr, E.d_tmp_top, E.d_tmp_top2, E.d_lzV, E.d_lzT,
                     E.d_lzw, E.d_lzq, E.d_lzs, E.d_ssinv, E.d_pcg, E.d_pV, E.d_pr, E.d_pz, E.d_pp, E.d_ps,
-                    E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2};
+                    E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2, E.d_rseed, E.d_rstep};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -120,6 +120,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         s.lub_bonded = d.lub_bonded;
         s.nper = d.Nmono_per_chain > 0 ? d.Nmono_per_chain : 1;
         s.ss_off = -1;
+        s.nch_aa = std::max(1, (d.Nm + AA_CHUNK_COLS - 1) / AA_CHUNK_COLS);
+        s.nch_bb = std::max(1, (d.Nc + BB_CHUNK_COLS - 1) / BB_CHUNK_COLS);
         if (d.aa_mode == PS_AA_RPY) {
             double b = d.beta, b2 = b * b;
             const double c[8] = {1.5, -b2, 0.75, 0.5 * b2, 1.0 / b, -0.1875 / b2, 1.0 / b, -0.28125 / b2};
@@ -179,12 +181,9 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     std::stable_sort(aa.begin(), aa.end(), by_cost);
     std::stable_sort(bb.begin(), bb.end(), by_cost);
     E.n_aa_tiles = (int)aa.size(); E.n_ab_tiles = (int)ab.size(); E.n_bb_tiles = (int)bb.size();
-    // column chunks so that the pair kernels fill the 148 SMs (>= 4 CTAs per SM)
-    const int target = 148 * 4;
-    int maxNm = 0, maxNc = 0;
-    for (auto &s : E.segs) { maxNm = std::max(maxNm, s.Nm); maxNc = std::max(maxNc, s.Nc); }
-    E.nch_aa = E.n_aa_tiles ? std::max(1, std::min((target + E.n_aa_tiles - 1) / E.n_aa_tiles, std::max(1, maxNm / 128))) : 1;
-    E.nch_bb = E.n_bb_tiles ? std::max(1, std::min((target + E.n_bb_tiles - 1) / E.n_bb_tiles, std::max(1, maxNc / 64))) : 1;
+    // grid extent in chunks: the largest per-replica chunk count
+    E.nch_aa = 1; E.nch_bb = 1;
+    for (auto &s : E.segs) { E.nch_aa = std::max(E.nch_aa, s.nch_aa); E.nch_bb = std::max(E.nch_bb, s.nch_bb); }
     E.part_stride = top;
     int rc;
     if ((rc = upload(E.d_segs, E.segs))) return rc;
@@ -263,6 +262,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     if ((rc = upload(E.d_time, tinit))) return rc;
     if ((rc = upload(E.d_stale, stale))) return rc;
     TRY_ALLOC(E.d_tab, sizeof(double) * 9 * R);
+    TRY_ALLOC(E.d_rseed, sizeof(uint64_t) * R);
+    TRY_ALLOC(E.d_rstep, sizeof(uint64_t) * R);
     // state
     TRY_ALLOC(E.d_x, sizeof(double) * 3 * bead);
     TRY_ALLOC(E.d_xn, sizeof(double) * 3 * bead);
@@ -347,6 +348,7 @@ int ps_ctx_create(const ps_desc *descs, int32_t nrep, int32_t precision, ps_ctx 
     if (cudaGetDevice(&dev) != cudaSuccess) { ps::set_error("no CUDA device"); return PS_ERR_CUDA; }
     ps_ctx *c = new ps_ctx();
     int rc = build(c->E, descs, nrep, precision);
+    if (!rc) rc = ps_set_seed(c, c->E.seed);   // per-replica streams from the default seed
     if (rc) { free_engine(c->E); delete c; return rc; }
     *out = c;
     return PS_OK;
@@ -395,11 +397,66 @@ int ps_set_lub_table(ps_ctx *ctx, const double *tab, int32_t nrow, int32_t ncol)
     return PS_OK;
 }
 
+static uint64_t splitmix64(uint64_t z)
+{
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
 int ps_set_seed(ps_ctx *ctx, uint64_t seed)
 {
     if (!ctx) return PS_ERR_ARG;
-    ctx->E.seed = seed;
-    ctx->E.step_counter = 0;
+    Engine &E = ctx->E;
+    E.seed = seed;
+    E.step_counter = 0;
+    std::vector<uint64_t> sd(E.R), zero(E.R, 0);
+    for (int r = 0; r < E.R; r++) sd[r] = splitmix64(seed + (uint64_t)r);
+    PS_CK(cudaMemcpy(E.d_rseed, sd.data(), sizeof(uint64_t) * E.R, cudaMemcpyHostToDevice));
+    PS_CK(cudaMemcpy(E.d_rstep, zero.data(), sizeof(uint64_t) * E.R, cudaMemcpyHostToDevice));
+    return PS_OK;
+}
+
+int ps_set_replica_seeds(ps_ctx *ctx, const uint64_t *seeds, const uint64_t *steps)
+{
+    if (!ctx || !seeds) return PS_ERR_ARG;
+    Engine &E = ctx->E;
+    PS_CK(cudaDeviceSynchronize());
+    PS_CK(cudaMemcpy(E.d_rseed, seeds, sizeof(uint64_t) * E.R, cudaMemcpyHostToDevice));
+    if (steps) PS_CK(cudaMemcpy(E.d_rstep, steps, sizeof(uint64_t) * E.R, cudaMemcpyHostToDevice));
+    return PS_OK;
+}
+
+int ps_get_aux(ps_ctx *ctx, double *time, double *ktrap, double *xpos0, void *stream)
+{
+    if (!ctx) return PS_ERR_ARG;
+    Engine &E = ctx->E;
+    cudaStream_t st = S(stream);
+    if (time) PS_CK(cudaMemcpyAsync(time, E.d_time, sizeof(double) * E.R, cudaMemcpyDefault, st));
+    if (ktrap) PS_CK(cudaMemcpyAsync(ktrap, E.d_ktrap, sizeof(double) * E.R, cudaMemcpyDefault, st));
+    if (xpos0 && E.ncoll) PS_CK(cudaMemcpyAsync(xpos0, E.d_xpos0, sizeof(double) * 3 * E.ncoll, cudaMemcpyDefault, st));
+    PS_CK(cudaStreamSynchronize(st));
+    return PS_OK;
+}
+
+int ps_set_aux(ps_ctx *ctx, const double *time, const double *ktrap, const double *xpos0, void *stream)
+{
+    if (!ctx) return PS_ERR_ARG;
+    Engine &E = ctx->E;
+    cudaStream_t st = S(stream);
+    if (time) PS_CK(cudaMemcpyAsync(E.d_time, time, sizeof(double) * E.R, cudaMemcpyDefault, st));
+    if (ktrap) PS_CK(cudaMemcpyAsync(E.d_ktrap, ktrap, sizeof(double) * E.R, cudaMemcpyDefault, st));
+    if (xpos0 && E.ncoll) PS_CK(cudaMemcpyAsync(E.d_xpos0, xpos0, sizeof(double) * 3 * E.ncoll, cudaMemcpyDefault, st));
+    PS_CK(cudaStreamSynchronize(st));
+    return PS_OK;
+}
+
+int ps_get_replica_steps(ps_ctx *ctx, uint64_t *steps)
+{
+    if (!ctx || !steps) return PS_ERR_ARG;
+    PS_CK(cudaDeviceSynchronize());
+    PS_CK(cudaMemcpy(steps, ctx->E.d_rstep, sizeof(uint64_t) * ctx->E.R, cudaMemcpyDeviceToHost));
     return PS_OK;
 }
 

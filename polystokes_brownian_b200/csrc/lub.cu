@@ -20,6 +20,7 @@
 // with B11 = Y11B eps.d, B12 = Y12B eps.d, B21 = -Y12B eps.d.
 // Compiled with --fmad=false (pair membership must round like the oracle).
 #include <cmath>
+#include <curand_kernel.h>
 #include <vector>
 #include "ps_internal.h"
 #include "ps_kernels.h"
@@ -194,13 +195,57 @@ __device__ void small_sqrt_apply(double *A, int n, const double *z, double *out)
     }
 }
 
-// Brownian lubrication force: per canonical pair (i < j, CSR order) p with
-// z_p (12 entries; monomer pairs use the first 6), w_p = R_p^{1/2} z_p is
-// scattered as scale * w_p into the constraint rows of rhs (atomic adds: the
-// noise sum is order-dependent only at the last bit).
+// 12x12 (or 6x6) pair block R_p in the canonical orientation d = (x_hi - x_lo)/r
+__device__ void lub_pair_block(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab, int nrow,
+                               long lo, long hi, bool mono, double *Rm)
+{
+    const double a = mono ? s.beta : 1.0, sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
+    double dx = x[3 * hi] - x[3 * lo], dy = x[3 * hi + 1] - x[3 * lo + 1], dz = x[3 * hi + 2] - x[3 * lo + 2];
+    mimg_l(s, dx, dy, dz);
+    double rr = sqrt(dx * dx + dy * dy + dz * dz);
+    double d[3] = {dx / rr, dy / rr, dz / rr};
+    double f[10];
+    lub_scalars(tab, nrow, rr / a, f);
+    const int nd = mono ? 6 : 12;
+    for (int k = 0; k < nd * nd; k++) Rm[k] = 0.0;
+    for (int p = 0; p < 3; p++)
+        for (int qq = 0; qq < 3; qq++) {
+            double dd = d[p] * d[qq], id = (p == qq) - dd;
+            double a11 = sa * (f[0] * dd + f[2] * id), a12 = sa * (f[1] * dd + f[3] * id);
+            Rm[(0 + p) * nd + 0 + qq] = a11; Rm[(3 + p) * nd + 3 + qq] = a11;
+            Rm[(0 + p) * nd + 3 + qq] = a12; Rm[(3 + p) * nd + 0 + qq] = a12;
+        }
+    if (mono) return;
+    for (int p = 0; p < 3; p++)
+        for (int qq = 0; qq < 3; qq++) {
+            int k3 = 3 - p - qq;
+            double ed = 0.0;
+            if (p != qq && k3 >= 0 && k3 < 3) ed = (((p - qq + 3) % 3) == 2 ? 1.0 : -1.0) * d[k3];
+            double b11 = sb * f[4] * ed, b12 = sb * f[5] * ed, b21 = -b12, b22 = -b11;
+            Rm[(6 + p) * nd + 0 + qq] = b11; Rm[(6 + p) * nd + 3 + qq] = b12;
+            Rm[(9 + p) * nd + 0 + qq] = b21; Rm[(9 + p) * nd + 3 + qq] = b22;
+            Rm[(0 + qq) * nd + 6 + p] = b11; Rm[(3 + qq) * nd + 6 + p] = b12;
+            Rm[(0 + qq) * nd + 9 + p] = b21; Rm[(3 + qq) * nd + 9 + p] = b22;
+            double dd = d[p] * d[qq], id = (p == qq) - dd;
+            double c11 = sc * (f[6] * dd + f[8] * id), c12 = sc * (f[7] * dd + f[9] * id);
+            Rm[(6 + p) * nd + 6 + qq] = c11; Rm[(9 + p) * nd + 9 + qq] = c11;
+            Rm[(6 + p) * nd + 9 + qq] = c12; Rm[(9 + p) * nd + 6 + qq] = c12;
+        }
+}
+
+// Brownian lubrication force, gathered per bead (no atomics: the sum over a
+// bead's pairs runs in ascending partner order, so the result is bit-exact and
+// independent of the rest of the batch).  Each canonical pair p = (lo < hi) with
+// index q in the canonical CSR list owns 12 normals z_p (monomer pairs use the
+// first 6): injected (z + 12 q) or drawn from the replica's Philox stream with
+// subsequence = q - (first canonical pair of the replica).  Both beads of a pair
+// compute w_p = R_p^{1/2} z_p identically and take their own rows;
+// rhs_bot += -sqrt(2 kT / dt) w.
 __global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                             const double *__restrict__ x, const double *__restrict__ tab, int nrow,
+                            const int *__restrict__ sptr, const int *__restrict__ snbr,
                             const int *__restrict__ cptr, const int *__restrict__ cnbr, const double *__restrict__ z,
+                            const uint64_t *__restrict__ rseed, const uint64_t *__restrict__ rstep,
                             double *__restrict__ rhs)
 {
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -209,59 +254,40 @@ __global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R,
     const Seg &s = segs[r];
     int i = (int)(b - s.bead_off);
     const bool mono = i < s.Nm;
-    const double a = mono ? s.beta : 1.0, sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
+    const int nd = mono ? 6 : 12;
     const double scale = -sqrt(2 * s.kT / s.dt);
-    for (int q = cptr[b]; q < cptr[b + 1]; q++) {
-        long j = cnbr[q];
-        int jl = (int)(j - s.bead_off);
-        double dx = x[3 * j] - x[3 * b], dy = x[3 * j + 1] - x[3 * b + 1], dz = x[3 * j + 2] - x[3 * b + 2];
-        mimg_l(s, dx, dy, dz);
-        double rr = sqrt(dx * dx + dy * dy + dz * dz);
-        double d[3] = {dx / rr, dy / rr, dz / rr};
-        double f[10];
-        lub_scalars(tab, nrow, rr / a, f);
-        int nd = mono ? 6 : 12;
-        double Rm[144];
-        for (int k = 0; k < nd * nd; k++) Rm[k] = 0.0;
-        for (int p = 0; p < 3; p++)
-            for (int qq = 0; qq < 3; qq++) {
-                double dd = d[p] * d[qq], id = (p == qq) - dd;
-                double a11 = sa * (f[0] * dd + f[2] * id), a12 = sa * (f[1] * dd + f[3] * id);
-                Rm[(0 + p) * nd + 0 + qq] = a11; Rm[(3 + p) * nd + 3 + qq] = a11;
-                Rm[(0 + p) * nd + 3 + qq] = a12; Rm[(3 + p) * nd + 0 + qq] = a12;
-            }
-        if (!mono) {
-            for (int p = 0; p < 3; p++)
-                for (int qq = 0; qq < 3; qq++) {
-                    int k3 = 3 - p - qq;
-                    double ed = 0.0;
-                    if (p != qq && k3 >= 0 && k3 < 3) ed = (((p - qq + 3) % 3) == 2 ? 1.0 : -1.0) * d[k3];
-                    double b11 = sb * f[4] * ed, b12 = sb * f[5] * ed, b21 = -b12, b22 = -b11;
-                    Rm[(6 + p) * nd + 0 + qq] = b11; Rm[(6 + p) * nd + 3 + qq] = b12;
-                    Rm[(9 + p) * nd + 0 + qq] = b21; Rm[(9 + p) * nd + 3 + qq] = b22;
-                    Rm[(0 + qq) * nd + 6 + p] = b11; Rm[(3 + qq) * nd + 6 + p] = b12;
-                    Rm[(0 + qq) * nd + 9 + p] = b21; Rm[(3 + qq) * nd + 9 + p] = b22;
-                    double dd = d[p] * d[qq], id = (p == qq) - dd;
-                    double c11 = sc * (f[6] * dd + f[8] * id), c12 = sc * (f[7] * dd + f[9] * id);
-                    Rm[(6 + p) * nd + 6 + qq] = c11; Rm[(9 + p) * nd + 9 + qq] = c11;
-                    Rm[(6 + p) * nd + 9 + qq] = c12; Rm[(9 + p) * nd + 6 + qq] = c12;
-                }
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = sptr[b]; t < sptr[b + 1]; t++) {
+        long j = snbr[t];
+        const bool low = b < j;
+        long lo = low ? b : j, hi = low ? j : b;
+        // canonical index of (lo, hi): binary search in lo's ascending list
+        int qa = cptr[lo], qb = cptr[lo + 1];
+        while (qb - qa > 1) {
+            int mid = (qa + qb) >> 1;
+            if (cnbr[mid] <= hi) qa = mid; else qb = mid;
         }
-        double w[12];
-        small_sqrt_apply(Rm, nd, z + 12L * q, w);
-        int tb, wb, tj, wj;
-        vel_dofs(s, i, tb, wb);
-        vel_dofs(s, jl, tj, wj);
-        long base = (long)s.vec_off + s.nm3nc11;
-        for (int k = 0; k < 3; k++) {
-            atomicAdd(&rhs[base + tb + k], scale * w[k]);
-            atomicAdd(&rhs[base + tj + k], scale * w[3 + k]);
-            if (!mono) {
-                atomicAdd(&rhs[base + wb + k], scale * w[6 + k]);
-                atomicAdd(&rhs[base + wj + k], scale * w[9 + k]);
-            }
+        const long q = qa;
+        double zp[12];
+        if (z) {
+            for (int k = 0; k < 12; k++) zp[k] = z[12 * q + k];
+        } else {
+            curandStatePhilox4_32_10_t stt;
+            curand_init(rseed[r], (unsigned long long)(q - cptr[s.bead_off]), (3ull * rstep[r] + 2) * 4ull, &stt);
+            for (int k = 0; k < 12; k++) zp[k] = curand_normal_double(&stt);
         }
+        double Rm[144], w[12];
+        lub_pair_block(s, x, tab, nrow, lo, hi, mono, Rm);
+        small_sqrt_apply(Rm, nd, zp, w);
+        const int o = low ? 0 : 3;
+        for (int k = 0; k < 3; k++) acc[k] += w[o + k];
+        if (!mono) for (int k = 0; k < 3; k++) acc[3 + k] += w[6 + o + k];
     }
+    int tb, wb;
+    vel_dofs(s, i, tb, wb);
+    long base = (long)s.vec_off + s.nm3nc11;
+    for (int k = 0; k < 3; k++) rhs[base + tb + k] += scale * acc[k];
+    if (!mono) for (int k = 0; k < 3; k++) rhs[base + wb + k] += scale * acc[3 + k];
 }
 
 // build the symmetric partner list (which 3) and the canonical i<j list (which 2)
@@ -317,7 +343,8 @@ int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st)
 {
     int thr = 64;
     ::ps_launch_count++, k_lub_noise<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_nbr_ptr, E.d_nbr, z, rhs);
+        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_nbr_ptr,
+        E.d_nbr, z, E.d_rseed, E.d_rstep, rhs);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

@@ -41,10 +41,15 @@ struct Seg {
     int lub_bonded;    // lubricate bonded chain neighbours too
     int nper;          // monomers per chain
     int ss_off;        // offset of the inverse stresslet block (nc5^2 doubles), -1 if none
+    int nch_aa, nch_bb; // column chunks of the far-field pair kernels (functions of Nm, Nc alone)
     // monomer-monomer scalars as x = c0/r + c1/r^3, y = c2/r + c3/r^3 (r > 2 beta)
     // and x = c4 + c5 r, y = c6 + c7 r (r <= 2 beta), for the selected aa_mode
     float aa_c[8];
 };
+
+// Column chunk widths of the far-field pair kernels.
+constexpr int AA_CHUNK_COLS = 256;
+constexpr int BB_CHUNK_COLS = 64;
 
 // Row tile of the far-field pair kernels.
 struct Tile { int rep; int row0; int nrow; int mtile; };

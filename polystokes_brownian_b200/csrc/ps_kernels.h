@@ -119,6 +119,7 @@ struct Engine {
     double *d_drift = nullptr, *d_sb = nullptr, *d_fext = nullptr, *d_fb = nullptr, *d_wr = nullptr;
     double *d_tmp_top = nullptr, *d_tmp_top2 = nullptr;
     uint64_t seed = 12345, step_counter = 0;
+    uint64_t *d_rseed = nullptr, *d_rstep = nullptr;   // per-replica Philox key and step counter
 
     // Lanczos workspace
     int lz_kmax = 0;

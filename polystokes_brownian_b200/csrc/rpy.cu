@@ -6,9 +6,10 @@
 // recomputed on the fly from the positions (O(N) memory); the O(N^2) loops are
 // thread-per-row with column tiles staged in shared memory, so every lane of a
 // warp reads the same column entry (a shared-memory broadcast).  Columns are
-// split into chunks across blockIdx.y when the batch has too few row tiles to
-// fill the 148 SMs; chunk partials are summed in fixed order by k_combine, so
-// results are deterministic and independent of the other replicas in a batch.
+// split into chunks across blockIdx.y (AA_CHUNK_COLS monomer or BB_CHUNK_COLS
+// colloid columns per chunk, so the chunking of a replica depends on its own
+// size only); chunk partials are summed in fixed order by k_combine, so results
+// are deterministic and bit-identical whatever else shares the batch.
 #include <algorithm>
 #include "ps_internal.h"
 #include "ps_kernels.h"
@@ -55,6 +56,8 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
     const int c = blockIdx.y;
+    nchunk = sg.nch_aa;               // per-replica chunk count: a function of Nm alone
+    if (c >= nchunk) return;
     const int Nm = sg.Nm;
     const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
     const int i = tl.row0 + threadIdx.x;
@@ -150,6 +153,8 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
     const int c = blockIdx.y;
+    nchunk = sg.nch_aa;               // per-replica chunk count: a function of Nm alone
+    if (c >= nchunk) return;
     const int Nm = sg.Nm;
     const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
     const int i0 = tl.row0 + threadIdx.x, i1 = i0 + AAF_THREADS;
@@ -343,6 +348,8 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
     const int c = blockIdx.y;
+    nchunk = sg.nch_bb;
+    if (c >= nchunk) return;
     const int Nc = sg.Nc, Nm = sg.Nm;
     const int j0 = (int)((long)Nc * c / nchunk), j1 = (int)((long)Nc * (c + 1) / nchunk);
     const int i = tl.row0 + threadIdx.x;
@@ -430,7 +437,7 @@ __global__ void k_combine(const Seg *__restrict__ segs, const int *__restrict__ 
         if (i < sg.nm3) {
             v = sg.beta_inv * x[xo + i];
             if (sg.mm_HI)
-                for (int c = 0; c < nchAA; c++) v += partAA[(long)c * part_stride + sg.top_off + i];
+                for (int c = 0; c < (nchAA ? sg.nch_aa : 0); c++) v += partAA[(long)c * part_stride + sg.top_off + i];
             if (sg.Nc > 0) v += partAB[sg.top_off + i];
         } else {
             int j = i - sg.nm3;          // colloid-local DOF in [0, nc11)
@@ -447,7 +454,7 @@ __global__ void k_combine(const Seg *__restrict__ segs, const int *__restrict__ 
             }
             v = self;
             if (sg.Nc >= 2)
-                for (int c = 0; c < nchBB; c++) v += partBB[(long)c * part_stride + sg.top_off + i];
+                for (int c = 0; c < sg.nch_bb; c++) v += partBB[(long)c * part_stride + sg.top_off + i];
             if (sg.Nm > 0)
                 for (int t = 0; t < sg.n_mtiles; t++) v += partBA[((long)sg.ba_off + (long)t * sg.Nc + cidx) * 11 + q];
             if (sg.shell_schur) {

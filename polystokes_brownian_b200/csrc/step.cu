@@ -82,12 +82,16 @@ int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps
 
 // ---------------------------------------------------------------------------
 // device RNG (Philox) for runs without injected noise
-__global__ void k_normals(long n, uint64_t seed, uint64_t stream_id, double *__restrict__ out)
+// element k of a layout (offs: per-replica offsets) draws from replica r's key
+// with subsequence = its index within the replica and offset (3 step + which)
+__global__ void k_normals(long n, const int *__restrict__ offs, int R, const uint64_t *__restrict__ rseed,
+                          const uint64_t *__restrict__ rstep, int which, double *__restrict__ out)
 {
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
+    int r = rep_lookup(offs, R, k);
     curandStatePhilox4_32_10_t stt;
-    curand_init(seed, (unsigned long long)k, stream_id * 4ull, &stt);
+    curand_init(rseed[r], (unsigned long long)(k - offs[r]), (3ull * rstep[r] + which) * 4ull, &stt);
     out[k] = curand_normal_double(&stt);
 }
 
@@ -235,6 +239,12 @@ __global__ void k_time(int R, const Seg *__restrict__ segs, double *__restrict__
     if (r < R) t[r] += segs[r].dt;
 }
 
+__global__ void k_step_count(int R, uint64_t *__restrict__ rstep)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < R) rstep[r]++;
+}
+
 static inline unsigned nb(long n, int thr) { return (unsigned)((n + thr - 1) / thr); }
 
 static int stage(Engine &E, double *rhs, cudaStream_t st)
@@ -278,11 +288,11 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         const double *fb = in ? in->fb : nullptr;
         const double *wr = in ? in->wrfd : nullptr;
         if (!fb) {
-            ::ps_launch_count++, k_normals<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.seed, 2 * E.step_counter, E.d_fb);
+            ::ps_launch_count++, k_normals<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_rseed, E.d_rstep, 0, E.d_fb);
             fb = E.d_fb;
         }
         if (!wr) {
-            ::ps_launch_count++, k_normals<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.seed, 2 * E.step_counter + 1, E.d_wr);
+            ::ps_launch_count++, k_normals<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_rseed, E.d_rstep, 1, E.d_wr);
             wr = E.d_wr;
         }
         ps_sqrt_opts so = {in && in->sqrt_kmax > 0 ? in->sqrt_kmax : 40, in && in->sqrt_tol > 0 ? in->sqrt_tol : 1e-6};
@@ -291,18 +301,9 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         if (res) { res->lanczos_iters = sr.iters_max; res->lanczos_nneg = sr.nneg; }
         ::ps_launch_count++, k_add_noise<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
         if (E.any_lub && E.lub_npairs > 0) {
-            // Brownian lubrication force: 12 normals per canonical pair
+            // Brownian lubrication force: 12 normals per canonical pair, injected
+            // or drawn inside the gather from the replica's Philox stream
             const double *zl = in ? in->zlub : nullptr;
-            if (!zl) {
-                long nz = 12 * E.lub_npairs;
-                if (nz > E.zlub_cap) {
-                    cudaFree(E.d_zlub);
-                    E.zlub_cap = nz * 3 / 2 + 1024;
-                    PS_CK(cudaMalloc(&E.d_zlub, sizeof(double) * E.zlub_cap));
-                }
-                ::ps_launch_count++, k_normals<<<nb(nz, thr), thr, 0, st>>>(nz, E.seed ^ 0x5bd1e995ull, 2 * E.step_counter + 1, E.d_zlub);
-                zl = E.d_zlub;
-            }
             if ((rc = lub_noise(E, zl, E.d_rhs, st))) return rc;
         }
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
@@ -344,6 +345,7 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         ::ps_launch_count++, k_step_rot<<<nb(E.ncoll, 128), 128, 0, st>>>(E.ncoll, E.d_segs, E.d_coll_rep, E.d_up, E.d_vdn, E.d_vdc, E.d_vb,
                                                      E.d_q);
     E.step_counter++;
+    ::ps_launch_count++, k_step_count<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_rstep);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

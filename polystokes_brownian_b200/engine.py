@@ -51,10 +51,12 @@ class Batch:
         lib().ps_ctx_sizes(self.h, sz)
         self.ntot, self.nvec, self.ntop, self.nvel, self.ncoll = [int(v) for v in sz[:5]]
         self.off = []
+        coll = 0
         for r in range(self.R):
             o = (C.c_int64 * 4)()
             lib().ps_ctx_offsets(self.h, r, o)
-            self.off.append(dict(bead=int(o[0]), vec=int(o[1]), top=int(o[2]), vel=int(o[3])))
+            self.off.append(dict(bead=int(o[0]), vec=int(o[1]), top=int(o[2]), vel=int(o[3]), coll=coll))
+            coll += systems[r].params["Nc"]
         if any(s.params.get("lub_on") for s in systems):
             from .lubdat import load_table
             tab = np.ascontiguousarray(load_table() if lub_table is None else lub_table, dtype=np.float64)
@@ -97,6 +99,25 @@ class Batch:
 
     def set_seed(self, seed: int):
         check(lib().ps_set_seed(self.h, int(seed)), "ps_set_seed")
+
+    def set_replica_seeds(self, seeds, steps=None):
+        sd = (C.c_uint64 * self.R)(*[int(v) for v in seeds])
+        stp = None if steps is None else (C.c_uint64 * self.R)(*[int(v) for v in steps])
+        check(lib().ps_set_replica_seeds(self.h, sd, stp), "ps_set_replica_seeds")
+
+    def replica_steps(self) -> list[int]:
+        out = (C.c_uint64 * self.R)()
+        check(lib().ps_get_replica_steps(self.h, out), "ps_get_replica_steps")
+        return list(out)
+
+    def aux(self):
+        """(time[R], ktrap[R], xpos0[3 ncoll]) as device tensors."""
+        t, k, xp = self.zeros(self.R), self.zeros(self.R), self.zeros(max(3 * self.ncoll, 1))
+        check(lib().ps_get_aux(self.h, _ptr(t), _ptr(k), _ptr(xp), self.stream), "ps_get_aux")
+        return t, k, xp[: 3 * self.ncoll]
+
+    def set_aux(self, time=None, ktrap=None, xpos0=None):
+        check(lib().ps_set_aux(self.h, _ptr(time), _ptr(ktrap), _ptr(xpos0), self.stream), "ps_set_aux")
 
     # stage -----------------------------------------------------------------
     def stage(self) -> torch.Tensor:
