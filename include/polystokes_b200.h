@@ -112,12 +112,13 @@ typedef struct ps_sqrt_result {
     int32_t nneg;       /* negative projected eigenvalues floored (sum over replicas) */
 } ps_sqrt_result;
 
-/* Optional injected noise for one step (device pointers, concatenated per
- * replica); NULL members are drawn on the device from the context's seed. */
+/* Optional injected noise for one step (device or host pointers, concatenated
+ * per replica; host arrays are copied in by the call); NULL members are drawn on
+ * the device from the replicas' Philox streams. */
 typedef struct ps_step_inputs {
     const double *fb;   /* nm3nc11 per replica: slip-velocity white noise (slip_vel.cpp:11-17) */
     const double *wrfd; /* nm3nc6 per replica: RFD displacement (drift.cpp:9-15) */
-    const double *zlub; /* 6 or 12 per lubricated pair, canonical pair order */
+    const double *zlub; /* 12 per lubricated pair (monomer pairs use 6), canonical pair order */
     double rtol;        /* MINRES rtol for the five solves */
     int32_t maxit;
     int32_t sqrt_kmax;  /* Lanczos subspace cap of the noise (0: 40) */
@@ -160,6 +161,8 @@ int ps_set_aux(ps_ctx *ctx, const double *time, const double *ktrap, const doubl
 const char *ps_last_error(void);
 
 /* state --------------------------------------------------------------------- */
+/* x (3 Np per replica), q (4 Nc per replica): device or host pointers; reads
+ * into host memory are complete when the call returns. */
 int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream);
 int ps_get_state(ps_ctx *ctx, double *x, double *q, void *stream);
 int ps_set_time(ps_ctx *ctx, double t);

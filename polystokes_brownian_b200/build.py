@@ -1,5 +1,7 @@
 """Build the B200 engine: every .cu under csrc/ -> one shared library
-polystokes_brownian_b200/_lib/libpsb200.so, compiled for sm_100a only.
+polystokes_brownian_b200/_lib/libpsb200.so, compiled for sm_100a only; then the
+host module csrc/host/polystokes_module.cpp (the reference's pybind11 module
+`PolyStokes`) -> polystokes_brownian_b200/_lib/PolyStokes<ext>, linked to it.
 
 Usage: python -m polystokes_brownian_b200.build [--force] [-j N]
 """
@@ -38,7 +40,7 @@ def _needs(obj, deps):
 
 def _compile(src):
     obj = os.path.join(BUILD, src[:-3] + ".o")
-    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
+    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     deps.append(os.path.join(HERE, "..", "include", "polystokes_b200.h"))
     if not _needs(obj, deps):
         return obj, ""
@@ -69,8 +71,29 @@ def build(force: bool = False, jobs: int = 8) -> str:
     return LIB
 
 
+def build_host(force: bool = False) -> str:
+    import sysconfig
+
+    import pybind11
+    src = os.path.join(CSRC, "host", "polystokes_module.cpp")
+    out = os.path.join(OUT, "PolyStokes" + sysconfig.get_config_var("EXT_SUFFIX"))
+    hdr = os.path.join(HERE, "..", "include", "polystokes_b200.h")
+    if not force and not _needs(out, [src, hdr, LIB]):
+        return out
+    cxx = shutil.which("g++") or "c++"
+    cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"],
+           "-I" + os.path.join(HERE, "..", "include"), src, "-o", out,
+           "-L" + OUT, "-lpsb200", "-Wl,-rpath,$ORIGIN"]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(f"host module build failed:\n{p.stdout}\n{p.stderr}")
+    return out
+
+
 if __name__ == "__main__":
     j = 8
     if "-j" in sys.argv:
         j = int(sys.argv[sys.argv.index("-j") + 1])
     print(build(force="--force" in sys.argv, jobs=j))
+    print(build_host(force="--force" in sys.argv))

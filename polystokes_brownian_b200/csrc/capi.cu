@@ -491,6 +491,7 @@ int ps_get_state(ps_ctx *ctx, double *x, double *q, void *stream)
     cudaStream_t st = S(stream);
     if (x) PS_CK(cudaMemcpyAsync(x, E.d_x, sizeof(double) * 3 * E.ntot, cudaMemcpyDefault, st));
     if (q && E.ncoll) PS_CK(cudaMemcpyAsync(q, E.d_q, sizeof(double) * 4 * E.ncoll, cudaMemcpyDefault, st));
+    if (ps::is_host_ptr(x) || ps::is_host_ptr(q)) PS_CK(cudaStreamSynchronize(st));   // host copies complete on return
     return PS_OK;
 }
 
@@ -579,6 +580,8 @@ int ps_step_outputs(ps_ctx *ctx, double *up, double *udiff, double *sb, double *
     if (udiff) PS_CK(cudaMemcpyAsync(udiff, E.d_ud, sizeof(double) * E.nvel, cudaMemcpyDefault, st));
     if (sb) PS_CK(cudaMemcpyAsync(sb, E.d_sb, sizeof(double) * E.nvel, cudaMemcpyDefault, st));
     if (fext) PS_CK(cudaMemcpyAsync(fext, E.d_fext, sizeof(double) * E.nvel, cudaMemcpyDefault, st));
+    if (ps::is_host_ptr(up) || ps::is_host_ptr(udiff) || ps::is_host_ptr(sb) || ps::is_host_ptr(fext))
+        PS_CK(cudaStreamSynchronize(st));
     return PS_OK;
 }
 

@@ -129,6 +129,10 @@ struct Engine {
     cudaStream_t internal = nullptr;
 };
 
+// true when p is host memory (pageable or pinned): the C-ABI accepts host
+// pointers for state and noise arguments and copies them itself
+bool is_host_ptr(const void *p);
+
 // rpy.cu
 // done: optional per-replica int flags (base pointer + byte stride); replicas
 // whose flag is nonzero are skipped by every kernel of the apply.

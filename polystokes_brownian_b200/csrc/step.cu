@@ -245,6 +245,14 @@ __global__ void k_step_count(int R, uint64_t *__restrict__ rstep)
     if (r < R) rstep[r]++;
 }
 
+bool is_host_ptr(const void *p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return true; }
+    return a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged;
+}
+
 static inline unsigned nb(long n, int thr) { return (unsigned)((n + thr - 1) / thr); }
 
 static int stage(Engine &E, double *rhs, cudaStream_t st)
@@ -287,6 +295,14 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
     if (E.any_kT) {
         const double *fb = in ? in->fb : nullptr;
         const double *wr = in ? in->wrfd : nullptr;
+        if (fb && is_host_ptr(fb)) {
+            PS_CK(cudaMemcpyAsync(E.d_fb, fb, sizeof(double) * E.ntop, cudaMemcpyHostToDevice, st));
+            fb = E.d_fb;
+        }
+        if (wr && is_host_ptr(wr)) {
+            PS_CK(cudaMemcpyAsync(E.d_wr, wr, sizeof(double) * E.nvel, cudaMemcpyHostToDevice, st));
+            wr = E.d_wr;
+        }
         if (!fb) {
             ::ps_launch_count++, k_normals<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_rseed, E.d_rstep, 0, E.d_fb);
             fb = E.d_fb;
@@ -304,6 +320,16 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
             // Brownian lubrication force: 12 normals per canonical pair, injected
             // or drawn inside the gather from the replica's Philox stream
             const double *zl = in ? in->zlub : nullptr;
+            if (zl && is_host_ptr(zl)) {
+                long nz = 12 * E.lub_npairs;
+                if (nz > E.zlub_cap) {
+                    cudaFree(E.d_zlub);
+                    E.zlub_cap = nz * 3 / 2 + 1024;
+                    PS_CK(cudaMalloc(&E.d_zlub, sizeof(double) * E.zlub_cap));
+                }
+                PS_CK(cudaMemcpyAsync(E.d_zlub, zl, sizeof(double) * nz, cudaMemcpyHostToDevice, st));
+                zl = E.d_zlub;
+            }
             if ((rc = lub_noise(E, zl, E.d_rhs, st))) return rc;
         }
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
