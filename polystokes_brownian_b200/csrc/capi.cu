@@ -61,13 +61,16 @@ static void free_engine(Engine &E)
                     E.d_rhs, E.d_X, E.d_Xd, E.d_Xdet, E.d_Wn, E.d_vdn, E.d_vdc, E.d_vb, E.d_up, E.d_ud,
                     E.d_drift, E.d_sb, E.d_fext, E.d_fb, E.d_wr, E.d_tmp_top, E.d_tmp_top2, E.d_lzV, E.d_lzT,
                     E.d_lzw, E.d_lzq, E.d_lzs, E.d_ssinv, E.d_pcg, E.d_pV, E.d_pr, E.d_pz, E.d_pp, E.d_ps,
-                    E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2, E.d_rseed, E.d_rstep};
+                    E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2, E.d_rseed, E.d_rstep,
+                    E.d_lubc_ptr, E.d_lubc_nbr, E.d_lub_pairs, E.d_pS, E.d_pP, E.d_py_[0], E.d_py_[1], E.d_py_[2],
+                    E.d_py_[3], E.d_py_[4], E.d_ppart};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
     ps::free_red_table(E.red);
     ps::free_red_table(E.red_top);
     ps::free_red_table(E.red_vel);
+    ps::free_red_table(E.red_bead);
 }
 
 static int build(Engine &E, const ps_desc *descs, int R, int precision)
@@ -288,6 +291,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_cellgeo, sizeof(double) * 20 * R);
     TRY_ALLOC(E.d_nbr_ptr, sizeof(int) * (bead + 1));
     TRY_ALLOC(E.d_lub_ptr, sizeof(int) * (bead + 1));
+    TRY_ALLOC(E.d_lubc_ptr, sizeof(int) * (bead + 1));
     TRY_ALLOC(E.d_nbr_count, sizeof(int) * (bead + 1));
     E.nbr_cap = 16 * bead + 1024;
     TRY_ALLOC(E.d_nbr, sizeof(int) * E.nbr_cap);
@@ -324,6 +328,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         double **pt[] = {&E.d_pu, &E.d_py, &E.d_pu2, &E.d_py2};
         for (double **p : pt) TRY_ALLOC(*p, sizeof(double) * top);
         if ((rc = ps::build_red_table(E, E.red_vel, 2))) return rc;
+        if ((rc = ps::build_red_table(E, E.red_bead, 3))) return rc;
     }
     // Lanczos
     if (E.any_mmhi) {

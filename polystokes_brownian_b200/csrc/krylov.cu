@@ -21,15 +21,15 @@
 
 namespace ps {
 
-// layout 0: saddle vectors, 1: mobility (top) vectors, 2: velocity vectors
+// layout 0: saddle vectors, 1: mobility (top) vectors, 2: velocity vectors, 3: beads
 int build_red_table(Engine &E, RedTable &T, int layout)
 {
     std::vector<RBlk> blk;
     std::vector<int> first(E.R), cnt(E.R);
     for (int r = 0; r < E.R; r++) {
         const Seg &s = E.segs[r];
-        int n = layout == 1 ? s.nm3nc11 : (layout == 2 ? s.nm3nc6 : s.n);
-        int off = layout == 1 ? s.top_off : (layout == 2 ? s.vel_off : s.vec_off);
+        int n = layout == 1 ? s.nm3nc11 : (layout == 2 ? s.nm3nc6 : (layout == 3 ? s.Np : s.n));
+        int off = layout == 1 ? s.top_off : (layout == 2 ? s.vel_off : (layout == 3 ? s.bead_off : s.vec_off));
         first[r] = (int)blk.size();
         int nb = (n + RB_SPAN - 1) / RB_SPAN;
         if (nb == 0) nb = 1;

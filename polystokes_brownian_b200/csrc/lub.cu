@@ -24,70 +24,11 @@
 #include <vector>
 #include "ps_internal.h"
 #include "ps_kernels.h"
+#include "lub_dev.cuh"
 
 namespace ps {
 
 int build_list(Engine &E, int which, long *npairs, cudaStream_t st);
-
-__device__ __forceinline__ int rep_of_b(const int *__restrict__ offs, int R, long k)
-{
-    int lo = 0, hi = R;
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (offs[mid] <= k) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ double lub_sing(int col, double xi)
-{
-    double l = log(xi);
-    switch (col) {
-    case 0: return 1.0 / (4.0 * xi) - (9.0 / 40.0) * l;
-    case 1: return -(1.0 / (4.0 * xi) - (9.0 / 40.0) * l);
-    case 2: return -(1.0 / 6.0) * l;
-    case 3: return (1.0 / 6.0) * l;
-    case 4: return (1.0 / 4.0) * l;
-    case 5: return -(1.0 / 4.0) * l;
-    case 8: return -(1.0 / 5.0) * l;
-    case 9: return -(1.0 / 20.0) * l;
-    default: return 0.0;
-    }
-}
-
-// ten scalar functions at rr = r / a
-__device__ void lub_scalars(const double *__restrict__ T, int nr, double rr, double f[10])
-{
-    double r0 = T[0], rl = T[(nr - 1) * 11];
-    if (rr >= rl) { for (int c = 0; c < 10; c++) f[c] = 0.0; return; }
-    if (rr <= r0) {
-        double xi = rr - 2.0;
-        if (xi < 1e-4) xi = 1e-4;
-        double xi0 = r0 - 2.0;
-        for (int c = 0; c < 10; c++) f[c] = T[1 + c] + lub_sing(c, xi) - lub_sing(c, xi0);
-        return;
-    }
-    int k = 0;
-    while (k + 1 < nr && T[(k + 1) * 11] <= rr) k++;
-    if (k >= nr - 1) k = nr - 2;
-    double ra = T[k * 11], rb = T[(k + 1) * 11], w = (rr - ra) / (rb - ra);
-    for (int c = 0; c < 10; c++) f[c] = (1 - w) * T[k * 11 + 1 + c] + w * T[(k + 1) * 11 + 1 + c];
-}
-
-__device__ __forceinline__ void mimg_l(const Seg &s, double &dx, double &dy, double &dz)
-{
-    if (!s.box_on) return;
-    dx -= s.L[0] * nearbyint(dx * (1.0 / s.L[0]));
-    dy -= s.L[1] * nearbyint(dy * (1.0 / s.L[1]));
-    dz -= s.L[2] * nearbyint(dz * (1.0 / s.L[2]));
-}
-
-// velocity-vector DOFs of bead b (local index i): translation, rotation (-1 for monomers)
-__device__ __forceinline__ void vel_dofs(const Seg &s, int i, int &t, int &w)
-{
-    if (i < s.Nm) { t = 3 * i; w = -1; }
-    else { int c = i - s.Nm; t = s.nm3 + 3 * c; w = s.nm3nc3 + 3 * c; }
-}
 
 // y_vel = R_lub u_vel, u read from the velocity block of a saddle vector
 // (u_off_kind 0) or from a velocity-layout vector (1); gather over the
@@ -153,86 +94,6 @@ __global__ void k_lub_apply(long ntot, const int *__restrict__ bead_offs, int R,
     }
 }
 
-// 12x12 (or 6x6) symmetric square root by cyclic Jacobi, negative eigenvalues floored at 0
-__device__ void small_sqrt_apply(double *A, int n, const double *z, double *out)
-{
-    double Q[144];
-    for (int k = 0; k < n * n; k++) Q[k] = (k / n == k % n) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 40; sweep++) {
-        double off = 0, tot = 0;
-        for (int p = 0; p < n; p++) for (int q = 0; q < n; q++) { double v = A[p * n + q] * A[p * n + q]; tot += v; if (p != q) off += v; }
-        if (off <= 1e-30 * tot || off == 0.0) break;
-        for (int p = 0; p < n - 1; p++)
-            for (int q = p + 1; q < n; q++) {
-                double apq = A[p * n + q];
-                if (fabs(apq) < 1e-300) continue;
-                double theta = (A[q * n + q] - A[p * n + p]) / (2 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-                double c = 1 / sqrt(t * t + 1), sn = t * c;
-                for (int k = 0; k < n; k++) {
-                    double akp = A[k * n + p], akq = A[k * n + q];
-                    A[k * n + p] = c * akp - sn * akq; A[k * n + q] = sn * akp + c * akq;
-                }
-                for (int k = 0; k < n; k++) {
-                    double apk = A[p * n + k], aqk = A[q * n + k];
-                    A[p * n + k] = c * apk - sn * aqk; A[q * n + k] = sn * apk + c * aqk;
-                    double qkp = Q[k * n + p], qkq = Q[k * n + q];
-                    Q[k * n + p] = c * qkp - sn * qkq; Q[k * n + q] = sn * qkp + c * qkq;
-                }
-            }
-    }
-    double t[12];
-    for (int jj = 0; jj < n; jj++) {
-        double acc = 0;
-        for (int ii = 0; ii < n; ii++) acc += Q[ii * n + jj] * z[ii];
-        double lam = A[jj * n + jj];
-        t[jj] = (lam > 0 ? sqrt(lam) : 0.0) * acc;
-    }
-    for (int ii = 0; ii < n; ii++) {
-        double acc = 0;
-        for (int jj = 0; jj < n; jj++) acc += Q[ii * n + jj] * t[jj];
-        out[ii] = acc;
-    }
-}
-
-// 12x12 (or 6x6) pair block R_p in the canonical orientation d = (x_hi - x_lo)/r
-__device__ void lub_pair_block(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab, int nrow,
-                               long lo, long hi, bool mono, double *Rm)
-{
-    const double a = mono ? s.beta : 1.0, sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
-    double dx = x[3 * hi] - x[3 * lo], dy = x[3 * hi + 1] - x[3 * lo + 1], dz = x[3 * hi + 2] - x[3 * lo + 2];
-    mimg_l(s, dx, dy, dz);
-    double rr = sqrt(dx * dx + dy * dy + dz * dz);
-    double d[3] = {dx / rr, dy / rr, dz / rr};
-    double f[10];
-    lub_scalars(tab, nrow, rr / a, f);
-    const int nd = mono ? 6 : 12;
-    for (int k = 0; k < nd * nd; k++) Rm[k] = 0.0;
-    for (int p = 0; p < 3; p++)
-        for (int qq = 0; qq < 3; qq++) {
-            double dd = d[p] * d[qq], id = (p == qq) - dd;
-            double a11 = sa * (f[0] * dd + f[2] * id), a12 = sa * (f[1] * dd + f[3] * id);
-            Rm[(0 + p) * nd + 0 + qq] = a11; Rm[(3 + p) * nd + 3 + qq] = a11;
-            Rm[(0 + p) * nd + 3 + qq] = a12; Rm[(3 + p) * nd + 0 + qq] = a12;
-        }
-    if (mono) return;
-    for (int p = 0; p < 3; p++)
-        for (int qq = 0; qq < 3; qq++) {
-            int k3 = 3 - p - qq;
-            double ed = 0.0;
-            if (p != qq && k3 >= 0 && k3 < 3) ed = (((p - qq + 3) % 3) == 2 ? 1.0 : -1.0) * d[k3];
-            double b11 = sb * f[4] * ed, b12 = sb * f[5] * ed, b21 = -b12, b22 = -b11;
-            Rm[(6 + p) * nd + 0 + qq] = b11; Rm[(6 + p) * nd + 3 + qq] = b12;
-            Rm[(9 + p) * nd + 0 + qq] = b21; Rm[(9 + p) * nd + 3 + qq] = b22;
-            Rm[(0 + qq) * nd + 6 + p] = b11; Rm[(3 + qq) * nd + 6 + p] = b12;
-            Rm[(0 + qq) * nd + 9 + p] = b21; Rm[(3 + qq) * nd + 9 + p] = b22;
-            double dd = d[p] * d[qq], id = (p == qq) - dd;
-            double c11 = sc * (f[6] * dd + f[8] * id), c12 = sc * (f[7] * dd + f[9] * id);
-            Rm[(6 + p) * nd + 6 + qq] = c11; Rm[(9 + p) * nd + 9 + qq] = c11;
-            Rm[(6 + p) * nd + 9 + qq] = c12; Rm[(9 + p) * nd + 6 + qq] = c12;
-        }
-}
-
 // Brownian lubrication force, gathered per bead (no atomics: the sum over a
 // bead's pairs runs in ascending partner order, so the result is bit-exact and
 // independent of the rest of the batch).  Each canonical pair p = (lo < hi) with
@@ -263,10 +124,12 @@ __global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R,
         long lo = low ? b : j, hi = low ? j : b;
         // canonical index of (lo, hi): binary search in lo's ascending list
         int qa = cptr[lo], qb = cptr[lo + 1];
+        const int qend = qb;
         while (qb - qa > 1) {
             int mid = (qa + qb) >> 1;
             if (cnbr[mid] <= hi) qa = mid; else qb = mid;
         }
+        if (qa >= qend || cnbr[qa] != hi) continue;    // not in the canonical list (lists disagree)
         const long q = qa;
         double zp[12];
         if (z) {
@@ -290,6 +153,13 @@ __global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R,
     if (!mono) for (int k = 0; k < 3; k++) rhs[base + wb + k] += scale * acc[3 + k];
 }
 
+__global__ void k_lub_pairs(long ntot, const int *__restrict__ ptr, const int *__restrict__ nbr, int2 *__restrict__ pairs)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    for (int q = ptr[b]; q < ptr[b + 1]; q++) pairs[q] = make_int2((int)b, nbr[q]);
+}
+
 // build the symmetric partner list (which 3) and the canonical i<j list (which 2)
 int lub_build(Engine &E, cudaStream_t st)
 {
@@ -304,11 +174,27 @@ int lub_build(Engine &E, cudaStream_t st)
     }
     PS_CK(cudaMemcpyAsync(E.d_lub_ptr, E.d_nbr_ptr, sizeof(int) * (E.ntot + 1), cudaMemcpyDeviceToDevice, st));
     if (np) PS_CK(cudaMemcpyAsync(E.d_lub_nbr, E.d_nbr, sizeof(int) * np, cudaMemcpyDeviceToDevice, st));
-    // canonical list stays in d_nbr_ptr / d_nbr
+    // canonical list (lo < hi, ascending), kept in its own buffers and as a flat pair array
     long nc = 0;
     rc = build_list(E, 2, &nc, st);
+    if (rc) return rc;
+    if (nc + 1 > E.lubc_cap) {
+        cudaFree(E.d_lubc_nbr);
+        cudaFree(E.d_lub_pairs);
+        E.lubc_cap = nc * 3 / 2 + 1024;
+        PS_CK(cudaMalloc(&E.d_lubc_nbr, sizeof(int) * E.lubc_cap));
+        PS_CK(cudaMalloc(&E.d_lub_pairs, sizeof(int2) * E.lubc_cap));
+    }
+    PS_CK(cudaMemcpyAsync(E.d_lubc_ptr, E.d_nbr_ptr, sizeof(int) * (E.ntot + 1), cudaMemcpyDeviceToDevice, st));
+    if (nc) {
+        PS_CK(cudaMemcpyAsync(E.d_lubc_nbr, E.d_nbr, sizeof(int) * nc, cudaMemcpyDeviceToDevice, st));
+        int thr = 128;
+        ::ps_launch_count++, k_lub_pairs<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_lubc_ptr,
+                                                                                           E.d_lubc_nbr, E.d_lub_pairs);
+    }
     E.lub_npairs = nc;
-    return rc;
+    PS_CK(cudaGetLastError());
+    return PS_OK;
 }
 
 void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st)
@@ -343,8 +229,8 @@ int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st)
 {
     int thr = 64;
     ::ps_launch_count++, k_lub_noise<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_nbr_ptr,
-        E.d_nbr, z, E.d_rseed, E.d_rstep, rhs);
+        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr,
+        E.d_lubc_nbr, z, E.d_rseed, E.d_rstep, rhs);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

@@ -95,6 +95,11 @@ struct Engine {
     double *d_luby = nullptr, *d_lub_diag = nullptr, *d_tmp_vel = nullptr, *d_tmp_vel2 = nullptr;
     double *d_zlub = nullptr; long zlub_cap = 0;
     int *d_lub_ptr = nullptr, *d_lub_nbr = nullptr; long lub_cap = 0; long lub_npairs = 0;
+    int *d_lubc_ptr = nullptr, *d_lubc_nbr = nullptr; int2 *d_lub_pairs = nullptr; long lubc_cap = 0;  // canonical
+    // pair-space lubricated solve: per pair K^{1/2} and preconditioner blocks (12x12), CG vectors (12 per pair)
+    double *d_pS = nullptr, *d_pP = nullptr, *d_py_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double *d_ppart = nullptr; long pair_cap = 0;
+    RedTable red_bead;               // over beads (pair-space sums by lower bead)
 
     // Krylov workspace
     RedTable red;                    // over saddle vectors
@@ -164,7 +169,7 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
 int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
                      cudaStream_t st);
 int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
-int build_red_table(Engine &E, RedTable &T, int layout);   // 0 saddle, 1 top, 2 velocity
+int build_red_table(Engine &E, RedTable &T, int layout);   // 0 saddle, 1 top, 2 velocity, 3 beads
 void free_red_table(RedTable &T);
 void seg_dot(Engine &E, RedTable &T, const double *a, const double *b, double *out_per_rep, cudaStream_t st);
 

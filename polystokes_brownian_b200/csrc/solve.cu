@@ -12,19 +12,12 @@
 // which costs two operator applies instead of a Krylov iteration.  The solution
 // is the same one MINRES converges to (it is the unique solution of the system).
 //
-// With lubrication the velocities solve the resistance form
-//     (R + Mr^{-1}) V = R g - b_bot,   V = U + g,
-//     Mr = M_tt - M_tS M_SS^{-1} M_St,  g = b_tt - M_tS M_SS^{-1} b_S,
-// by conjugate gradients preconditioned with the far-field mobility Mr, which
-// never needs Mr^{-1}: with p = Mr s tracked alongside, (R + Mr^{-1}) p = R p + s.
-// The preconditioned operator I + Mr R has its spectrum in [1, 1 + |Mr R|], so
-// the iteration count follows the stiffest lubricated gap, not the far field.
-// After k iterations the saddle residual is exactly [Mr r_k ; 0 ; 0]: the
-// stopping test ||D^{-1} Mr r|| <= rtol ||D^{-1} b|| (D the Jacobi diagonal) is
-// the MINRES test of the same system.
+// With lubrication the constraint rows couple U to the forces through R_lub;
+// the system is solved in pair space by preconditioned CG (pair_solve below),
+// with the same exact elimination of the stresslets and velocities around it.
 //
 // Replicas with more than 12 colloids (M_SS not solved densely), and replicas
-// whose PCG breaks down because Mr is not positive definite (the reference's
+// whose CG breaks down because Mr is not positive definite (the reference's
 // own monomer pair scalars make M indefinite), take the result as the warm
 // start of a MINRES polish.
 #include <cmath>
@@ -32,6 +25,7 @@
 #include "ps_internal.h"
 #include "ps_kernels.h"
 #include "ps_reduce.cuh"
+#include "lub_dev.cuh"
 
 namespace ps {
 
@@ -260,173 +254,441 @@ __global__ void k_pcg_g(RedTable T, const Seg *__restrict__ segs, const double *
     }
 }
 
-// c = R g - b_bot; V = 0; r = s = c; u_t = r
-__global__ void k_pcg_init(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ b,
-                           const double *__restrict__ Rg, double *__restrict__ V, double *__restrict__ r,
-                           double *__restrict__ sv, double *__restrict__ u)
+// ---------------------------------------------------------------------------
+// Lubricated solve in pair space.  With R = L L^T, L = [B_p K_p^{1/2}] over the
+// near pairs p (K_p the 12x12 pair block, B_p its velocity DOFs), the force
+// unknowns are F_t = -b_bot + L y, and y solves the SPD system
+//     (I + L^T Mr L) y = L^T (g + Mr b_bot),
+// of dimension 12 per pair (from (I + R Mr) F_t = R g - b_bot: F_t + b_bot lies
+// in the range of R; no term of the right-hand side carries the pair stiffness,
+// so the FP32 far field is not amplified by it).  CG is preconditioned
+// block-diagonally with (I + K_p^{1/2} M_pp K_p^{1/2})^{-1}, M_pp the pair's own
+// two-body FT mobility (self + pair blocks of the far field): the stiff squeeze
+// and shear modes of each near pair are resolved by its block, the far-field
+// coupling by CG.  After the solve U = Mr F_t - g exactly, so the saddle
+// residual is [0 ; 0 ; L r_y]: CG stops on ||D^{-1} L r_y|| <= rtol ||D^{-1} b||,
+// the MINRES test of the same system.
+//
+// Pair vectors hold 12 entries per canonical pair q (monomer pairs use the
+// first 6); pair-space sums run over the bead reduction table, each pair
+// attributed to its lower bead.
+
+constexpr int PS_THREADS = 64;
+
+// velocity DOFs of the pair in pair-DOF order: U_lo, U_hi, W_lo, W_hi
+__device__ __forceinline__ void pair_dofs(const Seg &s, long lo, long hi, bool mono, int dof[12], int &nd)
 {
-    const RBlk B = T.d_blk[blockIdx.x];
-    const Seg &s = segs[B.rep];
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long k = B.start + e;
-        int j = (int)(k - s.vel_off);
-        double c = Rg[k] - b[s.vec_off + s.nm3nc11 + j];
-        V[k] = 0.0; r[k] = c; sv[k] = c;
-        u[s.top_off + j] = c;
+    int il = (int)(lo - s.bead_off), ih = (int)(hi - s.bead_off);
+    int tl, wl, th, wh;
+    vel_dofs(s, il, tl, wl);
+    vel_dofs(s, ih, th, wh);
+    nd = mono ? 6 : 12;
+    for (int k = 0; k < 3; k++) {
+        dof[k] = tl + k; dof[3 + k] = th + k;
+        if (!mono) { dof[6 + k] = wl + k; dof[9 + k] = wh + k; }
     }
 }
 
-// z = (M [r ; F_S])_t split over the two applies; err = ||D_t^{-1} z||, rz = r.z
-__global__ void k_pcg_z(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ y,
-                        const double *__restrict__ y2, const double *__restrict__ D, const double *__restrict__ r,
-                        double *__restrict__ z, PcgScal *pc, int first, int maxit, int *nactive)
+// two-body FT far-field mobility of the pair in pair-DOF order, symmetrised
+__device__ void pair_mobility(const Seg &s, const double *__restrict__ x, const double *__restrict__ chain, long lo,
+                              long hi, bool mono, double *M)
+{
+    const int nd = mono ? 6 : 12;
+    for (int k = 0; k < nd * nd; k++) M[k] = 0.0;
+    double dx = x[3 * lo] - x[3 * hi], dy = x[3 * lo + 1] - x[3 * hi + 1], dz = x[3 * lo + 2] - x[3 * hi + 2];
+    double r2 = dx * dx + dy * dy + dz * dz, rinv = 1.0 / sqrt(r2), r = r2 * rinv;
+    double e[3] = {dx * rinv, dy * rinv, dz * rinv};
+    if (mono) {
+        for (int k = 0; k < 6; k++) M[k * 6 + k] = s.beta_inv;
+        bool coupled = s.mm_HI && !(s.chain_HI && chain[lo] == chain[hi]);
+        if (coupled) {
+            double xs, ys;
+            if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(r, rinv, 2.0 * s.beta, xs, ys);
+            else aa_scalars<double>(r, rinv, 2.0 * s.beta, xs, ys);
+            for (int a = 0; a < 3; a++)
+                for (int c = 0; c < 3; c++) {
+                    double v = (xs - ys) * e[a] * e[c] + (a == c ? ys : 0.0);
+                    M[a * 6 + 3 + c] = v;
+                    M[(3 + a) * 6 + c] = v;
+                }
+        }
+        return;
+    }
+    for (int k = 0; k < 3; k++) {
+        M[k * 12 + k] = 1.0; M[(3 + k) * 12 + 3 + k] = 1.0;
+        M[(6 + k) * 12 + 6 + k] = 0.75; M[(9 + k) * 12 + 9 + k] = 0.75;
+    }
+    // the partner's (F, T) column -> this bead's (U, W) rows, e = (x_lo - x_hi)/r as in the BB kernel
+    for (int side = 0; side < 2; side++) {
+        const bool is_lo = side == 0;
+        const int rowU = is_lo ? 0 : 3, rowW = is_lo ? 6 : 9, colF = is_lo ? 3 : 0, colT = is_lo ? 9 : 6;
+        for (int c = 0; c < 6; c++) {
+            double in[11], out[11];
+            for (int k = 0; k < 11; k++) { in[k] = 0.0; out[k] = 0.0; }
+            in[c] = 1.0;
+            bb_apply<double>(e, r, rinv, is_lo, in, out);
+            int col = c < 3 ? colF + c : colT + (c - 3);
+            for (int a = 0; a < 3; a++) { M[(rowU + a) * 12 + col] = out[a]; M[(rowW + a) * 12 + col] = out[3 + a]; }
+        }
+    }
+    for (int a = 0; a < 12; a++)
+        for (int c = a + 1; c < 12; c++) {
+            double v = 0.5 * (M[a * 12 + c] + M[c * 12 + a]);
+            M[a * 12 + c] = v; M[c * 12 + a] = v;
+        }
+}
+
+// per pair: S = K^{1/2} and P = (I + S M_pp S)^{-1} (identity if not positive definite)
+__global__ void __launch_bounds__(PS_THREADS)
+k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
+           const Seg *__restrict__ segs, const double *__restrict__ x, const double *__restrict__ chain,
+           const double *__restrict__ tab, int nrow, double *__restrict__ Sout, double *__restrict__ Pout)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npair) return;
+    const long lo = pairs[q].x, hi = pairs[q].y;
+    const Seg &s = segs[rep_of_b(bead_offs, R, lo)];
+    const bool mono = (lo - s.bead_off) < s.Nm;
+    const int nd = mono ? 6 : 12;
+    double K[144], Q[144], S[144], M[144];
+    lub_pair_block(s, x, tab, nrow, lo, hi, mono, K);
+    jacobi_eig(K, nd, Q);
+    for (int a = 0; a < nd; a++)
+        for (int c = 0; c < nd; c++) {
+            double v = 0.0;
+            for (int k = 0; k < nd; k++) {
+                double lam = K[k * nd + k];
+                v += Q[a * nd + k] * (lam > 0 ? sqrt(lam) : 0.0) * Q[c * nd + k];
+            }
+            S[a * nd + c] = v;
+        }
+    pair_mobility(s, x, chain, lo, hi, mono, M);
+    // T = I + S M S  (K <- M S, Q <- T)
+    for (int a = 0; a < nd; a++)
+        for (int c = 0; c < nd; c++) {
+            double v = 0.0;
+            for (int k = 0; k < nd; k++) v += M[a * nd + k] * S[k * nd + c];
+            K[a * nd + c] = v;
+        }
+    for (int a = 0; a < nd; a++)
+        for (int c = 0; c < nd; c++) {
+            double v = (a == c) ? 1.0 : 0.0;
+            for (int k = 0; k < nd; k++) v += S[a * nd + k] * K[k * nd + c];
+            Q[a * nd + c] = v;
+        }
+    // Cholesky T = C C^T in place (lower), then P = T^{-1} column by column
+    bool ok = true;
+    for (int j = 0; j < nd && ok; j++) {
+        double d = Q[j * nd + j];
+        for (int k = 0; k < j; k++) d -= Q[j * nd + k] * Q[j * nd + k];
+        if (!(d > 0)) { ok = false; break; }
+        d = sqrt(d);
+        Q[j * nd + j] = d;
+        for (int i = j + 1; i < nd; i++) {
+            double v = Q[i * nd + j];
+            for (int k = 0; k < j; k++) v -= Q[i * nd + k] * Q[j * nd + k];
+            Q[i * nd + j] = v / d;
+        }
+    }
+    double *So = Sout + 144 * q, *Po = Pout + 144 * q;
+    for (int k = 0; k < 144; k++) { So[k] = 0.0; Po[k] = 0.0; }
+    for (int a = 0; a < nd; a++)
+        for (int c = 0; c < nd; c++) So[a * 12 + c] = S[a * nd + c];
+    if (!ok) { for (int a = 0; a < nd; a++) Po[a * 12 + a] = 1.0; return; }
+    for (int c = 0; c < nd; c++) {
+        double v[12];
+        for (int i = 0; i < nd; i++) {
+            double t = (i == c) ? 1.0 : 0.0;
+            for (int k = 0; k < i; k++) t -= Q[i * nd + k] * v[k];
+            v[i] = t / Q[i * nd + i];
+        }
+        for (int i = nd - 1; i >= 0; i--) {
+            double t = v[i];
+            for (int k = i + 1; k < nd; k++) t -= Q[k * nd + i] * v[k];
+            v[i] = t / Q[i * nd + i];
+        }
+        for (int i = 0; i < nd; i++) Po[i * 12 + c] = v[i];
+    }
+}
+
+// v = L y (+ add): per bead, the rows of S_q y_q that belong to it, summed over
+// its near pairs in ascending partner order; optionally written into the first
+// nm3nc6 entries of a mobility-layout vector and reduced into ||D^{-1} L y||^2
+// per bead (constraint-row entries of D)
+__global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
+                       const int *__restrict__ sptr, const int *__restrict__ snbr, const int *__restrict__ cptr,
+                       const int *__restrict__ cnbr, const double *__restrict__ S, const double *__restrict__ y,
+                       const double *__restrict__ add, double *__restrict__ vel, double *__restrict__ top,
+                       const double *__restrict__ D, double *__restrict__ bead_part, const PcgScal *__restrict__ pc)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    const int r = rep_of_b(bead_offs, R, b);
+    if (pc && pc[r].done) return;
+    const Seg &s = segs[r];
+    const int i = (int)(b - s.bead_off);
+    const bool mono = i < s.Nm;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = sptr[b]; t < sptr[b + 1]; t++) {
+        long j = snbr[t];
+        const bool low = b < j;
+        long lo = low ? b : j, hi = low ? j : b;
+        int qa = cptr[lo], qb = cptr[lo + 1];
+        const int qend = qb;
+        while (qb - qa > 1) {
+            int mid = (qa + qb) >> 1;
+            if (cnbr[mid] <= hi) qa = mid; else qb = mid;
+        }
+        if (qa >= qend || cnbr[qa] != hi) continue;    // not in the canonical list (lists disagree)
+        const double *Sq = S + 144L * qa, *yq = y + 12L * qa;
+        const int ng = mono ? 1 : 2;
+        for (int g = 0; g < ng; g++)
+            for (int k = 0; k < 3; k++) {
+                const int row = 6 * g + (low ? 0 : 3) + k;
+                double v = 0.0;
+                for (int c = 0; c < 12; c++) v += Sq[row * 12 + c] * yq[c];
+                acc[3 * g + k] += v;
+            }
+    }
+    int tb, wb;
+    vel_dofs(s, i, tb, wb);
+    double nrm = 0.0;
+    for (int g = 0; g < (mono ? 1 : 2); g++)
+        for (int k = 0; k < 3; k++) {
+            const int d = (g == 0 ? tb : wb) + k;
+            double v = acc[3 * g + k] + (add ? add[s.vel_off + d] : 0.0);
+            if (vel) vel[s.vel_off + d] = v;
+            if (top) top[s.top_off + d] = v;
+            if (D) { double t = acc[3 * g + k] / D[s.vec_off + s.nm3nc11 + d]; nrm += t * t; }
+        }
+    if (bead_part) bead_part[b] = nrm;
+}
+
+// w_q = sign * S_q z_q (+ p_q), z gathered from the velocity rows of the Mr apply
+// (y + y2 for replicas with a dense stresslet block) plus an optional velocity
+// vector; part[q] = p_q . w_q
+__global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
+                        const Seg *__restrict__ segs, const double *__restrict__ S, const double *__restrict__ y,
+                        const double *__restrict__ y2, const double *__restrict__ addv, double sign,
+                        const double *__restrict__ p, double *__restrict__ w, double *__restrict__ part,
+                        const PcgScal *__restrict__ pc)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npair) return;
+    const long lo = pairs[q].x, hi = pairs[q].y;
+    const int r = rep_of_b(bead_offs, R, lo);
+    if (pc && pc[r].done) return;
+    const Seg &s = segs[r];
+    const bool mono = (lo - s.bead_off) < s.Nm;
+    int dof[12], nd;
+    pair_dofs(s, lo, hi, mono, dof, nd);
+    double z[12];
+    for (int k = 0; k < 12; k++) z[k] = 0.0;
+    for (int k = 0; k < nd; k++)
+        z[k] = y[s.top_off + dof[k]] + (s.ss_off >= 0 ? y2[s.top_off + dof[k]] : 0.0) +
+               (addv ? addv[s.vel_off + dof[k]] : 0.0);
+    const double *Sq = S + 144L * q;
+    double dot = 0.0;
+    for (int a = 0; a < 12; a++) {
+        double v = 0.0;
+        for (int c = 0; c < 12; c++) v += Sq[a * 12 + c] * z[c];
+        v *= sign;
+        if (p) { v += p[12 * q + a]; dot += p[12 * q + a] * v; }
+        w[12 * q + a] = v;
+    }
+    if (part) part[q] = dot;
+}
+
+// first iterate: y = 0, r = rhs (in rv), z = P r, p = z, part = r . z
+__global__ void k_ps_init(long npair, const double *__restrict__ P, double *__restrict__ yv,
+                          const double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ pv,
+                          double *__restrict__ part)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npair) return;
+    const double *Pq = P + 144L * q;
+    double dot = 0.0;
+    for (int a = 0; a < 12; a++) {
+        double v = 0.0;
+        for (int c = 0; c < 12; c++) v += Pq[a * 12 + c] * rv[12 * q + c];
+        zv[12 * q + a] = v;
+        pv[12 * q + a] = v;
+        yv[12 * q + a] = 0.0;
+        dot += rv[12 * q + a] * v;
+    }
+    part[q] = dot;
+}
+
+// y += alpha p ; r -= alpha Ap ; z = P r ; part = r . z
+__global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
+                            const PcgScal *__restrict__ pc, const double *__restrict__ P, const double *__restrict__ pv,
+                            const double *__restrict__ Ap, double *__restrict__ yv, double *__restrict__ rv,
+                            double *__restrict__ zv, double *__restrict__ part)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npair) return;
+    const PcgScal sc = pc[rep_of_b(bead_offs, R, pairs[q].x)];
+    if (sc.done) return;
+    double rq[12];
+    for (int a = 0; a < 12; a++) {
+        yv[12 * q + a] += sc.alpha * pv[12 * q + a];
+        rq[a] = rv[12 * q + a] - sc.alpha * Ap[12 * q + a];
+        rv[12 * q + a] = rq[a];
+    }
+    const double *Pq = P + 144L * q;
+    double dot = 0.0;
+    for (int a = 0; a < 12; a++) {
+        double v = 0.0;
+        for (int c = 0; c < 12; c++) v += Pq[a * 12 + c] * rq[c];
+        zv[12 * q + a] = v;
+        dot += rq[a] * v;
+    }
+    part[q] = dot;
+}
+
+// p = z + beta p
+__global__ void k_ps_dir(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
+                         const PcgScal *__restrict__ pc, const double *__restrict__ zv, double *__restrict__ pv)
+{
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npair) return;
+    const PcgScal sc = pc[rep_of_b(bead_offs, R, pairs[q].x)];
+    if (sc.done) return;
+    for (int a = 0; a < 12; a++) pv[12 * q + a] = zv[12 * q + a] + sc.beta * pv[12 * q + a];
+}
+
+// per-replica sums over the bead table: pair partials by lower bead, bead partials.
+// mode 0: alpha = rz / sum(part);  mode 1: first check (rz, err);  mode 2: iteration check
+__global__ void k_ps_reduce(RedTable T, const int *__restrict__ cptr, const double *__restrict__ part,
+                            const double *__restrict__ bead_part, PcgScal *pc, int mode, int maxit, int *nactive)
 {
     __shared__ double sh[RB_THREADS / 32][2];
     const RBlk B = T.d_blk[blockIdx.x];
     if (pc[B.rep].done) return;
-    const Seg &s = segs[B.rep];
     double v[2] = {0.0, 0.0};
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long k = B.start + e;
-        int j = (int)(k - s.vel_off);
-        double zk = y[s.top_off + j] + (s.ss_off >= 0 ? y2[s.top_off + j] : 0.0);
-        z[k] = zk;
-        double t = zk / D[s.vec_off + j];
-        v[0] += t * t;
-        v[1] += r[k] * zk;
+        long b = B.start + e;
+        for (int q = cptr[b]; q < cptr[b + 1]; q++) v[0] += part[q];
+        if (bead_part) v[1] += bead_part[b];
     }
     block_sum<2>(v, sh);
     double tot[2];
     if (finish_block<2>(T, B, blockIdx.x, v, tot)) {
         PcgScal p = pc[B.rep];
-        p.err = sqrt(tot[0]);
-        if (!first) p.it++;
-        if (p.err <= p.tol) { p.done = 1; p.reason = 2; }
-        else if (tot[1] <= 0.0) { p.done = 1; p.reason = -8; }          // preconditioner not positive
-        else if (p.it >= maxit) { p.done = 1; p.reason = -3; }
-        else {
-            p.beta = first ? 0.0 : tot[1] / p.rz;
-            p.rz = tot[1];
+        if (mode == 0) {
+            if (tot[0] <= 0.0) { p.done = 1; p.reason = -8; atomicSub(nactive, 1); }
+            else p.alpha = p.rz / tot[0];
+        } else {
+            p.err = sqrt(tot[1]);
+            if (mode == 2) p.it++;
+            if (p.err <= p.tol) { p.done = 1; p.reason = 2; }
+            else if (tot[0] <= 0.0) { p.done = 1; p.reason = -8; }
+            else if (p.it >= maxit) { p.done = 1; p.reason = -3; }
+            else {
+                p.beta = mode == 1 ? 0.0 : tot[0] / p.rz;
+                p.rz = tot[0];
+            }
+            if (p.done) atomicSub(nactive, 1);
         }
-        if (p.done) atomicSub(nactive, 1);
         pc[B.rep] = p;
     }
 }
 
-// p = z + beta p ; s = r + beta s
-__global__ void k_pcg_dir(RedTable T, const PcgScal *__restrict__ pc, const double *__restrict__ z,
-                          const double *__restrict__ r, double *__restrict__ p, double *__restrict__ sv, int first)
-{
-    const RBlk B = T.d_blk[blockIdx.x];
-    const PcgScal q = pc[B.rep];
-    if (q.done) return;
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long k = B.start + e;
-        if (first) { p[k] = z[k]; sv[k] = r[k]; }
-        else { p[k] = z[k] + q.beta * p[k]; sv[k] = r[k] + q.beta * sv[k]; }
-    }
-}
-
-// Ap = R p + s ; alpha = rz / p.Ap
-__global__ void k_pcg_alpha(RedTable T, const double *__restrict__ Rp, const double *__restrict__ sv,
-                            const double *__restrict__ p, double *__restrict__ Ap, PcgScal *pc, int *nactive)
-{
-    __shared__ double sh[RB_THREADS / 32][1];
-    const RBlk B = T.d_blk[blockIdx.x];
-    if (pc[B.rep].done) return;
-    double v[1] = {0.0};
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long k = B.start + e;
-        double a = Rp[k] + sv[k];
-        Ap[k] = a;
-        v[0] += p[k] * a;
-    }
-    block_sum<1>(v, sh);
-    double tot[1];
-    if (finish_block<1>(T, B, blockIdx.x, v, tot)) {
-        PcgScal q = pc[B.rep];
-        if (tot[0] <= 0.0) { q.done = 1; q.reason = -8; atomicSub(nactive, 1); }
-        else q.alpha = q.rz / tot[0];
-        pc[B.rep] = q;
-    }
-}
-
-// V += alpha p ; r -= alpha Ap ; u_t = r
-__global__ void k_pcg_update(RedTable T, const Seg *__restrict__ segs, const PcgScal *__restrict__ pc,
-                             const double *__restrict__ p, const double *__restrict__ Ap, double *__restrict__ V,
-                             double *__restrict__ r, double *__restrict__ u)
-{
-    const RBlk B = T.d_blk[blockIdx.x];
-    const PcgScal q = pc[B.rep];
-    if (q.done) return;
-    const Seg &s = segs[B.rep];
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long k = B.start + e;
-        V[k] += q.alpha * p[k];
-        double rk = r[k] - q.alpha * Ap[k];
-        r[k] = rk;
-        u[s.top_off + (k - s.vel_off)] = rk;
-    }
-}
-
-// U = V - g into the saddle solution
-__global__ void k_pcg_fin1(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ V,
-                           const double *__restrict__ g, double *__restrict__ x)
-{
-    const RBlk B = T.d_blk[blockIdx.x];
-    const Seg &s = segs[B.rep];
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long k = B.start + e;
-        x[s.vec_off + s.nm3nc11 + (k - s.vel_off)] = V[k] - g[k];
-    }
-}
-
-// F_t = -b_bot - R U into the saddle solution and into u_t
-__global__ void k_pcg_fin2(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ b,
-                           const double *__restrict__ RU, double *__restrict__ x, double *__restrict__ u)
+// c = -b_bot (velocity layout), u_t = b_bot
+__global__ void k_ps_c(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ b, double *__restrict__ c,
+                       double *__restrict__ u)
 {
     const RBlk B = T.d_blk[blockIdx.x];
     const Seg &s = segs[B.rep];
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
         long k = B.start + e;
         int j = (int)(k - s.vel_off);
-        double f = -b[s.vec_off + s.nm3nc11 + j] - RU[k];
-        x[s.vec_off + j] = f;
-        u[s.top_off + j] = f;
+        double v = b[s.vec_off + s.nm3nc11 + j];
+        c[k] = -v;
+        u[s.top_off + j] = v;
     }
 }
 
-// Mr r_t -> z (two applies: M [r;0], then M [0; -M_SS^{-1} (M [r;0])_S])
-static void pcg_precond(Engine &E, bool fp32, int first, int maxit, cudaStream_t st)
+// U = (y + y2)_t - g into the saddle solution
+__global__ void k_ps_fin(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ y,
+                         const double *__restrict__ y2, const double *__restrict__ g, double *__restrict__ x)
 {
-    RedTable &TV = E.red_vel;
-    const void *dn = &E.d_pcg[0].done;
-    const int ds = (int)sizeof(PcgScal);
+    const RBlk B = T.d_blk[blockIdx.x];
+    const Seg &s = segs[B.rep];
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        long k = B.start + e;
+        int j = (int)(k - s.vel_off);
+        double v = y[s.top_off + j] + (s.ss_off >= 0 ? y2[s.top_off + j] : 0.0) - g[k];
+        x[s.vec_off + s.nm3nc11 + j] = v;
+    }
+}
+
+// copy F_t (velocity layout) into the force rows of the saddle solution
+__global__ void k_ps_ft(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ ft, double *__restrict__ x)
+{
+    const RBlk B = T.d_blk[blockIdx.x];
+    const Seg &s = segs[B.rep];
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        long k = B.start + e;
+        x[s.vec_off + (k - s.vel_off)] = ft[k];
+    }
+}
+
+// Mr applied to the force rows held in E.d_pu (stresslet part zero):
+// d_py = M [u ; 0], d_pu2 = [0 ; -M_SS^{-1} (d_py)_S], d_py2 = M d_pu2
+static void mr_apply(Engine &E, bool fp32, const void *dn, int ds, cudaStream_t st)
+{
     apply_operator(E, 1, E.d_pu, E.d_py, nullptr, fp32, st, dn, ds);
     if (E.n_ss_reps) {
         ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, E.d_py, 1, -1.0,
-                                                                 nullptr, 1, 0.0, E.d_pu2, 1, E.d_pcg);
+                                                                 nullptr, 1, 0.0, E.d_pu2, 1,
+                                                                 dn ? E.d_pcg : nullptr);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, dn, ds, true);
     }
-    ::ps_launch_count++, k_pcg_z<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_py, E.d_py2, E.d_D, E.d_pr, E.d_pz,
-                                                              E.d_pcg, first, maxit, E.d_nactive);
-    ::ps_launch_count++, k_pcg_dir<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_pcg, E.d_pz, E.d_pr, E.d_pp, E.d_ps, first);
 }
 
-static int pcg_lub_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
-                         cudaStream_t st)
+static int ensure_pair_space(Engine &E)
 {
-    RedTable &TV = E.red_vel;
+    long need = std::max<long>(E.lub_npairs, 1);
+    if (need <= E.pair_cap) return PS_OK;
+    cudaFree(E.d_pS); cudaFree(E.d_pP); cudaFree(E.d_ppart);
+    for (auto &p : E.d_py_) cudaFree(p);
+    E.pair_cap = need * 3 / 2 + 256;
+    PS_CK(cudaMalloc(&E.d_pS, sizeof(double) * 144 * E.pair_cap));
+    PS_CK(cudaMalloc(&E.d_pP, sizeof(double) * 144 * E.pair_cap));
+    PS_CK(cudaMalloc(&E.d_ppart, sizeof(double) * E.pair_cap));
+    for (auto &p : E.d_py_) PS_CK(cudaMalloc(&p, sizeof(double) * 12 * E.pair_cap));
+    return PS_OK;
+}
+
+static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
+                      cudaStream_t st)
+{
+    RedTable &TV = E.red_vel, &TB = E.red_bead;
     const bool fp32 = E.precision == PS_PREC_MIXED;
     const int maxit = o->maxit > 0 ? o->maxit : 10000;
     const int check_every = o->check_every > 0 ? o->check_every : 8;
+    const long npair = E.lub_npairs;
+    const int thr = 128;
+    const unsigned nbp = (unsigned)((std::max<long>(npair, 1) + PS_THREADS - 1) / PS_THREADS);
+    const unsigned nbb = (unsigned)((E.ntot + thr - 1) / thr);
     int rc = diag_saddle(E, E.d_D, st);
     if (rc) return rc;
+    if ((rc = ensure_pair_space(E))) return rc;
+    double *yv = E.d_py_[0], *rv = E.d_py_[1], *zv = E.d_py_[2], *pv = E.d_py_[3], *Ap = E.d_py_[4];
+    // d_pr (nvel >= ntot doubles) holds the per-bead partials
+    double *cvel = E.d_pV, *g = E.d_pg, *tmp = E.d_tmp_vel, *bead_part = E.d_pr;
+    const void *dn = &E.d_pcg[0].done;
+    const int ds = (int)sizeof(PcgScal);
     PS_CK(cudaMemsetAsync(x, 0, sizeof(double) * E.nvec, st));
     PS_CK(cudaMemsetAsync(E.d_pu, 0, sizeof(double) * E.ntop, st));
     PS_CK(cudaMemsetAsync(E.d_pu2, 0, sizeof(double) * E.ntop, st));
     PS_CK(cudaMemsetAsync(E.d_py2, 0, sizeof(double) * E.ntop, st));
     ::ps_launch_count++, k_pcg_start<<<E.red.nblk, RB_THREADS, 0, st>>>(E.red, E.d_segs, b, E.d_D, E.d_pcg, o->rtol);
+    if (npair)
+        ::ps_launch_count++, k_ps_setup<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                                 E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.d_pS,
+                                                                 E.d_pP);
     if (E.n_ss_reps) {
         ::ps_launch_count++, k_ss_inverse<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, E.d_ssinv);
         // g: u2 = [0 ; M_SS^{-1} b_S]
@@ -434,10 +696,8 @@ static int pcg_lub_solve(Engine &E, const double *b, double *x, const ps_ksp_opt
                                                                  0, 0.0, E.d_pu2, 1, nullptr);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, nullptr, 0, true);
     }
-    ::ps_launch_count++, k_pcg_g<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, E.d_py2, E.d_pg);
-    lub_apply_vel(E, E.d_pg, E.d_tmp_vel, st);
-    ::ps_launch_count++, k_pcg_init<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, E.d_tmp_vel, E.d_pV, E.d_pr, E.d_ps,
-                                                                 E.d_pu);
+    ::ps_launch_count++, k_pcg_g<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, E.d_py2, g);
+    ::ps_launch_count++, k_ps_c<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, cvel, E.d_pu);
     PS_CK(cudaGetLastError());
     std::vector<PcgScal> hp(E.R);
     PS_CK(cudaMemcpyAsync(hp.data(), E.d_pcg, sizeof(PcgScal) * E.R, cudaMemcpyDeviceToHost, st));
@@ -446,30 +706,60 @@ static int pcg_lub_solve(Engine &E, const double *b, double *x, const ps_ksp_opt
     for (auto &p : hp) nact += !p.done;
     *E.h_nactive = nact;
     PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
-    if (nact > 0) pcg_precond(E, fp32, 1, maxit, st);
+    if (npair && nact) {
+        // rhs = L^T (g + Mr b_bot) ; r = rhs ; z = P r ; p = z
+        mr_apply(E, fp32, dn, ds, st);
+        ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                              E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
+                                                              E.d_pcg);
+        ::ps_launch_count++, k_ps_init<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_pP, yv, rv, zv, pv, E.d_ppart);
+    }
+    // initial residual ||D^{-1} L r||
+    ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
+                                                  E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr, nullptr, nullptr,
+                                                  E.d_D, bead_part, E.d_pcg);
+    ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, E.d_pcg, 1,
+                                                                  maxit, E.d_nactive);
+    PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    nact = *E.h_nactive;
     int k = 0;
     while (nact > 0 && k < maxit) {
         for (int j = 0; j < check_every && k < maxit; j++, k++) {
-            lub_apply_vel(E, E.d_pp, E.d_tmp_vel, st);
-            ::ps_launch_count++, k_pcg_alpha<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_tmp_vel, E.d_ps, E.d_pp, E.d_pAp,
-                                                                          E.d_pcg, E.d_nactive);
-            ::ps_launch_count++, k_pcg_update<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_pcg, E.d_pp, E.d_pAp,
-                                                                           E.d_pV, E.d_pr, E.d_pu);
-            pcg_precond(E, fp32, 0, maxit, st);
+            // Ap = p + L^T Mr L p
+            ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
+                                                          E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, pv, nullptr,
+                                                          nullptr, E.d_pu, nullptr, nullptr, E.d_pcg);
+            mr_apply(E, fp32, dn, ds, st);
+            ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                                  E.d_pS, E.d_py, E.d_py2, nullptr, 1.0, pv, Ap,
+                                                                  E.d_ppart, E.d_pcg);
+            ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, nullptr,
+                                                                          E.d_pcg, 0, maxit, E.d_nactive);
+            ::ps_launch_count++, k_ps_update<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                                      E.d_pcg, E.d_pP, pv, Ap, yv, rv, zv, E.d_ppart);
+            ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
+                                                          E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr,
+                                                          nullptr, nullptr, E.d_D, bead_part, E.d_pcg);
+            ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part,
+                                                                          E.d_pcg, 2, maxit, E.d_nactive);
+            ::ps_launch_count++, k_ps_dir<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_pcg,
+                                                                   zv, pv);
         }
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
         nact = *E.h_nactive;
     }
-    // reconstruct [F_t ; F_S ; U]
-    ::ps_launch_count++, k_pcg_fin1<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_pV, E.d_pg, x);
-    lub_apply(E, x, E.d_tmp_vel, st);
-    ::ps_launch_count++, k_pcg_fin2<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, E.d_tmp_vel, x, E.d_pu);
-    if (E.n_ss_reps) {
-        apply_operator(E, 1, E.d_pu, E.d_py, nullptr, fp32, st, nullptr, 0, true);   // colloid rows: M_St F_t
+    // F_t = -b_bot + L y (into u_t and the force rows), then U = Mr F_t - g, F_S
+    ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
+                                                  E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, yv, cvel, tmp, E.d_pu, nullptr,
+                                                  nullptr, nullptr);
+    ::ps_launch_count++, k_ps_ft<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, tmp, x);
+    mr_apply(E, fp32, nullptr, 0, st);
+    ::ps_launch_count++, k_ps_fin<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_py, E.d_py2, g, x);
+    if (E.n_ss_reps)
         ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, E.d_py,
                                                                  1, -1.0, x, 0, nullptr);
-    }
     PS_CK(cudaGetLastError());
     PS_CK(cudaMemcpyAsync(hp.data(), E.d_pcg, sizeof(PcgScal) * E.R, cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
@@ -494,7 +784,7 @@ int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o
 {
     if (E.any_lub) {
         ps_ksp_result r0 = {2, 0, 0, 0.0};
-        int rc = pcg_lub_solve(E, b, x, o, &r0, st);
+        int rc = pair_solve(E, b, x, o, &r0, st);
         if (rc) return rc;
         // replicas beyond the dense stresslet limit, and any whose PCG broke down
         // (an indefinite far-field mobility: the reference's own pair scalars),
