@@ -1,12 +1,19 @@
 """Benchmark: bead-steps/s of the per-timestep Stokesian-dynamics path on B200.
 
 One step = one full predictor-corrector step of every replica (5 saddle solves,
-Brownian noise M^{1/2} z and the RFD drift; src/run.cpp:70-162 of the
-reference).  bead-steps = sum over replicas of N_r x steps.
+Brownian noise M^{1/2} z, the RFD drift and lubrication; src/run.cpp:70-162 of
+the reference).  bead-steps = sum over replicas of N_r x steps.
+
+Default: the batched ensemble (256 replicas, N log-uniform in [64, 4096], full
+HI with lubrication), FP32-mixed far field, structured saddle solve, rtol 1e-8
+(the tolerance at which the mixed form stays within 1e-6 of FP64).  Beside the
+headline value the line carries the same ensemble in FP64 (batched), the plain
+FP64 GPU drop-in (one replica at a time, Jacobi MINRES) projected from a sample,
+and the mixed form's velocity error against FP64.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                   [--workload ensemble|brush|suspension|polymer_probe]
-                  [--precision fp64|mixed] [--replicas R]
+                  [--precision fp64|mixed] [--replicas R] [--no-lub] [--rtol T]
 
 For N > 1 it is launched under torchrun; every rank advances its own seeded
 ensemble (weak scaling, no collective in the step) and rank 0 prints the line.
@@ -45,22 +52,31 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "brush", "suspension", "polymer_probe"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--replicas", type=int, default=256)
-    ap.add_argument("--rtol", type=float, default=1e-6)
+    ap.add_argument("--no-lub", action="store_true", help="ensemble/suspension without near-field lubrication")
+    ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--solver", default="structured", choices=["minres", "structured"])
+    ap.add_argument("--plain-sample", type=int, default=12,
+                    help="replicas timed one by one in the plain FP64 drop-in form (0: skip)")
+    ap.add_argument("--err-sample", type=int, default=16, help="replicas of the mixed-vs-FP64 error check (0: skip)")
+    ap.add_argument("--no-fp64-batched", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
 
 def workload(args, rank=0):
     seed = args.seed + 1000 * rank
+    lub = not args.no_lub
     if args.workload == "ensemble":
-        return configs.ensemble(args.replicas, seed=seed), f"ensemble{args.replicas}"
+        return configs.ensemble(args.replicas, seed=seed, lub=lub), f"ensemble{args.replicas}" + ("_lub" if lub else "")
     if args.workload == "brush":
         return [configs.brush(seed=seed)], "brush4097"
     if args.workload == "suspension":
-        return [configs.suspension(seed=seed)], "suspension1024"
+        s = configs.suspension(seed=seed)
+        if lub:
+            s = configs.System(s.name, dict(s.params, lub_on=1, lub_gap=0.5), s.x)
+        return [s], "suspension1024" + ("_lub" if lub else "")
     return [configs.polymer_probe(seed=seed)], "polymer_probe222"
 
 
@@ -129,10 +145,15 @@ def cpu_baseline(systems, steps_budget_s=20.0, rtol=1e-6, threads=1):
         s = systems[int(idx)]
         if s.Np > 700 and sample:
             break
-        o = po.OracleSim(po.default_params(**dict(s.params, noise_lanczos=1)), s.x.ravel())
+        tab = None
+        if s.params.get("lub_on"):
+            from polystokes_brownian_b200.lubdat import load_table
+            tab = load_table()
+        o = po.OracleSim(po.default_params(**dict(s.params, noise_lanczos=1)), s.x.ravel(), lub_table=tab)
         rng = np.random.default_rng(0)
+        zl = rng.normal(size=12 * len(o.lub_pairs()[0])) if tab is not None else None
         t0 = time.perf_counter()
-        o.step(fb=rng.normal(size=o.nm3nc11), wrfd=rng.normal(size=o.nm3nc6), rtol=rtol)
+        o.step(fb=rng.normal(size=o.nm3nc11), wrfd=rng.normal(size=o.nm3nc6), zlub=zl, rtol=rtol)
         times.append(time.perf_counter() - t0)
         sample.append(s.Np)
         if time.perf_counter() - t_start > steps_budget_s:
@@ -158,7 +179,7 @@ def run_reference(args):
     systems, name = workload(args, 0)
     vals = []
     for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(systems, steps_budget_s=8.0, rtol=args.rtol)
+        cb = cpu_baseline(systems, steps_budget_s=6.0, rtol=args.rtol)
         if k >= args.warmup:
             vals.append(cb["value"])
     v = float(np.median(vals))
@@ -172,12 +193,80 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def plain_fp64(systems, args, budget_s=60.0):
+    """The plain FP64 GPU drop-in: each replica in its own context, one at a time,
+    FP64 operator and Jacobi-preconditioned MINRES -- the reference's MatShell +
+    KSPSolve path moved to the GPU.  A stratified sample of replicas is stepped
+    (1 warm-up + 1 timed step each, CUDA events); the per-replica step time is
+    fitted as a + b N + c N^2 and summed over the whole workload."""
+    import torch
+    from polystokes_brownian_b200 import _capi
+    from polystokes_brownian_b200.engine import Batch
+    Ns = np.array([s.Np for s in systems])
+    order = np.argsort(Ns)
+    k = min(args.plain_sample, len(systems))
+    pick = [int(order[int(round(i * (len(order) - 1) / max(1, k - 1)))]) for i in range(k)]
+    pick = sorted(set(pick), key=lambda i: Ns[i])
+    n, ms, iters = [], [], []
+    t_start = time.perf_counter()
+    for idx in pick:
+        b = Batch([systems[idx]], precision=_capi.PS_PREC_FP64)
+        b.step(rtol=args.rtol, maxit=50000, solver=_capi.PS_SOLVE_MINRES)
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        r = b.step(rtol=args.rtol, maxit=50000, solver=_capi.PS_SOLVE_MINRES)
+        e1.record(st)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        n.append(systems[idx].Np)
+        iters.append(max(r.iters))
+        b.close()
+        if time.perf_counter() - t_start > budget_s:
+            break
+    n = np.array(n, float)
+    A = np.stack([np.ones_like(n), n, n * n], 1)
+    coef, *_ = np.linalg.lstsq(A, np.array(ms), rcond=None)
+    if len(n) < 3 or np.any(A @ coef <= 0):
+        coef = np.array([0.0, 0.0, float(np.sum(ms) / np.sum(n * n))])
+    total_ms = float(sum(max(coef[0] + coef[1] * N + coef[2] * N * N, 1e-3) for N in Ns))
+    return {"value": float(Ns.sum()) / (total_ms * 1e-3), "unit": METRIC, "ms_per_step_projected": total_ms,
+            "sample_N": [int(v) for v in n], "sample_ms": ms, "sample_max_minres_iters": iters,
+            "form": "FP64, one replica per context, Jacobi-preconditioned MINRES (the reference's KSPSolve), "
+                    "rtol as the batched run",
+            "projection": "per-replica step time fitted as a + b N + c N^2 over the sample, summed over all replicas"}
+
+
+def velocity_error(systems, args):
+    """Relative velocity error of one step of the benchmarked form against FP64
+    at rtol 1e-10 on the same state and the same injected noise (first
+    err_sample replicas)."""
+    import torch
+    from polystokes_brownian_b200 import _capi
+    from polystokes_brownian_b200.engine import Batch
+    sub = systems[: args.err_sample]
+    prec = _capi.PS_PREC_MIXED if args.precision == "mixed" else _capi.PS_PREC_FP64
+    solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
+    out = []
+    for pr, rt in ((prec, args.rtol), (_capi.PS_PREC_FP64, 1e-10)):
+        b = Batch(sub, precision=pr)
+        fb = torch.from_numpy(np.random.default_rng(1).normal(size=b.ntop)).cuda()
+        wr = torch.from_numpy(np.random.default_rng(2).normal(size=b.nvel)).cuda()
+        b.step(fb=fb, wrfd=wr, rtol=rt, maxit=50000, solver=solver)
+        out.append(b.step_outputs()["up"].cpu().numpy())
+        b.close()
+    err = float(np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1]))
+    return {"rel_err_up": err, "replicas": len(sub), "against": "FP64 at rtol 1e-10, same state and injected noise",
+            "bound": 1e-6, "ok": err <= 1e-6}
+
+
 def run_b200(args):
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
     from polystokes_brownian_b200 import _capi
     from polystokes_brownian_b200.engine import Batch, _ptr
-    import ctypes as C
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -188,6 +277,7 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     systems, name = workload(args, rank)
     prec = _capi.PS_PREC_MIXED if args.precision == "mixed" else _capi.PS_PREC_FP64
+    solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
     b = Batch(systems, precision=prec)
     beads = int(sum(s.Np for s in systems))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
@@ -198,17 +288,14 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
     for _ in range(args.warmup):
         b.step(rtol=args.rtol, solver=solver)
     barrier()
     L = _capi.lib()
     launches0 = L.ps_kernel_launches()
     clk = Clocks(local)
-    lat = []
+    lat, iters, reasons = [], [], []
     t_total = 0.0
-    iters = []
-    reasons = []
     for _ in range(args.steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -222,10 +309,10 @@ def run_b200(args):
         iters.append(list(r.iters) + [r.lanczos_iters])
         reasons.append(r.reason)
     barrier()
-    xs, _ = b.state()
-    finite = bool(torch.isfinite(xs).all().item())
     clocks = clk.stop()
     launches = int(L.ps_kernel_launches() - launches0)
+    xs, _ = b.state()
+    finite = bool(torch.isfinite(xs).all().item())
     tmax = torch.tensor([t_total], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
@@ -234,16 +321,13 @@ def run_b200(args):
 
     # end to end through the C-ABI with host buffers: H2D positions, step, D2H positions
     xh = torch.empty(3 * b.ntot, dtype=torch.float64, pin_memory=True)
-    xd_state, _ = b.state()
-    xh.copy_(xd_state.cpu())
+    xh.copy_(xs.cpu())
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
-    e2e_iters = []
     for _ in range(args.steps):
         _capi.check(L.ps_set_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_set_state")
-        r = b.step(rtol=args.rtol, solver=solver)
-        e2e_iters.append(list(r.iters))
+        b.step(rtol=args.rtol, solver=solver)
         _capi.check(L.ps_get_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_get_state")
     e1.record(st)
     e1.synchronize()
@@ -254,40 +338,68 @@ def run_b200(args):
 
     # roofline of the dominant kernel (monomer-monomer pair kernel), timed live
     u = torch.randn(b.ntop, dtype=torch.float64, device="cuda")
-    ms_aa = C.c_double(0)
+    ms_aa, ms_all, peak = C.c_double(0), C.c_double(0), C.c_double(0)
     _capi.check(L.ps_time_kernel(b.h, 0, 10, _ptr(u), C.byref(ms_aa), b.stream), "ps_time_kernel")
-    ms_all = C.c_double(0)
     _capi.check(L.ps_time_kernel(b.h, 3, 10, _ptr(u), C.byref(ms_all), b.stream), "ps_time_kernel")
-    peak = C.c_double(0)
     _capi.check(L.ps_fma_peak(1 if prec == _capi.PS_PREC_FP64 else 0, C.byref(peak), b.stream), "ps_fma_peak")
     flops = pair_flops(systems)
     achieved = flops / (ms_aa.value * 1e-3) / 1e12 if ms_aa.value > 0 else 0.0
-    roof = {"bound": "fp64" if prec == _capi.PS_PREC_FP64 else "fp32", "kernel": "k_rpy_aa",
+    roof = {"bound": "fp64" if prec == _capi.PS_PREC_FP64 else "fp32",
+            "kernel": "k_rpy_aa_f2" if prec == _capi.PS_PREC_MIXED else "k_rpy_aa",
             "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value if peak.value else None, "traffic": None,
-            "peak_source": "measured in bench.py (FMA microkernel, ps_fma_peak)",
-            "flop_per_launch": flops, "ms_per_launch": ms_aa.value, "ms_mobility_apply": ms_all.value}
+            "peak_source": "measured FMA throughput of this GPU in bench.py (ps_fma_peak); CUDA-core work, "
+                           "no tensor-core or HBM denominator applies",
+            "flop_per_launch": flops, "flop_unit": "40 per directed monomer pair",
+            "ms_per_launch": ms_aa.value, "ms_mobility_apply": ms_all.value}
+    ntot = b.ntot
+    b.close()
+    del flush
+
+    extra = {}
+    if rank == 0 and world == 1:
+        if not args.no_fp64_batched and prec == _capi.PS_PREC_MIXED:
+            bf = Batch(systems, precision=_capi.PS_PREC_FP64)
+            bf.step(rtol=args.rtol, solver=solver)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(2):
+                bf.step(rtol=args.rtol, solver=solver)
+            e1.record(st)
+            e1.synchronize()
+            extra["fp64_batched"] = {"value": beads * 2 / (e0.elapsed_time(e1) * 1e-3), "unit": METRIC,
+                                     "ms_per_step": e0.elapsed_time(e1) / 2, "form": "FP64, batched, same solver"}
+            bf.close()
+        if args.plain_sample > 0:
+            pf = plain_fp64(systems, args)
+            pf["ratio"] = value / pf["value"]
+            extra["plain_fp64_drop_in"] = pf
+        if args.err_sample > 0:
+            extra["velocity_error"] = velocity_error(systems, args)
 
     if rank == 0:
         cb = cpu_baseline(systems, rtol=args.rtol) if world == 1 else None
         lat_sorted = sorted(lat)
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == _capi.PS_PREC_FP64 else "f32+f64",
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec == _capi.PS_PREC_MIXED else "f64",
                "data": "synthetic",
                "config": {"workload": name, "replicas": len(systems), "beads": beads, "rtol": args.rtol,
                           "precision": args.precision, "solver": args.solver,
                           "l2": "flushed (256 MB write) before every timed step",
-                          "parallelism": f"replicas x{world}"},
-               "latency_ms": {"p50": lat_sorted[len(lat) // 2], "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
-               "minres_iters": iters, "minres_iters_note": "per step: max MINRES iterations of the 5 solves, then the Lanczos subspace size", "minres_reason": reasons, "e2e_minres_iters": e2e_iters,
-               "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * 3 * b.ntot,
-                       "d2h_bytes_per_step": 8 * 3 * b.ntot},
+                          "parallelism": f"independent replicas x{world}, no collective"},
+               "latency_ms": {"p50": lat_sorted[len(lat) // 2],
+                              "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
+               "iters": iters, "iters_note": "per step: max Krylov iterations of the 5 solves, then the Lanczos "
+                                             "subspace size", "reason": reasons,
+               "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * 3 * ntot,
+                       "d2h_bytes_per_step": 8 * 3 * ntot},
                "gpu_launches": launches, "roofline": roof, "clocks": clocks, "state_finite": finite}
+        out.update(extra)
         if cb:
             out["cpu_baseline"] = cb
         print(json.dumps(out), flush=True)
-    b.close()
     if world > 1:
         dist.destroy_process_group()
 
