@@ -63,7 +63,7 @@ static void free_engine(Engine &E)
                     E.d_lzw, E.d_lzq, E.d_lzs, E.d_ssinv, E.d_pcg, E.d_pV, E.d_pr, E.d_pz, E.d_pp, E.d_ps,
                     E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2, E.d_rseed, E.d_rstep,
                     E.d_lubc_ptr, E.d_lubc_nbr, E.d_lub_pairs, E.d_pS, E.d_pP, E.d_py_[0], E.d_py_[1], E.d_py_[2],
-                    E.d_py_[3], E.d_py_[4], E.d_ppart};
+                    E.d_py_[3], E.d_py_[4], E.d_ppart, E.d_scan_sums};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -293,6 +293,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_lub_ptr, sizeof(int) * (bead + 1));
     TRY_ALLOC(E.d_lubc_ptr, sizeof(int) * (bead + 1));
     TRY_ALLOC(E.d_nbr_count, sizeof(int) * (bead + 1));
+    E.scan_cap = (std::max<long>(bead, cells) + 4095) / 4096 + 8;
+    TRY_ALLOC(E.d_scan_sums, sizeof(int) * E.scan_cap);
     E.nbr_cap = 16 * bead + 1024;
     TRY_ALLOC(E.d_nbr, sizeof(int) * E.nbr_cap);
     // Krylov

@@ -559,7 +559,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     seg_dot(E, T, z, z, nrm2, st);
     ::ps_launch_count++, k_lz_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, V, z, lz, nrm2);
     PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
-    int check = 4;
+    const int check = 8;   // convergence test every 8 vectors; the cap is handled after the loop
     size_t smem = sizeof(double) * (2 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
     std::vector<LzScal> hl(E.R);
     int j = 0;
@@ -573,8 +573,8 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
         seg_dot(E, T, q, q, nrm2, st);
         ::ps_launch_count++, k_lz_breakdown<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, nrm2, j);
         if (j + 1 < kmax) ::ps_launch_count++, k_lz_next<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, nrm2, betad);
-        if ((j + 1) % check == 0 || j + 1 == kmax) {
-            ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, j + 1, tol, j + 1 == kmax);
+        if ((j + 1) % check == 0 && j + 1 < kmax) {
+            ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, j + 1, tol, 0);
             PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
             PS_CK(cudaStreamSynchronize(st));
             bool all = true;
@@ -582,7 +582,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
             if (all) break;
         }
     }
-    // replicas stopped by breakdown (done == 2) still need their final estimate
+    // final estimate: replicas at the cap, and replicas stopped by breakdown
     ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, std::min(j + 1, kmax), tol, 1);
     ::ps_launch_count++, k_lz_combine<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, lz, gbuf, w);
     PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));

@@ -139,9 +139,22 @@ __global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R,
             curand_init(rseed[r], (unsigned long long)(q - cptr[s.bead_off]), (3ull * rstep[r] + 2) * 4ull, &stt);
             for (int k = 0; k < 12; k++) zp[k] = curand_normal_double(&stt);
         }
-        double Rm[144], w[12];
-        lub_pair_block(s, x, tab, nrow, lo, hi, mono, Rm);
-        small_sqrt_apply(Rm, nd, zp, w);
+        double w[12];
+        if (mono) {
+            double d[3], lam[4], sq[4], Sm[36];
+            mono_pair_modes(s, x, tab, nrow, lo, hi, d, lam);
+            for (int k = 0; k < 4; k++) sq[k] = lam[k] > 0 ? sqrt(lam[k]) : 0.0;
+            mono_pair_matrix(d, sq, Sm, 6);
+            for (int a = 0; a < 6; a++) {
+                double v = 0.0;
+                for (int c = 0; c < 6; c++) v += Sm[a * 6 + c] * zp[c];
+                w[a] = v;
+            }
+        } else {
+            double Rm[144];
+            lub_pair_block(s, x, tab, nrow, lo, hi, mono, Rm);
+            small_sqrt_apply(Rm, nd, zp, w);
+        }
         const int o = low ? 0 : 3;
         for (int k = 0; k < 3; k++) acc[k] += w[o + k];
         if (!mono) for (int k = 0; k < 3; k++) acc[3 + k] += w[6 + o + k];
@@ -153,14 +166,26 @@ __global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R,
     if (!mono) for (int k = 0; k < 3; k++) rhs[base + wb + k] += scale * acc[3 + k];
 }
 
-__global__ void k_lub_pairs(long ntot, const int *__restrict__ ptr, const int *__restrict__ nbr, int2 *__restrict__ pairs)
+__global__ void k_canon_count(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr, int *__restrict__ cnt)
 {
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
-    for (int q = ptr[b]; q < ptr[b + 1]; q++) pairs[q] = make_int2((int)b, nbr[q]);
+    int n = 0;
+    for (int t = sptr[b]; t < sptr[b + 1]; t++) n += snbr[t] > b;
+    cnt[b] = n;
 }
 
-// build the symmetric partner list (which 3) and the canonical i<j list (which 2)
+__global__ void k_canon_fill(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr,
+                             const int *__restrict__ cptr, int *__restrict__ cnbr, int2 *__restrict__ pairs)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    int q = cptr[b];
+    for (int t = sptr[b]; t < sptr[b + 1]; t++)
+        if (snbr[t] > b) { cnbr[q] = snbr[t]; pairs[q] = make_int2((int)b, snbr[t]); q++; }
+}
+
+// build the symmetric partner list (which 3) and from it the canonical i<j list
 int lub_build(Engine &E, cudaStream_t st)
 {
     long np = 0;
@@ -174,24 +199,23 @@ int lub_build(Engine &E, cudaStream_t st)
     }
     PS_CK(cudaMemcpyAsync(E.d_lub_ptr, E.d_nbr_ptr, sizeof(int) * (E.ntot + 1), cudaMemcpyDeviceToDevice, st));
     if (np) PS_CK(cudaMemcpyAsync(E.d_lub_nbr, E.d_nbr, sizeof(int) * np, cudaMemcpyDeviceToDevice, st));
-    // canonical list (lo < hi, ascending), kept in its own buffers and as a flat pair array
-    long nc = 0;
-    rc = build_list(E, 2, &nc, st);
-    if (rc) return rc;
-    if (nc + 1 > E.lubc_cap) {
+    // canonical list (lo < hi, ascending): the partners j > b of the symmetric
+    // list, which holds every pair twice (the membership test is symmetric)
+    // (capacity for np entries: a bound whatever the list holds)
+    const long nc = np / 2;
+    if (np + 1 > E.lubc_cap) {
         cudaFree(E.d_lubc_nbr);
         cudaFree(E.d_lub_pairs);
-        E.lubc_cap = nc * 3 / 2 + 1024;
+        E.lubc_cap = np * 3 / 2 + 1024;
         PS_CK(cudaMalloc(&E.d_lubc_nbr, sizeof(int) * E.lubc_cap));
         PS_CK(cudaMalloc(&E.d_lub_pairs, sizeof(int2) * E.lubc_cap));
     }
-    PS_CK(cudaMemcpyAsync(E.d_lubc_ptr, E.d_nbr_ptr, sizeof(int) * (E.ntot + 1), cudaMemcpyDeviceToDevice, st));
-    if (nc) {
-        PS_CK(cudaMemcpyAsync(E.d_lubc_nbr, E.d_nbr, sizeof(int) * nc, cudaMemcpyDeviceToDevice, st));
-        int thr = 128;
-        ::ps_launch_count++, k_lub_pairs<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_lubc_ptr,
-                                                                                           E.d_lubc_nbr, E.d_lub_pairs);
-    }
+    int thr = 128;
+    unsigned nb = (unsigned)((E.ntot + thr - 1) / thr);
+    ::ps_launch_count++, k_canon_count<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_nbr_count);
+    if ((rc = exclusive_scan(E, E.d_nbr_count, E.d_lubc_ptr, E.ntot, st))) return rc;
+    ::ps_launch_count++, k_canon_fill<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
+                                                       E.d_lub_pairs);
     E.lub_npairs = nc;
     PS_CK(cudaGetLastError());
     return PS_OK;

@@ -156,4 +156,38 @@ __device__ inline void lub_pair_block(const Seg &s, const double *__restrict__ x
         }
 }
 
+// Monomer pair block in closed form.  K = [[A11, A12], [A12, A11]] with
+// A11 = a (f0 dd + f2 (I - dd)), A12 = a (f1 dd + f3 (I - dd)): the symmetric
+// modes (v, v)/sqrt2 see A11 + A12, the antisymmetric (v, -v)/sqrt2 see
+// A11 - A12, each with one eigenvalue along d and a double one across.
+// lam = {sym along, sym across, anti along, anti across}; d = (x_hi - x_lo)/r.
+__device__ inline void mono_pair_modes(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab,
+                                       int nrow, long lo, long hi, double d[3], double lam[4])
+{
+    const double a = s.beta;
+    double dx = x[3 * hi] - x[3 * lo], dy = x[3 * hi + 1] - x[3 * lo + 1], dz = x[3 * hi + 2] - x[3 * lo + 2];
+    mimg_l(s, dx, dy, dz);
+    double rr = sqrt(dx * dx + dy * dy + dz * dz);
+    d[0] = dx / rr; d[1] = dy / rr; d[2] = dz / rr;
+    double f[10];
+    lub_scalars(tab, nrow, rr / a, f);
+    lam[0] = a * (f[0] + f[1]); lam[1] = a * (f[2] + f[3]);
+    lam[2] = a * (f[0] - f[1]); lam[3] = a * (f[2] - f[3]);
+}
+
+// 6x6 matrix [[B, C], [C, B]] (row-major, leading dimension ld) from mode
+// values g = {sym along, sym across, anti along, anti across}:
+// B = (Gs + Ga)/2, C = (Gs - Ga)/2, G = g_along dd + g_across (I - dd)
+__device__ inline void mono_pair_matrix(const double d[3], const double g[4], double *Mout, int ld)
+{
+    for (int p = 0; p < 3; p++)
+        for (int q = 0; q < 3; q++) {
+            double dd = d[p] * d[q], id = (p == q) - dd;
+            double gs = g[0] * dd + g[1] * id, ga = g[2] * dd + g[3] * id;
+            double B = 0.5 * (gs + ga), Cc = 0.5 * (gs - ga);
+            Mout[p * ld + q] = B; Mout[(3 + p) * ld + 3 + q] = B;
+            Mout[p * ld + 3 + q] = Cc; Mout[(3 + p) * ld + q] = Cc;
+        }
+}
+
 }  // namespace ps

@@ -156,15 +156,62 @@ __global__ void k_pairs_fill(long ntot, const int *__restrict__ bead_offs, int R
     }
 }
 
-__global__ void k_scan_int(long n, const int *__restrict__ in, int *__restrict__ out)
+// Exclusive scan out[0..n] of in[0..n-1] (out[n] = total), three phases: each
+// block scans SCAN_SPAN elements (16 per thread, warp-shuffle scan of the thread
+// totals), one block scans the block totals, then every block adds its offset.
+constexpr int SCAN_T = 256, SCAN_E = 16, SCAN_SPAN = SCAN_T * SCAN_E;
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_local(long n, const int *__restrict__ in, int *__restrict__ out,
+                                                       int *__restrict__ sums)
+{
+    __shared__ int ws[SCAN_T / 32];
+    const long base = (long)blockIdx.x * SCAN_SPAN + (long)threadIdx.x * SCAN_E;
+    int v[SCAN_E], tot = 0;
+#pragma unroll
+    for (int e = 0; e < SCAN_E; e++) {
+        long k = base + e;
+        v[e] = k < n ? in[k] : 0;
+        tot += v[e];
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) ws[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int x = lane < SCAN_T / 32 ? ws[lane] : 0, xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += t;
+        }
+        if (lane < SCAN_T / 32) ws[lane] = xi - x;
+    }
+    __syncthreads();
+    int ex = ws[w] + inc - tot;
+#pragma unroll
+    for (int e = 0; e < SCAN_E; e++) {
+        long k = base + e;
+        if (k < n) out[k] = ex;
+        ex += v[e];
+    }
+    if (threadIdx.x == SCAN_T - 1) sums[blockIdx.x] = ws[w] + inc;
+}
+
+// in-place exclusive scan of the m block totals, total into sums[m]
+__global__ void k_scan_sums(int m, int *__restrict__ sums)
 {
     __shared__ int carry;
     __shared__ int tmp[1024];
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (long base = 0; base < n; base += 1024) {
-        long k = base + threadIdx.x;
-        int v = k < n ? in[k] : 0;
+    for (int base = 0; base < m; base += 1024) {
+        int k = base + threadIdx.x;
+        int v = k < m ? sums[k] : 0;
         tmp[threadIdx.x] = v;
         __syncthreads();
         for (int o = 1; o < 1024; o <<= 1) {
@@ -173,12 +220,35 @@ __global__ void k_scan_int(long n, const int *__restrict__ in, int *__restrict__
             tmp[threadIdx.x] += t;
             __syncthreads();
         }
-        if (k < n) out[k] = carry + tmp[threadIdx.x] - v;
+        if (k < m) sums[k] = carry + tmp[threadIdx.x] - v;
         __syncthreads();
         if (threadIdx.x == 1023) carry += tmp[1023];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[n] = carry;
+    if (threadIdx.x == 0) sums[m] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_add(long n, int m, const int *__restrict__ sums, int *__restrict__ out)
+{
+    const int off = sums[blockIdx.x];
+    const long base = (long)blockIdx.x * SCAN_SPAN;
+    for (int e = threadIdx.x; e < SCAN_SPAN; e += SCAN_T) {
+        long k = base + e;
+        if (k < n) out[k] += off;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = sums[m];
+}
+
+int exclusive_scan(Engine &E, const int *in, int *out, long n, cudaStream_t st)
+{
+    long m = (n + SCAN_SPAN - 1) / SCAN_SPAN;
+    if (m < 1) m = 1;
+    if (m + 1 > E.scan_cap) { set_error("scan scratch too small"); return PS_ERR_STATE; }
+    ::ps_launch_count++, k_scan_local<<<(unsigned)m, SCAN_T, 0, st>>>(n, in, out, E.d_scan_sums);
+    ::ps_launch_count++, k_scan_sums<<<1, 1024, 0, st>>>((int)m, E.d_scan_sums);
+    ::ps_launch_count++, k_scan_add<<<(unsigned)m, SCAN_T, 0, st>>>(n, (int)m, E.d_scan_sums, out);
+    PS_CK(cudaGetLastError());
+    return PS_OK;
 }
 
 __global__ void k_pairs_expand(long ntot, const int *__restrict__ ptr, const int *__restrict__ nbr,
@@ -197,7 +267,8 @@ int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
     unsigned nbk = (unsigned)((E.ntot + thr - 1) / thr);
     ::ps_launch_count++, k_pairs_count<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
                                        E.d_cell_start, E.d_cell_sorted, which, E.d_nbr_count);
-    ::ps_launch_count++, k_scan_int<<<1, 1024, 0, st>>>(E.ntot, E.d_nbr_count, E.d_nbr_ptr);
+    int rc = exclusive_scan(E, E.d_nbr_count, E.d_nbr_ptr, E.ntot, st);
+    if (rc) return rc;
     int tot = 0;
     PS_CK(cudaMemcpyAsync(&tot, E.d_nbr_ptr + E.ntot, sizeof(int), cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));

@@ -89,6 +89,7 @@ struct Engine {
     int *d_nbr_ptr = nullptr, *d_nbr = nullptr;   // CSR neighbour lists (i<j pairs per i)
     long nbr_cap = 0;
     int *d_nbr_count = nullptr;
+    int *d_scan_sums = nullptr; long scan_cap = 0;   // block totals of exclusive_scan
 
     // lubrication
     double *d_lubtab = nullptr; int lub_nrow = 0;
@@ -161,6 +162,8 @@ int stage_assemble(Engine &E, cudaStream_t st);
 int stage_schur(Engine &E, cudaStream_t st);
 int diag_saddle(Engine &E, double *d, cudaStream_t st);
 int pair_list(Engine &E, int which, int32_t *pi, int32_t *pj, int64_t maxp, int64_t *count, cudaStream_t st);
+// out[0..n] = exclusive scan of in[0..n-1], out[n] = total (pairs.cu)
+int exclusive_scan(Engine &E, const int *in, int *out, long n, cudaStream_t st);
 int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
 int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStream_t st);
 // krylov.cu

@@ -141,7 +141,51 @@ constexpr int AAF_THREADS = 64;
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-__global__ void __launch_bounds__(AAF_THREADS)
+// one staged column tile against the thread's two rows; CHECK: the tile may
+// hold the rows themselves or (chain_HI) same-chain partners, which get rinv = 0
+template <bool CHECK>
+__device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const float4 *__restrict__ sB,
+                                           const float2 *__restrict__ sC, int jt, int nj, int i0, int i1,
+                                           bool chain_hi, float w0, float w1, float2 px, float2 py, float2 pz,
+                                           float2 lx, float2 ly, float2 lz, float2 cx1, float2 cx3, float2 cy1,
+                                           float2 cy3, float nx0, float nx1, float ny0, float ny1, float two_beta,
+                                           float2 &tx, float2 &ty, float2 &tz)
+{
+#pragma unroll 4
+    for (int k = 0; k < nj; k++) {
+        const float4 A = sA[k], B = sB[k];
+        const float2 C = sC[k];
+        float2 dx = __fadd2_rn(__fadd2_rn(px, f2(-A.x)), __fadd2_rn(lx, f2(-B.x)));
+        float2 dy = __fadd2_rn(__fadd2_rn(py, f2(-A.y)), __fadd2_rn(ly, f2(-B.y)));
+        float2 dz = __fadd2_rn(__fadd2_rn(pz, f2(-A.z)), __fadd2_rn(lz, f2(-B.z)));
+        float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        bool e0 = false, e1 = false;
+        if constexpr (CHECK) {
+            const int j = jt + k;
+            e0 = (j == i0) || (chain_hi && w0 == A.w);
+            e1 = (j == i1) || (chain_hi && w1 == A.w);
+        }
+        float2 ri = make_float2(e0 ? 0.f : rsqrtf(r2.x), e1 ? 0.f : rsqrtf(r2.y));
+        float2 ri2 = __fmul2_rn(ri, ri);
+        float2 ri3 = __fmul2_rn(ri2, ri);
+        float2 x = __ffma2_rn(cx3, ri3, __fmul2_rn(cx1, ri));
+        float2 y = __ffma2_rn(cy3, ri3, __fmul2_rn(cy1, ri));
+        float2 r = __fmul2_rn(r2, ri);
+        const bool n0 = !e0 && r.x <= two_beta, n1 = !e1 && r.y <= two_beta;
+        if (__any_sync(0xffffffffu, n0 || n1)) {
+            if (n0) { x.x = nx0 + nx1 * r.x; y.x = ny0 + ny1 * r.x; }
+            if (n1) { x.y = nx0 + nx1 * r.y; y.y = ny0 + ny1 * r.y; }
+        }
+        // mob_a u = y u + (x - y)(d.u) d / r^2
+        float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(B.w))));
+        float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(x, make_float2(-y.x, -y.y)), du), ri2);
+        tx = __ffma2_rn(f, dx, __ffma2_rn(y, f2(B.w), tx));
+        ty = __ffma2_rn(f, dy, __ffma2_rn(y, f2(C.x), ty));
+        tz = __ffma2_rn(f, dz, __ffma2_rn(y, f2(C.y), tz));
+    }
+}
+
+__global__ void __launch_bounds__(AAF_THREADS, 16)
 k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const float4 *__restrict__ pos,
             const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
             long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
@@ -181,35 +225,14 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
         }
         __syncthreads();
         float2 tx = f2(0.f), ty = f2(0.f), tz = f2(0.f);
-#pragma unroll 4
-        for (int k = 0; k < nj; k++) {
-            const float4 A = sA[k], B = sB[k];
-            const float2 C = sC[k];
-            const int j = jt + k;
-            float2 dx = __fadd2_rn(__fadd2_rn(px, f2(-A.x)), __fadd2_rn(lx, f2(-B.x)));
-            float2 dy = __fadd2_rn(__fadd2_rn(py, f2(-A.y)), __fadd2_rn(ly, f2(-B.y)));
-            float2 dz = __fadd2_rn(__fadd2_rn(pz, f2(-A.z)), __fadd2_rn(lz, f2(-B.z)));
-            float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const bool e0 = (j == i0) || (chain_hi && P0.w == A.w);
-            const bool e1 = (j == i1) || (chain_hi && P1.w == A.w);
-            float2 ri = make_float2(e0 ? 0.f : rsqrtf(r2.x), e1 ? 0.f : rsqrtf(r2.y));
-            float2 ri2 = __fmul2_rn(ri, ri);
-            float2 ri3 = __fmul2_rn(ri2, ri);
-            float2 x = __ffma2_rn(cx3, ri3, __fmul2_rn(cx1, ri));
-            float2 y = __ffma2_rn(cy3, ri3, __fmul2_rn(cy1, ri));
-            float2 r = __fmul2_rn(r2, ri);
-            const bool n0 = !e0 && r.x <= two_beta, n1 = !e1 && r.y <= two_beta;
-            if (__any_sync(0xffffffffu, n0 || n1)) {
-                if (n0) { x.x = nx0 + nx1 * r.x; y.x = ny0 + ny1 * r.x; }
-                if (n1) { x.y = nx0 + nx1 * r.y; y.y = ny0 + ny1 * r.y; }
-            }
-            // mob_a u = y u + (x - y)(d.u) d / r^2
-            float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(B.w))));
-            float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(x, make_float2(-y.x, -y.y)), du), ri2);
-            tx = __ffma2_rn(f, dx, __ffma2_rn(y, f2(B.w), tx));
-            ty = __ffma2_rn(f, dy, __ffma2_rn(y, f2(C.x), ty));
-            tz = __ffma2_rn(f, dz, __ffma2_rn(y, f2(C.y), tz));
-        }
+        // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
+        const bool check = chain_hi || (jt < tl.row0 + 2 * AAF_THREADS && jt + nj > tl.row0);
+        if (check)
+            aa_f2_cols<true>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, cx1, cx3, cy1,
+                             cy3, nx0, nx1, ny0, ny1, two_beta, tx, ty, tz);
+        else
+            aa_f2_cols<false>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, cx1, cx3, cy1,
+                              cy3, nx0, nx1, ny0, ny1, two_beta, tx, ty, tz);
         // Kahan across column tiles
         float2 yy, tt;
         yy = __fadd2_rn(tx, make_float2(-kx.x, -kx.y)); tt = __fadd2_rn(sx, yy);

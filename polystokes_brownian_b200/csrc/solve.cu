@@ -338,7 +338,8 @@ __device__ void pair_mobility(const Seg &s, const double *__restrict__ x, const 
         }
 }
 
-// per pair: S = K^{1/2} and P = (I + S M_pp S)^{-1} (identity if not positive definite)
+// per pair: S = K^{1/2} and P = (I + S M_pp S)^{-1} (identity if not positive
+// definite); monomer pairs in closed form, colloid pairs by Jacobi + Cholesky
 __global__ void __launch_bounds__(PS_THREADS)
 k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
            const Seg *__restrict__ segs, const double *__restrict__ x, const double *__restrict__ chain,
@@ -349,7 +350,31 @@ k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ b
     const long lo = pairs[q].x, hi = pairs[q].y;
     const Seg &s = segs[rep_of_b(bead_offs, R, lo)];
     const bool mono = (lo - s.bead_off) < s.Nm;
-    const int nd = mono ? 6 : 12;
+    double *So = Sout + 144 * q, *Po = Pout + 144 * q;
+    if (mono) {
+        // closed form: S and the mobility share the modes of the pair block
+        double d[3], lam[4], sq[4], pm[4];
+        mono_pair_modes(s, x, tab, nrow, lo, hi, d, lam);
+        double xs = 0.0, ys = 0.0;
+        if (s.mm_HI && !(s.chain_HI && chain[lo] == chain[hi])) {
+            double dx = x[3 * lo] - x[3 * hi], dy = x[3 * lo + 1] - x[3 * hi + 1], dz = x[3 * lo + 2] - x[3 * hi + 2];
+            double r2 = dx * dx + dy * dy + dz * dz, rinv = 1.0 / sqrt(r2);
+            if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(r2 * rinv, rinv, 2.0 * s.beta, xs, ys);
+            else aa_scalars<double>(r2 * rinv, rinv, 2.0 * s.beta, xs, ys);
+        }
+        const double mob[4] = {s.beta_inv + xs, s.beta_inv + ys, s.beta_inv - xs, s.beta_inv - ys};
+        for (int k = 0; k < 4; k++) {
+            double l = lam[k] > 0 ? lam[k] : 0.0;
+            sq[k] = sqrt(l);
+            double t = 1.0 + l * mob[k];
+            pm[k] = t > 0 ? 1.0 / t : 1.0;
+        }
+        for (int k = 0; k < 144; k++) { So[k] = 0.0; Po[k] = 0.0; }
+        mono_pair_matrix(d, sq, So, 12);
+        mono_pair_matrix(d, pm, Po, 12);
+        return;
+    }
+    const int nd = 12;
     double K[144], Q[144], S[144], M[144];
     lub_pair_block(s, x, tab, nrow, lo, hi, mono, K);
     jacobi_eig(K, nd, Q);
@@ -390,7 +415,6 @@ k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ b
             Q[i * nd + j] = v / d;
         }
     }
-    double *So = Sout + 144 * q, *Po = Pout + 144 * q;
     for (int k = 0; k < 144; k++) { So[k] = 0.0; Po[k] = 0.0; }
     for (int a = 0; a < nd; a++)
         for (int c = 0; c < nd; c++) So[a * 12 + c] = S[a * nd + c];

@@ -197,31 +197,6 @@ __global__ void k_cell_assign(long ntot, const int *__restrict__ bead_offs, int 
 }
 
 // exclusive scan over all cells (single block, sequential chunks; cell counts are small)
-__global__ void k_scan(long n, const int *__restrict__ in, int *__restrict__ out)
-{
-    __shared__ int carry;
-    __shared__ int tmp[1024];
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (long base = 0; base < n; base += 1024) {
-        long k = base + threadIdx.x;
-        int v = k < n ? in[k] : 0;
-        tmp[threadIdx.x] = v;
-        __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            int t = threadIdx.x >= o ? tmp[threadIdx.x - o] : 0;
-            __syncthreads();
-            tmp[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (k < n) out[k] = carry + tmp[threadIdx.x] - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry += tmp[1023];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) out[n] = carry;
-}
-
 // deterministic fill: each cell's members in ascending bead order
 __global__ void k_cell_fill(long ntot, const int *__restrict__ cell, const int *__restrict__ start,
                             int *__restrict__ fillc, int *__restrict__ sorted)
@@ -253,7 +228,8 @@ int stage_cells(Engine &E, cudaStream_t st, const long *d_cell_off, long ncells)
     unsigned nb = (unsigned)((E.ntot + thr - 1) / thr);
     ::ps_launch_count++, k_cell_assign<<<nb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, d_cell_off, E.d_cell,
                                       E.d_cell_count);
-    ::ps_launch_count++, k_scan<<<1, 1024, 0, st>>>(ncells, E.d_cell_count, E.d_cell_start);
+    int rc = exclusive_scan(E, E.d_cell_count, E.d_cell_start, ncells, st);
+    if (rc) return rc;
     PS_CK(cudaMemsetAsync(E.d_cell_count, 0, sizeof(int) * (ncells + 1), st));
     ::ps_launch_count++, k_cell_fill<<<nb, thr, 0, st>>>(E.ntot, E.d_cell, E.d_cell_start, E.d_cell_count, E.d_cell_sorted);
     ::ps_launch_count++, k_cell_sort<<<(unsigned)((ncells + thr - 1) / thr), thr, 0, st>>>(ncells, E.d_cell_start, E.d_cell_sorted);
