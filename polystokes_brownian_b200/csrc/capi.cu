@@ -63,7 +63,11 @@ static void free_engine(Engine &E)
                     E.d_lzw, E.d_lzq, E.d_lzs, E.d_ssinv, E.d_pcg, E.d_pV, E.d_pr, E.d_pz, E.d_pp, E.d_ps,
                     E.d_pAp, E.d_pg, E.d_pu, E.d_py, E.d_pu2, E.d_py2, E.d_rseed, E.d_rstep,
                     E.d_lubc_ptr, E.d_lubc_nbr, E.d_lub_pairs, E.d_pS, E.d_pP, E.d_py_[0], E.d_py_[1], E.d_py_[2],
-                    E.d_py_[3], E.d_py_[4], E.d_ppart, E.d_scan_sums};
+                    E.d_py_[3], E.d_py_[4], E.d_ppart, E.d_scan_sums, E.d_sv[0], E.d_sv[1], E.d_sv[2],
+                    E.d_sv[3], E.d_sv[4], E.d_sbead[0], E.d_sbead[1], E.d_ppart2, E.d_pmr,
+                    E.d_pmp[0], E.d_pmp[1], E.d_pmp[2], E.d_pmp[3], E.d_pmp[4], E.d_pmp[5], E.d_pmp[6],
+                    E.d_pmp[7], E.d_pmp[8], E.d_pmp[9], E.d_pms[0], E.d_pms[1], E.d_pms[2], E.d_pms[3],
+                    E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8]};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -142,7 +146,11 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         if (s.shell_schur) { s.schur_off = (int)schur; schur += (long)s.nc11 * s.nc11; schur_reps.push_back(r); }
         if (d.Nc > 0) {
             if (s.nc5 <= 64) { ss_reps.push_back(r); s.ss_off = (int)ssinv; ssinv += (long)s.nc5 * s.nc5; }
-            else ss_polish++;
+            else { ss_polish++; E.any_indef = true; }   // colloid suspensions: far-field FTS indefinite near contact
+        }
+        // the reference's own monomer pair scalars make the far-field mobility indefinite
+        if (d.mm_HI && ((d.Nm >= 2 && d.aa_mode == PS_AA_REFERENCE) || (d.Nm >= 1 && d.Nc >= 1 && d.ab_mode == PS_AB_REFERENCE))) {
+            E.any_indef = true;
         }
         // tiles
         s.n_mtiles = (d.Nm + TR - 1) / TR;
@@ -321,7 +329,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
                           &E.d_luby, &E.d_lub_diag, &E.d_tmp_vel, &E.d_tmp_vel2};
     for (double **p : velbufs) TRY_ALLOC(*p, sizeof(double) * vel);
     // lubricated structured solve
-    if (E.any_lub) {
+    if (E.any_lub || ss_polish) {
         E.n_ssinv = ssinv;
         TRY_ALLOC(E.d_ssinv, sizeof(double) * std::max<long>(ssinv, 1));
         TRY_ALLOC(E.d_pcg, sizeof(ps::PcgScal) * R);
@@ -331,6 +339,10 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         for (double **p : pt) TRY_ALLOC(*p, sizeof(double) * top);
         if ((rc = ps::build_red_table(E, E.red_vel, 2))) return rc;
         if ((rc = ps::build_red_table(E, E.red_bead, 3))) return rc;
+        for (auto &p : E.d_sv) TRY_ALLOC(p, sizeof(double) * top);
+        for (auto &p : E.d_sbead) TRY_ALLOC(p, sizeof(double) * bead);
+        for (auto &p : E.d_pms) TRY_ALLOC(p, sizeof(double) * top);
+        TRY_ALLOC(E.d_pmr, sizeof(ps::MinresScal) * R);
     }
     // Lanczos
     if (E.any_mmhi) {

@@ -16,10 +16,10 @@
 // the system is solved in pair space by preconditioned CG (pair_solve below),
 // with the same exact elimination of the stresslets and velocities around it.
 //
-// Replicas with more than 12 colloids (M_SS not solved densely), and replicas
-// whose CG breaks down because Mr is not positive definite (the reference's
-// own monomer pair scalars make M indefinite), take the result as the warm
-// start of a MINRES polish.
+// Replicas with more than 12 colloids (M_SS not solved densely) keep the
+// stresslets as CG unknowns in the same solve.  Replicas whose CG breaks down
+// because M is not positive definite (the reference's own monomer pair scalars
+// make it indefinite) take the result as the warm start of a MINRES polish.
 #include <cmath>
 #include <vector>
 #include "ps_internal.h"
@@ -198,11 +198,11 @@ __global__ void k_ss_inverse(const Seg *__restrict__ segs, const int *__restrict
 // stresslet block; layouts: 0 saddle vector, 1 mobility vector
 __global__ void k_ss_apply(const Seg *__restrict__ segs, const int *__restrict__ reps, const double *__restrict__ ssinv,
                            const double *__restrict__ a, int la, double ca, const double *__restrict__ b, int lb,
-                           double cb, double *__restrict__ out, int lo, const PcgScal *__restrict__ pc)
+                           double cb, double *__restrict__ out, int lo, const char *__restrict__ done, int dstride)
 {
     __shared__ double in[SS_MAX];
     const int r = reps[blockIdx.x];
-    if (pc && pc[r].done) return;
+    if (done && *(const int *)(done + (long)r * dstride)) return;
     const Seg &s = segs[r];
     const int n = s.nc5;
     const long oa = (la == 0 ? s.vec_off : s.top_off) + s.nm3nc6, ob = (lb == 0 ? s.vec_off : s.top_off) + s.nm3nc6;
@@ -234,9 +234,9 @@ __global__ void k_pcg_start(RedTable T, const Seg *__restrict__ segs, const doub
         const Seg &s = segs[B.rep];
         PcgScal p = {};
         p.tol = rtol * sqrt(tot[0]);
-        // replicas whose stresslet block is not dense-solved are left to the MINRES polish
-        p.done = (s.Nc > 0 && s.ss_off < 0) ? 1 : 0;
-        p.reason = p.done ? -1 : 0;
+        (void)s;
+        p.done = 0;
+        p.reason = 0;
         pc[B.rep] = p;
     }
 }
@@ -269,11 +269,26 @@ __global__ void k_pcg_g(RedTable T, const Seg *__restrict__ segs, const double *
 // residual is [0 ; 0 ; L r_y]: CG stops on ||D^{-1} L r_y|| <= rtol ||D^{-1} b||,
 // the MINRES test of the same system.
 //
+// Replicas with more than 12 colloids (no dense M_SS inverse) keep the
+// stresslets as unknowns beside y: with F_t = -b_bot + L y the system in (y, F_S)
+//     [ I + L^T M_tt L   L^T M_tS ] [ y  ]   [ L^T (b_tt + M_tt b_bot) ]
+//     [ M_St L           M_SS     ] [F_S ] = [ b_S + M_St b_bot        ]
+// is SPD too (J + P^T M P with P = diag(L, I)); each iteration costs one plain M
+// apply, the stresslet part is preconditioned by the inverse self block, and the
+// saddle residual is [0 ; r_S ; L r_y].  This covers colloid suspensions of any
+// size, with or without lubrication.
+//
 // Pair vectors hold 12 entries per canonical pair q (monomer pairs use the
 // first 6); pair-space sums run over the bead reduction table, each pair
-// attributed to its lower bead.
+// attributed to its lower bead, and stresslet sums per colloid bead.
 
 constexpr int PS_THREADS = 64;
+
+// per-replica done flag at done + r * stride (CG or MINRES scalars); null: none done
+__device__ __forceinline__ bool rep_done(const char *done, int stride, int r)
+{
+    return done && *(const int *)(done + (long)r * stride);
+}
 
 // velocity DOFs of the pair in pair-DOF order: U_lo, U_hi, W_lo, W_hi
 __device__ __forceinline__ void pair_dofs(const Seg &s, long lo, long hi, bool mono, int dof[12], int &nd)
@@ -443,12 +458,13 @@ __global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, cons
                        const int *__restrict__ sptr, const int *__restrict__ snbr, const int *__restrict__ cptr,
                        const int *__restrict__ cnbr, const double *__restrict__ S, const double *__restrict__ y,
                        const double *__restrict__ add, double *__restrict__ vel, double *__restrict__ top,
-                       const double *__restrict__ D, double *__restrict__ bead_part, const PcgScal *__restrict__ pc)
+                       const double *__restrict__ D, double *__restrict__ bead_part, const char *__restrict__ done,
+                       int dstride)
 {
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     const int r = rep_of_b(bead_offs, R, b);
-    if (pc && pc[r].done) return;
+    if (rep_done(done, dstride, r)) return;
     const Seg &s = segs[r];
     const int i = (int)(b - s.bead_off);
     const bool mono = i < s.Nm;
@@ -495,13 +511,13 @@ __global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *_
                         const Seg *__restrict__ segs, const double *__restrict__ S, const double *__restrict__ y,
                         const double *__restrict__ y2, const double *__restrict__ addv, double sign,
                         const double *__restrict__ p, double *__restrict__ w, double *__restrict__ part,
-                        const PcgScal *__restrict__ pc)
+                        const char *__restrict__ done, int dstride)
 {
     long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npair) return;
     const long lo = pairs[q].x, hi = pairs[q].y;
     const int r = rep_of_b(bead_offs, R, lo);
-    if (pc && pc[r].done) return;
+    if (rep_done(done, dstride, r)) return;
     const Seg &s = segs[r];
     const bool mono = (lo - s.bead_off) < s.Nm;
     int dof[12], nd;
@@ -581,10 +597,13 @@ __global__ void k_ps_dir(long npair, const int2 *__restrict__ pairs, const int *
     for (int a = 0; a < 12; a++) pv[12 * q + a] = zv[12 * q + a] + sc.beta * pv[12 * q + a];
 }
 
-// per-replica sums over the bead table: pair partials by lower bead, bead partials.
+// per-replica sums over the bead table: pair partials by lower bead plus the
+// per-bead stresslet partials (add0), and the per-bead residual partials
+// (bead_part + add1).
 // mode 0: alpha = rz / sum(part);  mode 1: first check (rz, err);  mode 2: iteration check
 __global__ void k_ps_reduce(RedTable T, const int *__restrict__ cptr, const double *__restrict__ part,
-                            const double *__restrict__ bead_part, PcgScal *pc, int mode, int maxit, int *nactive)
+                            const double *__restrict__ bead_part, const double *__restrict__ add0,
+                            const double *__restrict__ add1, PcgScal *pc, int mode, int maxit, int *nactive)
 {
     __shared__ double sh[RB_THREADS / 32][2];
     const RBlk B = T.d_blk[blockIdx.x];
@@ -593,7 +612,9 @@ __global__ void k_ps_reduce(RedTable T, const int *__restrict__ cptr, const doub
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
         long b = B.start + e;
         for (int q = cptr[b]; q < cptr[b + 1]; q++) v[0] += part[q];
+        if (add0) v[0] += add0[b];
         if (bead_part) v[1] += bead_part[b];
+        if (add1) v[1] += add1[b];
     }
     block_sum<2>(v, sh);
     double tot[2];
@@ -658,6 +679,68 @@ __global__ void k_ps_ft(RedTable T, const Seg *__restrict__ segs, const double *
     }
 }
 
+// stresslet unknowns of the joint replicas (Nc > 0 without a dense M_SS
+// inverse), one thread per bead; vectors in mobility layout (S part), with
+// the inverse self block (1.8 I, 0.9 coupling of components 0 and 4) as the
+// preconditioner.  mode 0 init (r = b_S + y_S), 1 Ap = y_S, 2 update, 3 direction,
+// 4 finish (F_S into u and the solution).  Per-bead partials: a0 (r.z or p.Ap),
+// a1 (||D^{-1} r_S||^2); zero for every other bead.
+__global__ void k_ps_S(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs, int mode,
+                       const PcgScal *__restrict__ pc, const double *__restrict__ b, const double *__restrict__ y,
+                       const double *__restrict__ D, double *__restrict__ yS, double *__restrict__ rS,
+                       double *__restrict__ zS, double *__restrict__ pS, double *__restrict__ ApS,
+                       double *__restrict__ u, double *__restrict__ x, double *__restrict__ a0, double *__restrict__ a1)
+{
+    long bd = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (bd >= ntot) return;
+    const int r = rep_of_b(bead_offs, R, bd);
+    const Seg &s = segs[r];
+    const int i = (int)(bd - s.bead_off);
+    const bool joint = s.Nc > 0 && s.ss_off < 0 && i >= s.Nm;
+    if (mode != 4 && pc[r].done) return;
+    if (!joint) {
+        if (mode <= 2) { if (a0) a0[bd] = 0.0; if (a1) a1[bd] = 0.0; }
+        return;
+    }
+    const int c = i - s.Nm;
+    const long t0 = (long)s.top_off + s.nm3nc6 + 5 * c;       // S entries in mobility layout
+    const long v0 = (long)s.vec_off + s.nm3nc6 + 5 * c;       // S rows of the saddle vector
+    const double det = 1.8 * 1.8 - 0.9 * 0.9;
+    double dot = 0.0, nrm = 0.0;
+    if (mode == 0 || mode == 2) {
+        double rv[5], zv[5];
+        for (int k = 0; k < 5; k++) {
+            if (mode == 0) { rv[k] = b[v0 + k] + y[t0 + k]; yS[t0 + k] = 0.0; }
+            else {
+                const double al = pc[r].alpha;
+                yS[t0 + k] += al * pS[t0 + k];
+                rv[k] = rS[t0 + k] - al * ApS[t0 + k];
+            }
+            rS[t0 + k] = rv[k];
+        }
+        zv[0] = (1.8 * rv[0] - 0.9 * rv[4]) / det;
+        zv[4] = (1.8 * rv[4] - 0.9 * rv[0]) / det;
+        for (int k = 1; k < 4; k++) zv[k] = rv[k] / 1.8;
+        for (int k = 0; k < 5; k++) {
+            zS[t0 + k] = zv[k];
+            dot += rv[k] * zv[k];
+            double t = rv[k] / D[v0 + k];
+            nrm += t * t;
+            if (mode == 0) { pS[t0 + k] = zv[k]; u[t0 + k] = zv[k]; }
+        }
+        a0[bd] = dot;
+        a1[bd] = nrm;
+    } else if (mode == 1) {
+        for (int k = 0; k < 5; k++) { double ap = y[t0 + k]; ApS[t0 + k] = ap; dot += pS[t0 + k] * ap; }
+        a0[bd] = dot;
+    } else if (mode == 3) {
+        const double be = pc[r].beta;
+        for (int k = 0; k < 5; k++) { double p = zS[t0 + k] + be * pS[t0 + k]; pS[t0 + k] = p; u[t0 + k] = p; }
+    } else {
+        for (int k = 0; k < 5; k++) { u[t0 + k] = yS[t0 + k]; x[v0 + k] = yS[t0 + k]; }
+    }
+}
+
 // Mr applied to the force rows held in E.d_pu (stresslet part zero):
 // d_py = M [u ; 0], d_pu2 = [0 ; -M_SS^{-1} (d_py)_S], d_py2 = M d_pu2
 static void mr_apply(Engine &E, bool fp32, const void *dn, int ds, cudaStream_t st)
@@ -665,32 +748,323 @@ static void mr_apply(Engine &E, bool fp32, const void *dn, int ds, cudaStream_t 
     apply_operator(E, 1, E.d_pu, E.d_py, nullptr, fp32, st, dn, ds);
     if (E.n_ss_reps) {
         ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, E.d_py, 1, -1.0,
-                                                                 nullptr, 1, 0.0, E.d_pu2, 1,
-                                                                 dn ? E.d_pcg : nullptr);
+                                                                 nullptr, 1, 0.0, E.d_pu2, 1, (const char *)dn, ds);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, dn, ds, true);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Pair-space MINRES, for replica sets whose far-field mobility may be
+// indefinite (colloid pairs near contact: the far-field FTS mobility is not
+// positive definite there; the reference's own monomer pair scalars).  The
+// operator and preconditioner are those of the CG above; the recurrences are
+// Paige & Saunders' preconditioned MINRES as in krylov.cu, with PETSc's test on
+// the preconditioned residual estimate (np * prod |s_k| <= rtol * np_0).
+// Vectors live in the two storages of the pair space: 12 entries per pair, and
+// the stresslet entries of the joint replicas' colloids (mobility layout).
+struct PMVec { double *pair; double *s; };
+struct PMArgs {
+    PMVec R[3], W[3], v, z, x;
+    const double *Az;          // operator output, pair storage (S part: y_S of the apply)
+    const double *y;           // the apply's output (mobility layout)
+    double *u;                 // the apply's input (mobility layout): its S part gets z_S
+    const double *P;           // pair preconditioner blocks
+    double *part, *part2;      // per-pair partials
+    double *sA, *sB;           // per-bead partials
+};
+
+__device__ __forceinline__ void s_precond(const double r[5], double z[5])
+{
+    const double det = 1.8 * 1.8 - 0.9 * 0.9;
+    z[0] = (1.8 * r[0] - 0.9 * r[4]) / det;
+    z[4] = (1.8 * r[4] - 0.9 * r[0]) / det;
+    for (int k = 1; k < 4; k++) z[k] = r[k] / 1.8;
+}
+
+// one thread per pair (t < npair) or per bead (t - npair; stresslet entries of
+// joint-replica colloids, nothing for other beads).
+// mode 0 init, 1 alpha (pending w/x update, v = z/beta, Av), 2 beta (r_{k+1}, z = P r), 3 flush
+__global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs,
+                          int R, const Seg *__restrict__ segs, const MinresScal *__restrict__ mr, int mode, int k,
+                          PMArgs A)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool is_pair = t < npair;
+    if (t >= npair + ntot) return;
+    long base, bead;
+    int n;
+    double *u_s = nullptr;
+    const double *y_s = nullptr;
+    if (is_pair) {
+        base = 12 * t;
+        n = 12;
+        bead = pairs[t].x;
+    } else {
+        bead = t - npair;
+        const Seg &s0 = segs[rep_of_b(bead_offs, R, bead)];
+        const int i = (int)(bead - s0.bead_off);
+        if (!(s0.Nc > 0 && s0.ss_off < 0 && i >= s0.Nm)) {
+            if (mode <= 2) { A.sA[bead] = 0.0; A.sB[bead] = 0.0; }
+            return;
+        }
+        base = (long)s0.top_off + s0.nm3nc6 + 5 * (i - s0.Nm);
+        n = 5;
+        u_s = A.u + base;
+        y_s = A.y + base;
+    }
+    const int r = rep_of_b(bead_offs, R, bead);
+    const MinresScal m = mr[r];
+    auto V = [&](const PMVec &p) { return (is_pair ? p.pair : p.s) + base; };
+    double dot0 = 0.0, dot1 = 0.0;
+    if (mode == 0) {
+        double rv[12], zv[12];
+        double *rr = V(A.R[1]);
+        for (int a = 0; a < n; a++) rv[a] = rr[a];
+        if (is_pair) {
+            const double *Pq = A.P + 144L * t;
+            for (int a = 0; a < 12; a++) {
+                double acc = 0.0;
+                for (int c = 0; c < 12; c++) acc += Pq[a * 12 + c] * rv[c];
+                zv[a] = acc;
+            }
+        } else {
+            s_precond(rv, zv);
+        }
+        double *zz = V(A.z), *xx = V(A.x), *vv = V(A.v), *w0 = V(A.W[0]), *w1 = V(A.W[1]), *w2 = V(A.W[2]);
+        for (int a = 0; a < n; a++) {
+            zz[a] = zv[a]; xx[a] = 0.0; vv[a] = 0.0; w0[a] = 0.0; w1[a] = 0.0; w2[a] = 0.0;
+            dot0 += rv[a] * zv[a];
+            dot1 += zv[a] * zv[a];
+            if (u_s) u_s[a] = zv[a];
+        }
+    } else if (mode == 1 || mode == 3) {
+        double *vv = V(A.v);
+        if (m.pending) {
+            double *wn = V(A.W[(k + 2) % 3]);
+            const double *w1 = V(A.W[k % 3]), *w2 = V(A.W[(k + 1) % 3]);
+            double *xx = V(A.x);
+            for (int a = 0; a < n; a++) {
+                double w = (vv[a] - m.up_oldeps * w1[a] - m.up_delta * w2[a]) * m.up_ginv;
+                wn[a] = w;
+                xx[a] += m.up_phi * w;
+            }
+        }
+        if (mode == 1 && !m.done) {
+            const double *zz = V(A.z);
+            const double *az = is_pair ? A.Az + base : y_s;
+            double *av = V(A.R[(k + 1) % 3]);
+            const double *rm1 = V(A.R[(k + 2) % 3]);
+            const double c1 = (k >= 2) ? m.beta / m.oldb : 0.0;
+            for (int a = 0; a < n; a++) {
+                double vq = zz[a] * m.sinv;
+                double x = m.sinv * az[a];
+                if (k >= 2) x -= c1 * rm1[a];
+                vv[a] = vq;
+                av[a] = x;
+                dot0 += vq * x;
+            }
+        }
+    } else if (mode == 2 && !m.done) {
+        double *av = V(A.R[(k + 1) % 3]);
+        const double *rk = V(A.R[k % 3]);
+        const double c2 = m.alfa / m.beta;
+        double rv[12], zv[12];
+        for (int a = 0; a < n; a++) { rv[a] = av[a] - c2 * rk[a]; av[a] = rv[a]; }
+        if (is_pair) {
+            const double *Pq = A.P + 144L * t;
+            for (int a = 0; a < 12; a++) {
+                double acc = 0.0;
+                for (int c = 0; c < 12; c++) acc += Pq[a * 12 + c] * rv[c];
+                zv[a] = acc;
+            }
+        } else {
+            s_precond(rv, zv);
+        }
+        double *zz = V(A.z);
+        for (int a = 0; a < n; a++) {
+            zz[a] = zv[a];
+            dot0 += rv[a] * zv[a];
+            if (u_s) u_s[a] = zv[a];
+        }
+    }
+    if (mode <= 2) {
+        if (is_pair) { A.part[t] = dot0; A.part2[t] = dot1; }
+        else { A.sA[bead] = dot0; A.sB[bead] = dot1; }
+    }
+}
+
+// per-replica MINRES scalar updates over the bead table (pair partials by lower bead)
+__global__ void k_pm_reduce(RedTable T, const int *__restrict__ cptr, const double *__restrict__ part,
+                            const double *__restrict__ part2, const double *__restrict__ sA,
+                            const double *__restrict__ sB, MinresScal *mr, int mode, int maxit, double rtol,
+                            int *nactive)
+{
+    __shared__ double sh[RB_THREADS / 32][2];
+    const RBlk B = T.d_blk[blockIdx.x];
+    const MinresScal m0 = mr[B.rep];
+    if (mode != 1 && m0.done) return;
+    if (mode == 1 && m0.done && !m0.pending) return;
+    double v[2] = {0.0, 0.0};
+    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
+        long b = B.start + e;
+        for (int q = cptr[b]; q < cptr[b + 1]; q++) { v[0] += part[q]; v[1] += part2[q]; }
+        v[0] += sA[b];
+        v[1] += sB[b];
+    }
+    block_sum<2>(v, sh);
+    double tot[2];
+    if (!finish_block<2>(T, B, blockIdx.x, v, tot)) return;
+    MinresScal m = m0;
+    if (mode == 0) {
+        m = MinresScal{};
+        double np0 = sqrt(tot[1]);
+        m.np = np0;
+        m.ttol = fmax(rtol * np0, 1e-50);
+        if (tot[0] < 0) { m.done = 1; m.reason = -8; }
+        else if (np0 <= m.ttol || tot[0] == 0.0) { m.done = 1; m.reason = 2; }
+        else {
+            m.beta = sqrt(tot[0]); m.phibar = m.beta; m.cs = -1; m.sn = 0; m.sinv = 1.0 / m.beta;
+        }
+        if (m.done) atomicSub(nactive, 1);
+    } else if (mode == 1) {
+        if (m.pending) m.pending = 0;
+        if (!m.done) m.alfa = tot[0];
+    } else {
+        m.it += 1;
+        double bb = tot[0];
+        m.oldb = m.beta;
+        if (bb < 0) {
+            m.done = 1; m.reason = -8;
+        } else {
+            m.beta = sqrt(bb);
+            double oldeps = m.epsln;
+            double delta = m.cs * m.dbar + m.sn * m.alfa;
+            double gbar = m.sn * m.dbar - m.cs * m.alfa;
+            m.epsln = m.sn * m.beta;
+            m.dbar = -m.cs * m.beta;
+            double gamma = sqrt(gbar * gbar + m.beta * m.beta);
+            if (gamma < 2.2250738585072014e-308) gamma = 2.2250738585072014e-308;
+            m.cs = gbar / gamma;
+            m.sn = m.beta / gamma;
+            double phi = m.cs * m.phibar;
+            m.phibar = m.sn * m.phibar;
+            m.up_oldeps = oldeps; m.up_delta = delta; m.up_ginv = 1.0 / gamma; m.up_phi = phi;
+            m.pending = 1;
+            m.np = m.np * fabs(m.sn);
+            if (m.np <= m.ttol) { m.done = 1; m.reason = 2; }
+            else if (m.beta == 0.0) { m.done = 1; m.reason = 3; }
+            else if (m.it >= maxit) { m.done = 1; m.reason = -3; }
+            m.sinv = m.beta != 0.0 ? 1.0 / m.beta : 0.0;
+        }
+        if (m.done) atomicSub(nactive, 1);
+    }
+    mr[B.rep] = m;
 }
 
 static int ensure_pair_space(Engine &E)
 {
     long need = std::max<long>(E.lub_npairs, 1);
     if (need <= E.pair_cap) return PS_OK;
-    cudaFree(E.d_pS); cudaFree(E.d_pP); cudaFree(E.d_ppart);
+    cudaFree(E.d_pS); cudaFree(E.d_pP); cudaFree(E.d_ppart); cudaFree(E.d_ppart2);
     for (auto &p : E.d_py_) cudaFree(p);
+    for (auto &p : E.d_pmp) cudaFree(p);
     E.pair_cap = need * 3 / 2 + 256;
     PS_CK(cudaMalloc(&E.d_pS, sizeof(double) * 144 * E.pair_cap));
     PS_CK(cudaMalloc(&E.d_pP, sizeof(double) * 144 * E.pair_cap));
     PS_CK(cudaMalloc(&E.d_ppart, sizeof(double) * E.pair_cap));
+    PS_CK(cudaMalloc(&E.d_ppart2, sizeof(double) * E.pair_cap));
     for (auto &p : E.d_py_) PS_CK(cudaMalloc(&p, sizeof(double) * 12 * E.pair_cap));
+    for (auto &p : E.d_pmp) PS_CK(cudaMalloc(&p, sizeof(double) * 12 * E.pair_cap));
+    return PS_OK;
+}
+
+// MINRES iterations of the pair-space system; the setup (pair blocks, g, the
+// u_t = b_bot apply input) has run.  Returns the solution's pair and stresslet
+// storages in *ysol / *ssol.
+static int pair_minres(Engine &E, const double *b, const double *g, int maxit, double rtol, bool fp32,
+                       cudaStream_t st, double **ysol, double **ssol, int *iters)
+{
+    RedTable &TB = E.red_bead;
+    const long npair = E.lub_npairs;
+    const int thr = 128;
+    const unsigned nbp = (unsigned)((std::max<long>(npair, 1) + PS_THREADS - 1) / PS_THREADS);
+    const unsigned nbb = (unsigned)((E.ntot + thr - 1) / thr);
+    const unsigned nbe = (unsigned)((npair + E.ntot + thr - 1) / thr);
+    const char *dn = (const char *)&E.d_pmr[0].done;
+    const int ds = (int)sizeof(MinresScal);
+    PMArgs A;
+    for (int k = 0; k < 3; k++) { A.R[k] = {E.d_pmp[k], E.d_pms[k]}; A.W[k] = {E.d_pmp[3 + k], E.d_pms[3 + k]}; }
+    A.v = {E.d_pmp[6], E.d_pms[6]};
+    A.z = {E.d_pmp[7], E.d_pms[7]};
+    A.x = {E.d_pmp[8], E.d_pms[8]};
+    A.Az = E.d_pmp[9];
+    A.y = E.d_py;
+    A.u = E.d_pu;
+    A.P = E.d_pP;
+    A.part = E.d_ppart; A.part2 = E.d_ppart2;
+    A.sA = E.d_sbead[0]; A.sB = E.d_sbead[1];
+    PS_CK(cudaMemsetAsync(E.d_pmr, 0, sizeof(MinresScal) * E.R, st));
+    // rhs into R[1]: pairs L^T (g + Mr b_bot), stresslets b_S + (M b_bot)_S
+    mr_apply(E, fp32, dn, ds, st);
+    if (npair)
+        ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                              E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, A.R[1].pair,
+                                                              nullptr, dn, ds);
+    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
+                                                  E.d_sv[0], A.R[1].s, E.d_sv[2], E.d_sv[3], E.d_sv[4], E.d_pu,
+                                                  nullptr, A.sA, A.sB);
+    *E.h_nactive = E.R;
+    PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
+    ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                     E.d_pmr, 0, 0, A);
+    ::ps_launch_count++, k_pm_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, A.part, A.part2, A.sA, A.sB,
+                                                                  E.d_pmr, 0, maxit, rtol, E.d_nactive);
+    PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    int nact = *E.h_nactive, k = 0;
+    while (nact > 0 && k < maxit) {
+        for (int j = 0; j < 8 && k < maxit; j++) {
+            k++;
+            // Az = A z: u = [L z_y ; z_S] (z_S already in u), apply, z_y + L^T (...)_t
+            ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
+                                                          E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, A.z.pair,
+                                                          nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds);
+            mr_apply(E, fp32, dn, ds, st);
+            if (npair)
+                ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                                      E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
+                                                                      A.z.pair, E.d_pmp[9], nullptr, dn, ds);
+            ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                             E.d_segs, E.d_pmr, 1, k, A);
+            ::ps_launch_count++, k_pm_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, A.part, A.part2, A.sA,
+                                                                          A.sB, E.d_pmr, 1, maxit, rtol, E.d_nactive);
+            ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                             E.d_segs, E.d_pmr, 2, k, A);
+            ::ps_launch_count++, k_pm_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, A.part, A.part2, A.sA,
+                                                                          A.sB, E.d_pmr, 2, maxit, rtol, E.d_nactive);
+        }
+        PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PS_CK(cudaStreamSynchronize(st));
+        nact = *E.h_nactive;
+    }
+    // the last pending w/x update
+    ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                     E.d_pmr, 3, k + 1, A);
+    PS_CK(cudaGetLastError());
+    *ysol = A.x.pair;
+    *ssol = A.x.s;
+    *iters = k;
     return PS_OK;
 }
 
 static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
-                      cudaStream_t st)
+                      cudaStream_t st, bool minres)
 {
     RedTable &TV = E.red_vel, &TB = E.red_bead;
     const bool fp32 = E.precision == PS_PREC_MIXED;
-    const int maxit = o->maxit > 0 ? o->maxit : 10000;
+    // CG converges in tens of iterations on positive definite far fields; a cap
+    // hands the rare indefinite case to MINRES early
+    const int maxit = minres ? (o->maxit > 0 ? o->maxit : 10000) : std::min(o->maxit > 0 ? o->maxit : 10000, 1000);
     const int check_every = o->check_every > 0 ? o->check_every : 8;
     const long npair = E.lub_npairs;
     const int thr = 128;
@@ -700,6 +1074,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     if (rc) return rc;
     if ((rc = ensure_pair_space(E))) return rc;
     double *yv = E.d_py_[0], *rv = E.d_py_[1], *zv = E.d_py_[2], *pv = E.d_py_[3], *Ap = E.d_py_[4];
+    double *yS = E.d_sv[0], *rS = E.d_sv[1], *zS = E.d_sv[2], *pS = E.d_sv[3], *ApS = E.d_sv[4];
+    double *sA = E.d_sbead[0], *sB = E.d_sbead[1];     // per-bead stresslet partials
     // d_pr (nvel >= ntot doubles) holds the per-bead partials
     double *cvel = E.d_pV, *g = E.d_pg, *tmp = E.d_tmp_vel, *bead_part = E.d_pr;
     const void *dn = &E.d_pcg[0].done;
@@ -717,7 +1093,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
         ::ps_launch_count++, k_ss_inverse<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, E.d_ssinv);
         // g: u2 = [0 ; M_SS^{-1} b_S]
         ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, nullptr,
-                                                                 0, 0.0, E.d_pu2, 1, nullptr);
+                                                                 0, 0.0, E.d_pu2, 1, nullptr, 0);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, nullptr, 0, true);
     }
     ::ps_launch_count++, k_pcg_g<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, E.d_py2, g);
@@ -730,73 +1106,107 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     for (auto &p : hp) nact += !p.done;
     *E.h_nactive = nact;
     PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
-    if (npair && nact) {
-        // rhs = L^T (g + Mr b_bot) ; r = rhs ; z = P r ; p = z
-        mr_apply(E, fp32, dn, ds, st);
-        ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                              E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
-                                                              E.d_pcg);
-        ::ps_launch_count++, k_ps_init<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_pP, yv, rv, zv, pv, E.d_ppart);
-    }
-    // initial residual ||D^{-1} L r||
-    ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
-                                                  E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr, nullptr, nullptr,
-                                                  E.d_D, bead_part, E.d_pcg);
-    ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, E.d_pcg, 1,
-                                                                  maxit, E.d_nactive);
-    PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PS_CK(cudaStreamSynchronize(st));
-    nact = *E.h_nactive;
-    int k = 0;
-    while (nact > 0 && k < maxit) {
-        for (int j = 0; j < check_every && k < maxit; j++, k++) {
-            // Ap = p + L^T Mr L p
-            ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                          E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, pv, nullptr,
-                                                          nullptr, E.d_pu, nullptr, nullptr, E.d_pcg);
+    if (minres) {
+        int nit = 0;
+        rc = pair_minres(E, b, g, maxit, o->rtol, fp32, st, &yv, &yS, &nit);
+        if (rc) return rc;
+    } else {
+        if (nact) {
+            // rhs = L^T (g + Mr b_bot) (joint replicas: Mr -> M, and b_S + (M b_bot)_S) ; r = rhs ; z = P r ; p = z
             mr_apply(E, fp32, dn, ds, st);
-            ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                                  E.d_pS, E.d_py, E.d_py2, nullptr, 1.0, pv, Ap,
-                                                                  E.d_ppart, E.d_pcg);
-            ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, nullptr,
-                                                                          E.d_pcg, 0, maxit, E.d_nactive);
-            ::ps_launch_count++, k_ps_update<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                      E.d_pcg, E.d_pP, pv, Ap, yv, rv, zv, E.d_ppart);
-            ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                          E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr,
-                                                          nullptr, nullptr, E.d_D, bead_part, E.d_pcg);
-            ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part,
-                                                                          E.d_pcg, 2, maxit, E.d_nactive);
-            ::ps_launch_count++, k_ps_dir<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_pcg,
-                                                                   zv, pv);
+            if (npair) {
+                ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                                      E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
+                                                                      (const char *)dn, ds);
+                ::ps_launch_count++, k_ps_init<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_pP, yv, rv, zv, pv, E.d_ppart);
+            }
         }
+        ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
+                                                      yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
+        // initial residual ||D^{-1} L r||^2 + ||D^{-1} r_S||^2
+        ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
+                                                      E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr, nullptr, nullptr,
+                                                      E.d_D, bead_part, (const char *)dn, ds);
+        ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA, sB,
+                                                                      E.d_pcg, 1, maxit, E.d_nactive);
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
         nact = *E.h_nactive;
+        int k = 0;
+        while (nact > 0 && k < maxit) {
+            for (int j = 0; j < check_every && k < maxit; j++, k++) {
+                // Ap = p + L^T Mr L p  (joint replicas: [p_y + L^T (M u)_t ; (M u)_S], u = [L p_y ; p_S])
+                ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
+                                                              E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, pv, nullptr,
+                                                              nullptr, E.d_pu, nullptr, nullptr, (const char *)dn, ds);
+                mr_apply(E, fp32, dn, ds, st);
+                if (npair)
+                    ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                                          E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
+                                                                          pv, Ap, E.d_ppart, (const char *)dn, ds);
+                ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 1, E.d_pcg, b, E.d_py,
+                                                              E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, nullptr);
+                ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, nullptr, sA,
+                                                                              nullptr, E.d_pcg, 0, maxit, E.d_nactive);
+                if (npair)
+                    ::ps_launch_count++, k_ps_update<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                                              E.d_pcg, E.d_pP, pv, Ap, yv, rv, zv,
+                                                                              E.d_ppart);
+                ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
+                                                              E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
+                ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
+                                                              E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr,
+                                                              nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds);
+                ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA,
+                                                                              sB, E.d_pcg, 2, maxit, E.d_nactive);
+                if (npair)
+                    ::ps_launch_count++, k_ps_dir<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                                           E.d_pcg, zv, pv);
+                ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
+                                                              E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
+            }
+            PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PS_CK(cudaStreamSynchronize(st));
+            nact = *E.h_nactive;
+        }
     }
     // F_t = -b_bot + L y (into u_t and the force rows), then U = Mr F_t - g, F_S
     ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
                                                   E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, yv, cvel, tmp, E.d_pu, nullptr,
-                                                  nullptr, nullptr);
+                                                  nullptr, nullptr, 0);
     ::ps_launch_count++, k_ps_ft<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, tmp, x);
+    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
+                                                  yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
     mr_apply(E, fp32, nullptr, 0, st);
     ::ps_launch_count++, k_ps_fin<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_py, E.d_py2, g, x);
     if (E.n_ss_reps)
         ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, E.d_py,
-                                                                 1, -1.0, x, 0, nullptr);
+                                                                 1, -1.0, x, 0, nullptr, 0);
     PS_CK(cudaGetLastError());
-    PS_CK(cudaMemcpyAsync(hp.data(), E.d_pcg, sizeof(PcgScal) * E.R, cudaMemcpyDeviceToHost, st));
-    PS_CK(cudaStreamSynchronize(st));
     int worst = 1000, itmax = 0;
     long itsum = 0;
     double emax = 0;
-    for (auto &p : hp) {
-        if (p.reason == -1) continue;               // left to the polish
-        int reason = p.done ? p.reason : -3;
-        worst = std::min(worst, reason);
-        itmax = std::max(itmax, p.it);
-        itsum += p.it;
-        emax = std::max(emax, p.err);
+    if (minres) {
+        std::vector<MinresScal> hm(E.R);
+        PS_CK(cudaMemcpyAsync(hm.data(), E.d_pmr, sizeof(MinresScal) * E.R, cudaMemcpyDeviceToHost, st));
+        PS_CK(cudaStreamSynchronize(st));
+        for (auto &m : hm) {
+            int reason = m.done ? m.reason : -3;
+            worst = std::min(worst, reason);
+            itmax = std::max(itmax, m.it);
+            itsum += m.it;
+            emax = std::max(emax, m.np);
+        }
+    } else {
+        PS_CK(cudaMemcpyAsync(hp.data(), E.d_pcg, sizeof(PcgScal) * E.R, cudaMemcpyDeviceToHost, st));
+        PS_CK(cudaStreamSynchronize(st));
+        for (auto &p : hp) {
+            int reason = p.done ? p.reason : -3;
+            worst = std::min(worst, reason);
+            itmax = std::max(itmax, p.it);
+            itsum += p.it;
+            emax = std::max(emax, p.err);
+        }
     }
     if (worst == 1000) worst = 2;
     if (res) { res->reason = worst; res->iters_max = itmax; res->iters_sum = itsum; res->rnorm_max = emax; }
@@ -806,14 +1216,20 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
 int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
                      cudaStream_t st)
 {
-    if (E.any_lub) {
+    if (E.any_lub || E.n_ss_polish) {
         ps_ksp_result r0 = {2, 0, 0, 0.0};
-        int rc = pair_solve(E, b, x, o, &r0, st);
+        int rc = pair_solve(E, b, x, o, &r0, st, E.any_indef);
         if (rc) return rc;
-        // replicas beyond the dense stresslet limit, and any whose PCG broke down
-        // (an indefinite far-field mobility: the reference's own pair scalars),
-        // finish with MINRES from the PCG iterate
-        if (E.n_ss_polish || r0.reason < 0) {
+        if (r0.reason < 0 && !E.any_indef) {      // CG met an indefinite far field: MINRES on the same system
+            ps_ksp_result r2 = {2, 0, 0, 0.0};
+            if ((rc = pair_solve(E, b, x, o, &r2, st, true))) return rc;
+            r2.iters_max += r0.iters_max;
+            r2.iters_sum += r0.iters_sum;
+            r0 = r2;
+        }
+        // replicas whose CG broke down (an indefinite far-field mobility: the
+        // reference's own pair scalars) finish with MINRES from the CG iterate
+        if (r0.reason < 0) {
             ps_ksp_opts po = *o;
             po.warm = 1;
             po.method = PS_SOLVE_MINRES;
