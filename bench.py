@@ -62,10 +62,16 @@ def parse():
     ap.add_argument("--err-sample", type=int, default=16, help="replicas of the mixed-vs-FP64 error check (0: skip)")
     ap.add_argument("--no-fp64-batched", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="N > 1: weak = one seeded ensemble per rank; strong = one ensemble split across ranks (LPT)")
     return ap.parse_args()
 
 
-def workload(args, rank=0):
+def workload(args, rank=0, world=1):
+    if args.scaling == "strong" and world > 1:
+        from polystokes_brownian_b200 import shard
+        systems, name = workload(args, 0, 1)
+        return shard.rank_systems(systems, rank, world), name
     seed = args.seed + 1000 * rank
     lub = not args.no_lub
     if args.workload == "ensemble":
@@ -275,7 +281,8 @@ def run_b200(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    systems, name = workload(args, rank)
+    from polystokes_brownian_b200 import shard
+    systems, name = workload(args, rank, world)
     prec = _capi.PS_PREC_MIXED if args.precision == "mixed" else _capi.PS_PREC_FP64
     solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
     b = Batch(systems, precision=prec)
@@ -313,11 +320,9 @@ def run_b200(args):
     launches = int(L.ps_kernel_launches() - launches0)
     xs, _ = b.state()
     finite = bool(torch.isfinite(xs).all().item())
-    tmax = torch.tensor([t_total], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    t_total = float(tmax.item())
-    value = beads * args.steps * world / (t_total * 1e-3)
+    t_total = shard.max_over_ranks(t_total, device="cuda")
+    job_beads = int(shard.sum_over_ranks(beads, device="cuda"))
+    value = job_beads * args.steps / (t_total * 1e-3)
 
     # end to end through the C-ABI with host buffers: H2D positions, step, D2H positions
     xh = torch.empty(3 * b.ntot, dtype=torch.float64, pin_memory=True)
@@ -331,10 +336,8 @@ def run_b200(args):
         _capi.check(L.ps_get_state(b.h, C.c_void_p(xh.data_ptr()), None, b.stream), "ps_get_state")
     e1.record(st)
     e1.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e = beads * args.steps * world / (float(te.item()) * 1e-3)
+    te = shard.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    e2e = job_beads * args.steps / (te * 1e-3)
 
     # roofline of the dominant kernel (monomer-monomer pair kernel), timed live
     u = torch.randn(b.ntop, dtype=torch.float64, device="cuda")
@@ -383,12 +386,14 @@ def run_b200(args):
         lat_sorted = sorted(lat)
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec == _capi.PS_PREC_MIXED else "f64",
+               "scaling": args.scaling, "vs_baseline": None, "dtype": "f32+f64" if prec == _capi.PS_PREC_MIXED else "f64",
                "data": "synthetic",
-               "config": {"workload": name, "replicas": len(systems), "beads": beads, "rtol": args.rtol,
+               "config": {"workload": name, "replicas_per_rank": len(systems), "beads_job": job_beads,
+                          "rtol": args.rtol,
                           "precision": args.precision, "solver": args.solver,
                           "l2": "flushed (256 MB write) before every timed step",
-                          "parallelism": f"independent replicas x{world}, no collective"},
+                          "parallelism": f"independent replicas on {world} GPU(s) ({args.scaling} scaling), "
+                                         "no collective in the step"},
                "latency_ms": {"p50": lat_sorted[len(lat) // 2],
                               "p99": lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))]},
                "iters": iters, "iters_note": "per step: max Krylov iterations of the 5 solves, then the Lanczos "
