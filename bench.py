@@ -137,18 +137,39 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(systems, steps_budget_s=20.0, rtol=1e-6, threads=1):
-    """Oracle (CPU restatement, 1 thread) on a stratified sample of replicas; the
-    per-replica step time is fitted as a N^2 + b N and projected onto the whole
-    workload."""
+def scaled_instances(args):
+    """Smaller instances of a single-system workload (same kind, density and
+    parameters) for the CPU sample: the oracle cannot step the full system in a
+    bounded time."""
+    lub = not args.no_lub
+    if args.workload == "suspension":
+        out = []
+        for n in (24, 48, 72):
+            s = configs.suspension(n=n, seed=args.seed)
+            if lub:
+                s = configs.System(s.name, dict(s.params, lub_on=1, lub_gap=0.5), s.x)
+            out.append(s)
+        return out, "suspensions of 24, 48 and 72 colloids at volume fraction 0.2"
+    if args.workload == "brush":
+        return [configs.brush(nchain=k, nper=32, seed=args.seed) for k in (2, 4, 6)], \
+            "brushes of 2, 4 and 6 chains of 32 beads on the same colloid"
+    return None, None
+
+
+def cpu_baseline(systems, steps_budget_s=20.0, rtol=1e-6, threads=1, sample_systems=None, sample_desc=None):
+    """Oracle (CPU restatement, 1 thread) on a stratified sample of replicas (or
+    on smaller instances of a single-system workload); the per-replica step time
+    is fitted as a N^2 + b N and projected onto the whole workload."""
     from oracle import psoracle as po
     Ns = np.array([s.Np for s in systems])
-    order = np.argsort(Ns)
+    if sample_systems is not None:
+        pool = sample_systems
+    else:
+        pool = [systems[int(i)] for i in np.argsort(Ns)[:: max(1, len(systems) // 12)]]
     # smallest-to-larger sample until the budget is used
     sample, times = [], []
     t_start = time.perf_counter()
-    for idx in order[:: max(1, len(order) // 12)]:
-        s = systems[int(idx)]
+    for s in pool:
         if s.Np > 700 and sample:
             break
         tab = None
@@ -169,10 +190,11 @@ def cpu_baseline(systems, steps_budget_s=20.0, rtol=1e-6, threads=1):
     coef, *_ = np.linalg.lstsq(A, np.array(times), rcond=None)
     coef = np.maximum(coef, 0)
     proj = float(sum(coef[0] * N * N + coef[1] * N for N in Ns))
-    if len(systems) == 1:
+    if len(systems) == 1 and sample_systems is None:
         proj = float(np.mean(times))
     value = float(Ns.sum()) / proj
-    desc = (f"oracle (C restatement) 1 thread, one step of each of {len(sample)} replicas with N in "
+    what = sample_desc or f"{len(sample)} replicas"
+    desc = (f"oracle (C restatement) 1 thread, one step of each of {what}, N in "
             f"[{int(n.min())},{int(n.max())}], step time fitted a*N^2+b*N and projected onto the workload")
     return {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": desc,
             "sample_seconds": float(sum(times))}
@@ -185,7 +207,8 @@ def run_reference(args):
     systems, name = workload(args, 0)
     vals = []
     for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(systems, steps_budget_s=6.0, rtol=args.rtol)
+        ss, sd = scaled_instances(args) if len(systems) == 1 and systems[0].Np > 700 else (None, None)
+        cb = cpu_baseline(systems, steps_budget_s=6.0, rtol=args.rtol, sample_systems=ss, sample_desc=sd)
         if k >= args.warmup:
             vals.append(cb["value"])
     v = float(np.median(vals))
@@ -217,7 +240,8 @@ def plain_fp64(systems, args, budget_s=60.0):
     t_start = time.perf_counter()
     for idx in pick:
         b = Batch([systems[idx]], precision=_capi.PS_PREC_FP64)
-        b.step(rtol=args.rtol, maxit=50000, solver=_capi.PS_SOLVE_MINRES)
+        if len(systems) > 1:      # single large systems: one step, no warm-up (bounded time)
+            b.step(rtol=args.rtol, maxit=50000, solver=_capi.PS_SOLVE_MINRES)
         st = torch.cuda.current_stream()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
@@ -382,7 +406,8 @@ def run_b200(args):
             extra["velocity_error"] = velocity_error(systems, args)
 
     if rank == 0:
-        cb = cpu_baseline(systems, rtol=args.rtol) if world == 1 else None
+        ss, sd = scaled_instances(args) if len(systems) == 1 and systems[0].Np > 700 else (None, None)
+        cb = cpu_baseline(systems, rtol=args.rtol, sample_systems=ss, sample_desc=sd) if world == 1 else None
         lat_sorted = sorted(lat)
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,

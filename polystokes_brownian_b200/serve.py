@@ -254,20 +254,26 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--nmax", type=int, default=16384)
     ap.add_argument("--smax", type=int, default=500)
+    ap.add_argument("--no-lub", action="store_true")
+    ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--rebuild-every", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args()
-    prec = _capi.PS_PREC_MIXED if a.precision == "mixed" else _capi.PS_PREC_FP64
-    trace = make_trace(a.requests, a.rate, seed=a.seed, nmax=a.nmax, smax=a.smax)
-    srv = Server(precision=prec, rebuild_every=a.rebuild_every)
-    t = time.perf_counter()
-    res = srv.run(trace)
-    wall = time.perf_counter() - t
-    print(json.dumps({"requests": len(res), "rate": a.rate, "precision": a.precision, "wall_s": wall,
-                      **srv.stats(res, wall)}))
+    trace = make_trace(a.requests, a.rate, seed=a.seed, nmax=a.nmax, smax=a.smax, lub=not a.no_lub)
+    precs = ["mixed", "fp64"] if a.precision == "both" else [a.precision]
+    out = {"requests": len(trace), "rate": a.rate, "lub": not a.no_lub, "rtol": a.rtol,
+           "bead_steps_requested": int(sum(r.system.Np * r.steps for r in trace))}
+    for name in precs:
+        prec = _capi.PS_PREC_MIXED if name == "mixed" else _capi.PS_PREC_FP64
+        srv = Server(precision=prec, rebuild_every=a.rebuild_every, rtol=a.rtol)
+        t = time.perf_counter()
+        res = srv.run(trace)
+        wall = time.perf_counter() - t
+        out[name] = {"wall_s": wall, **srv.stats(res, wall)}
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":
