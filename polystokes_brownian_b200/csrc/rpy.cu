@@ -513,9 +513,13 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
     if (E.n_ab_tiles)
         ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
                                                          E.d_partBA, done, dstride);
+    // colloid-colloid FTS blocks stay FP64 in the mixed form: near contact the
+    // far-field FTS mobility is ill-conditioned and FP32 blocks leave a 1.2e-6
+    // velocity error on a suspension at gap 0.01 (FP64: tracks rtol); they are
+    // cheap wherever monomers carry the O(N^2) work
     if (E.n_bb_tiles)
-        ::ps_launch_count++, k_rpy_bb<T><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, pos, E.d_pos32lo, u, in_top,
-                                                                         E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
+        ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(
+            E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, in_top, E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
 }
 
 void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st,
@@ -557,8 +561,7 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
             if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
             else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
         } else if (which == 2 && E.n_bb_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_bb<float><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
-            else ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
+            ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
         } else if (which == 3) {
             apply_operator(E, 1, u, E.d_tmp_top2, nullptr, fp32, st);
         }
