@@ -142,13 +142,16 @@ constexpr int AAF_THREADS = 64;
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 // one staged column tile against the thread's two rows; CHECK: the tile may
-// hold the rows themselves or (chain_HI) same-chain partners, which get rinv = 0
+// hold the rows themselves or (chain_HI) same-chain partners, which get rinv = 0.
+// Far form in factored scalars: y = ri (c + d ri^2), (x - y)/r^2 = ri^3 (a + b ri^2),
+// a = c0 - c2, b = c1 - c3, c = c2, d = c3; the near form (r^2 <= (2 beta)^2, taken
+// only when some lane of the warp needs it) overwrites both.
 template <bool CHECK>
 __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const float4 *__restrict__ sB,
                                            const float2 *__restrict__ sC, int jt, int nj, int i0, int i1,
                                            bool chain_hi, float w0, float w1, float2 px, float2 py, float2 pz,
-                                           float2 lx, float2 ly, float2 lz, float2 cx1, float2 cx3, float2 cy1,
-                                           float2 cy3, float nx0, float nx1, float ny0, float ny1, float two_beta,
+                                           float2 lx, float2 ly, float2 lz, float2 fa, float2 fb, float2 fc,
+                                           float2 fd, float nx0, float nx1, float ny0, float ny1, float tb2,
                                            float2 &tx, float2 &ty, float2 &tz)
 {
 #pragma unroll 4
@@ -167,21 +170,27 @@ __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const 
         }
         float2 ri = make_float2(e0 ? 0.f : rsqrtf(r2.x), e1 ? 0.f : rsqrtf(r2.y));
         float2 ri2 = __fmul2_rn(ri, ri);
-        float2 ri3 = __fmul2_rn(ri2, ri);
-        float2 x = __ffma2_rn(cx3, ri3, __fmul2_rn(cx1, ri));
-        float2 y = __ffma2_rn(cy3, ri3, __fmul2_rn(cy1, ri));
-        float2 r = __fmul2_rn(r2, ri);
-        const bool n0 = !e0 && r.x <= two_beta, n1 = !e1 && r.y <= two_beta;
+        float2 yv = __fmul2_rn(__ffma2_rn(fd, ri2, fc), ri);                     // y
+        float2 g = __fmul2_rn(__ffma2_rn(fb, ri2, fa), __fmul2_rn(ri2, ri));    // (x - y) / r^2
+        const bool n0 = !e0 && r2.x <= tb2, n1 = !e1 && r2.y <= tb2;
         if (__any_sync(0xffffffffu, n0 || n1)) {
-            if (n0) { x.x = nx0 + nx1 * r.x; y.x = ny0 + ny1 * r.x; }
-            if (n1) { x.y = nx0 + nx1 * r.y; y.y = ny0 + ny1 * r.y; }
+            if (n0) {
+                float r = r2.x * ri.x, x = nx0 + nx1 * r;
+                yv.x = ny0 + ny1 * r;
+                g.x = (x - yv.x) * ri2.x;
+            }
+            if (n1) {
+                float r = r2.y * ri.y, x = nx0 + nx1 * r;
+                yv.y = ny0 + ny1 * r;
+                g.y = (x - yv.y) * ri2.y;
+            }
         }
         // mob_a u = y u + (x - y)(d.u) d / r^2
         float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(B.w))));
-        float2 f = __fmul2_rn(__fmul2_rn(__fadd2_rn(x, make_float2(-y.x, -y.y)), du), ri2);
-        tx = __ffma2_rn(f, dx, __ffma2_rn(y, f2(B.w), tx));
-        ty = __ffma2_rn(f, dy, __ffma2_rn(y, f2(C.x), ty));
-        tz = __ffma2_rn(f, dz, __ffma2_rn(y, f2(C.y), tz));
+        float2 f = __fmul2_rn(g, du);
+        tx = __ffma2_rn(f, dx, __ffma2_rn(yv, f2(B.w), tx));
+        ty = __ffma2_rn(f, dy, __ffma2_rn(yv, f2(C.x), ty));
+        tz = __ffma2_rn(f, dz, __ffma2_rn(yv, f2(C.y), tz));
     }
 }
 
@@ -209,9 +218,10 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
     const float2 px = make_float2(P0.x, P1.x), py = make_float2(P0.y, P1.y), pz = make_float2(P0.z, P1.z);
     const float2 lx = make_float2(L0.x, L1.x), ly = make_float2(L0.y, L1.y), lz = make_float2(L0.z, L1.z);
     const bool chain_hi = sg.chain_HI != 0;
-    const float2 cx1 = f2(sg.aa_c[0]), cx3 = f2(sg.aa_c[1]), cy1 = f2(sg.aa_c[2]), cy3 = f2(sg.aa_c[3]);
+    const float2 fa = f2(sg.aa_c[0] - sg.aa_c[2]), fb = f2(sg.aa_c[1] - sg.aa_c[3]);
+    const float2 fc = f2(sg.aa_c[2]), fd = f2(sg.aa_c[3]);
     const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
-    const float two_beta = (float)(2.0 * sg.beta);
+    const float tb2 = (float)(4.0 * sg.beta * sg.beta);
     float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), kx = f2(0.f), ky = f2(0.f), kz = f2(0.f);
     for (int jt = j0; jt < j1; jt += 128) {
         const int nj = min(128, j1 - jt);
@@ -228,11 +238,11 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
         // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
         const bool check = chain_hi || (jt < tl.row0 + 2 * AAF_THREADS && jt + nj > tl.row0);
         if (check)
-            aa_f2_cols<true>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, cx1, cx3, cy1,
-                             cy3, nx0, nx1, ny0, ny1, two_beta, tx, ty, tz);
+            aa_f2_cols<true>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, fa, fb, fc,
+                             fd, nx0, nx1, ny0, ny1, tb2, tx, ty, tz);
         else
-            aa_f2_cols<false>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, cx1, cx3, cy1,
-                              cy3, nx0, nx1, ny0, ny1, two_beta, tx, ty, tz);
+            aa_f2_cols<false>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, fa, fb, fc,
+                              fd, nx0, nx1, ny0, ny1, tb2, tx, ty, tz);
         // Kahan across column tiles
         float2 yy, tt;
         yy = __fadd2_rn(tx, make_float2(-kx.x, -kx.y)); tt = __fadd2_rn(sx, yy);
