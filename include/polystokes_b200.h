@@ -46,6 +46,11 @@ extern "C" {
 /* AB translational block mode: reference-faithful or RPY. */
 #define PS_AB_REFERENCE 0
 #define PS_AB_RPY 1
+/* PS_AB_RPY with the overlap and full-overlap branches of the unequal-radii RPY
+ * (Zuk et al. 2014) for the translation and rotation couplings; the stresslet
+ * coupling stays far-field.  The reference carries these branches commented out
+ * (mob.cpp:414-453, mobdat/rpy_kk_mobilities.tex). */
+#define PS_AB_RPY_REG 2
 
 /* Monomer-monomer translation scalars: the reference's own (mob.cpp:122-131)
  * or the equal-sphere RPY of radius beta with its overlap form. */
@@ -77,7 +82,7 @@ typedef struct ps_desc {
     double ktrap, tstart, trun, weaken_trap;
     double t0;          /* start time (restart) */
     int32_t restart;    /* nonzero: trap centres are not re-derived from x */
-    int32_t ab_mode;    /* PS_AB_REFERENCE | PS_AB_RPY */
+    int32_t ab_mode;    /* PS_AB_REFERENCE | PS_AB_RPY | PS_AB_RPY_REG */
     double hs_kpref;    /* HS_KPREF, default 1.0 */
     int32_t hs_kmode;   /* HS_KMODE, default 0 */
     int32_t lanczos_nc; /* POLYSTOKES_LANCZOS_NC, default 64 */
@@ -159,6 +164,29 @@ int ps_get_replica_steps(ps_ctx *ctx, uint64_t *host_steps);
 int ps_get_aux(ps_ctx *ctx, double *time, double *ktrap, double *xpos0, void *stream);
 int ps_set_aux(ps_ctx *ctx, const double *time, const double *ktrap, const double *xpos0, void *stream);
 const char *ps_last_error(void);
+
+/* Trajectory observables accumulated on the device, per replica (the analysis
+ * the reference runs on its output files: bond and trap statistics,
+ * test_sim_dumbbells_thermal.py:178-330; the windowed MSD tensor of the
+ * colloids, get_msd.py:5-28).  Host arrays; NULL members are skipped.
+ *   bond  R x 10: count, sum of bond vectors (3), sum |b|, sum |b|^2,
+ *                 increment count, sum of bond-vector increments between samples (3)
+ *   trap  R x 9:  count, sum of displacements from the trap centre (3), sum |d|,
+ *                 sum |d|^2, sum d_x^2, d_y^2, d_z^2
+ *   bond_hist, trap_hist  R x nbins: counts of |b| in [0, bond_max), |d| in [0, trap_max)
+ *   msd  R x lags x 6: sums over colloids and time origins of dx dx, dy dy, dz dz,
+ *                 dx dy, dx dz, dy dz at lag l samples; msd_count R x lags       */
+typedef struct ps_obs_out {
+    double *bond;
+    uint64_t *bond_hist;
+    double *trap;
+    uint64_t *trap_hist;
+    double *msd;
+    uint64_t *msd_count;
+} ps_obs_out;
+int ps_obs_reset(ps_ctx *ctx, int32_t nbins, double bond_max, double trap_max, int32_t lags);
+int ps_observe(ps_ctx *ctx, void *stream);        /* one sample of the current state */
+int ps_obs_read(ps_ctx *ctx, ps_obs_out *out, void *stream);
 
 /* state --------------------------------------------------------------------- */
 /* x (3 Np per replica), q (4 Nc per replica): device or host pointers; reads

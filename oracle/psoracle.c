@@ -224,12 +224,38 @@ void or_tensor_aa(double r, double rinv, const double e[3], double beta, int mod
 
 /* unequal-radii far-field translation block computed (and left unused) by
  * mobility_AB, mob.cpp:410-411; used only in OR_AB_RPY mode */
-void or_tensor_ab_rpy(double r, double rinv, const double e[3], double beta, double a9[9])
+/* Zuk et al. (2014) unequal-radii RPY, colloid radius 1, monomer radius beta < 1,
+ * in the reference's units (6 pi eta = 1) and sign convention (yb = -mu^rt),
+ * the branches of mob.cpp:414-453 (commented out there) and
+ * mobdat/rpy_kk_mobilities.tex eqs. for mu^tt and mu^rt. */
+void or_ab_reg_scalars(double r, double beta, double *x, double *y, double *yb)
 {
-    (void)r;
-    double ri3 = rinv * rinv * rinv, b2 = beta * beta;
+    double b2 = beta * beta;
+    if (r >= 1.0 + beta) {
+        *x = 1.5 / r - 0.5 * (1.0 + b2) / (r * r * r);
+        *y = 0.75 / r + 0.25 * (1.0 + b2) / (r * r * r);
+        *yb = -0.75 / (r * r);
+    } else if (r > 1.0 - beta) {
+        double rd = 1.0 - beta, r2 = r * r, r3 = r2 * r;
+        double t = rd * rd + 3.0 * r2, u = rd * rd - r2;
+        double I = (16.0 * r3 * (1.0 + beta) - t * t) / (32.0 * r3);
+        *y = I / beta;
+        *x = (I + 3.0 * u * u / (32.0 * r3)) / beta;
+        *yb = -(3.0 / (8.0 * beta)) * (rd + r) * (rd + r) * (b2 + 2.0 * beta * (1.0 + r) - 3.0 * (1.0 - r) * (1.0 - r))
+              / (8.0 * r2);
+    } else {
+        *x = 1.0;
+        *y = 1.0;
+        *yb = -0.75 * r;
+    }
+}
+
+void or_tensor_ab_rpy(double r, double rinv, const double e[3], double beta, int reg, double a9[9])
+{
+    double ri3 = rinv * rinv * rinv, b2 = beta * beta, yb;
     double x = (3. / 2.) * rinv - (1. / 2.) * (1.0 + b2) * ri3;
     double y = (3. / 4.) * rinv + (1. / 4.) * (1.0 + b2) * ri3;
+    if (reg) or_ab_reg_scalars(r, beta, &x, &y, &yb);
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) {
             double ee = e[i] * e[j];
@@ -238,15 +264,15 @@ void or_tensor_ab_rpy(double r, double rinv, const double e[3], double beta, dou
 }
 
 /* monomer-colloid rotation-force and stresslet-force blocks, mob.cpp:455-537 */
-void or_tensor_ab(double r, double rinv, const double e[3], double beta, double b9[9], double gt15[15])
+void or_tensor_ab(double r, double rinv, const double e[3], double beta, int reg, double b9[9], double gt15[15])
 {
-    (void)r;
     double ee[3][3];
     for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) ee[i][j] = e[i] * e[j];
     double ri2 = rinv * rinv, ri3 = ri2 * rinv, ri4 = ri3 * rinv;
     (void)ri3;
     double b2 = beta * beta;
     double y12b = -(3. / 4.) * ri2;
+    if (reg) { double xx, yy; or_ab_reg_scalars(r, beta, &xx, &yy, &y12b); }
     double x12g = (9. / 4.) * ri2 - (9. / 20.) * ri4 * (3 + 5 * b2);
     double y12g = (9. / 10.) * ri4 * ((1. / 2.) + (5. / 6.) * b2);
     for (int i = 0; i < 3; i++)
@@ -633,8 +659,9 @@ void or_mob(or_sim *s)
             for (int c = 0; c < Nc; c++) {
                 const double *pd = pdk(s, mI, Nm + c, NULL);
                 double b[9], g[15], a[9];
-                or_tensor_ab(pd[3], pd[4], pd, s->p.beta, b, g);
-                if (s->p.ab_mode == OR_AB_RPY) or_tensor_ab_rpy(pd[3], pd[4], pd, s->p.beta, a);
+                or_tensor_ab(pd[3], pd[4], pd, s->p.beta, s->p.ab_mode == OR_AB_RPY_REG, b, g);
+                if (s->p.ab_mode != OR_AB_REFERENCE)
+                    or_tensor_ab_rpy(pd[3], pd[4], pd, s->p.beta, s->p.ab_mode == OR_AB_RPY_REG, a);
                 else memset(a, 0, sizeof a);
                 int t = 3 * c, r = s->nc3 + 3 * c, st = s->nc6 + 5 * c, col = 3 * mI;
                 for (int i = 0; i < 3; i++) {
@@ -822,8 +849,9 @@ void or_mobility_apply(const or_sim *s, const double *u, double *y)
         for (int c = 0; c < Nc; c++) {
             const double *pd = pdk(s, m, Nm + c, NULL);
             double B[9], G[15], T[9];
-            or_tensor_ab(pd[3], pd[4], pd, s->p.beta, B, G);
-            if (s->p.ab_mode == OR_AB_RPY) or_tensor_ab_rpy(pd[3], pd[4], pd, s->p.beta, T);
+            or_tensor_ab(pd[3], pd[4], pd, s->p.beta, s->p.ab_mode == OR_AB_RPY_REG, B, G);
+            if (s->p.ab_mode != OR_AB_REFERENCE)
+                or_tensor_ab_rpy(pd[3], pd[4], pd, s->p.beta, s->p.ab_mode == OR_AB_RPY_REG, T);
             else memcpy(T, s->tab, sizeof T);
             int mm = 3 * m, t = nm3 + 3 * c, r = nm3 + s->nc3 + 3 * c, st = s->nm3nc6 + 5 * c;
             for (int a = 0; a < 3; a++) {

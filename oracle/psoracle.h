@@ -28,8 +28,11 @@ extern "C" {
  *                    mob_a left by the last pair tensor evaluated before the AB
  *                    loop (mob.cpp:845-904).
  *   OR_AB_RPY:       the unequal-radii far-field RPY scalars that mobility_AB
- *                    computes but never uses (mob.cpp:410-411).               */
-enum { OR_AB_REFERENCE = 0, OR_AB_RPY = 1 };
+ *                    computes but never uses (mob.cpp:410-411).
+ *   OR_AB_RPY_REG:   OR_AB_RPY plus the overlap / full-overlap branches of the
+ *                    unequal-radii RPY (Zuk et al. 2014) for the translation and
+ *                    rotation couplings, commented out in mob.cpp:414-453.    */
+enum { OR_AB_REFERENCE = 0, OR_AB_RPY = 1, OR_AB_RPY_REG = 2 };
 
 /* Monomer-monomer translation scalars.  OR_AA_REFERENCE: mob.cpp:122-131
  * (x = 3/(8r) - 2/r^3, y = 3/(4r) - 1/(2r^3); overlap x = 3r/8 - 1, y = 1 - 9r/32).
@@ -74,9 +77,11 @@ void    or_set_lub_tables(or_sim *s, const double *tab, int nrow, int ncol);
 
 /* pair tensors (mob.cpp:30-537), outputs as the double the reference stores */
 void or_tensor_aa(double r, double rinv, const double e[3], double beta, int mode, double a[9]);
-void or_tensor_ab(double r, double rinv, const double e[3], double beta,
+void or_tensor_ab(double r, double rinv, const double e[3], double beta, int reg,
                   double b[9], double gt[15]);
-void or_tensor_ab_rpy(double r, double rinv, const double e[3], double beta, double a[9]);
+void or_tensor_ab_rpy(double r, double rinv, const double e[3], double beta, int reg, double a[9]);
+/* regularised translation (x along e, y across) and rotation-translation (yb) scalars */
+void or_ab_reg_scalars(double r, double beta, double *x, double *y, double *yb);
 void or_tensor_bb(double r, double rinv, const double e[3], double a[9], double b[9],
                   double c[9], double gt[15], double ht[15], double m[25]);
 

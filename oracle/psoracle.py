@@ -19,6 +19,7 @@ _lib = None
 
 AB_REFERENCE = 0
 AB_RPY = 1
+AB_RPY_REG = 2
 
 
 class OrParams(C.Structure):
@@ -69,8 +70,9 @@ def lib():
         L.or_sizes.argtypes = [C.c_void_p, I]
         L.or_set_lub_tables.argtypes = [C.c_void_p, P, C.c_int, C.c_int]
         L.or_tensor_aa.argtypes = [C.c_double, C.c_double, P, C.c_double, C.c_int, P]
-        L.or_tensor_ab_rpy.argtypes = [C.c_double, C.c_double, P, C.c_double, P]
-        L.or_tensor_ab.argtypes = [C.c_double, C.c_double, P, C.c_double, P, P]
+        L.or_tensor_ab_rpy.argtypes = [C.c_double, C.c_double, P, C.c_double, C.c_int, P]
+        L.or_tensor_ab.argtypes = [C.c_double, C.c_double, P, C.c_double, C.c_int, P, P]
+        L.or_ab_reg_scalars.argtypes = [C.c_double, C.c_double, P, P, P]
         L.or_tensor_bb.argtypes = [C.c_double, C.c_double, P, P, P, P, P, P, P]
         for f in ("or_check_dist", "or_mob", "or_schur_sync"):
             getattr(L, f).argtypes = [C.c_void_p]
@@ -306,11 +308,11 @@ def tensor_bb(e, r):
     return outs
 
 
-def tensor_ab(e, r, beta):
+def tensor_ab(e, r, beta, reg=0):
     e = np.ascontiguousarray(e, dtype=np.float64)
     b = np.zeros(9)
     g = np.zeros(15)
-    lib().or_tensor_ab(r, 1.0 / r, _p(e), beta, _p(b), _p(g))
+    lib().or_tensor_ab(r, 1.0 / r, _p(e), beta, reg, _p(b), _p(g))
     return b, g
 
 
@@ -321,8 +323,14 @@ def tensor_aa(e, r, beta, mode=0):
     return a
 
 
-def tensor_ab_rpy(e, r, beta):
+def tensor_ab_rpy(e, r, beta, reg=0):
     e = np.ascontiguousarray(e, dtype=np.float64)
     a = np.zeros(9)
-    lib().or_tensor_ab_rpy(r, 1.0 / r, _p(e), beta, _p(a))
+    lib().or_tensor_ab_rpy(r, 1.0 / r, _p(e), beta, reg, _p(a))
     return a
+
+
+def ab_reg_scalars(r, beta):
+    out = [np.zeros(1) for _ in range(3)]
+    lib().or_ab_reg_scalars(r, beta, *[_p(o) for o in out])
+    return tuple(float(o[0]) for o in out)

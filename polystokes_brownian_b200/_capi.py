@@ -70,6 +70,11 @@ class PsStepResult(C.Structure):
                 ("lanczos_nneg", C.c_int32)]
 
 
+class PsObsOut(C.Structure):
+    _fields_ = [("bond", C.c_void_p), ("bond_hist", C.c_void_p), ("trap", C.c_void_p), ("trap_hist", C.c_void_p),
+                ("msd", C.c_void_p), ("msd_count", C.c_void_p)]
+
+
 def declared_symbols(header: str = HEADER) -> list[str]:
     """Names of every function the public header declares."""
     txt = open(header).read()
@@ -100,6 +105,9 @@ def lib():
     L.ps_set_replica_seeds.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.ps_get_replica_steps.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.ps_get_aux.argtypes = [vp, P, P, P, vp]
+    L.ps_obs_reset.argtypes = [vp, C.c_int32, C.c_double, C.c_double, C.c_int32]
+    L.ps_observe.argtypes = [vp, vp]
+    L.ps_obs_read.argtypes = [vp, C.POINTER(PsObsOut), vp]
     L.ps_set_aux.argtypes = [vp, P, P, P, vp]
     L.ps_set_state.argtypes = [vp, P, P, vp]
     L.ps_get_state.argtypes = [vp, P, P, vp]

@@ -225,6 +225,33 @@ def ensemble_member(rng, N: int, beta: float = 1.0 / 3.0, dt: float = 1e-4, pair
     return System(f"ensemble_{N}", params, x)
 
 
+def dumbbells(seed: int = 0, n_db: int = 4, beta: float = 0.3, r0: float = 1.2, kbond: float = 25.0,
+              ktrap: float = 50.0, dt: float = 1e-3, mm_HI: int = 1) -> System:
+    """One trapped colloid at the origin and n_db harmonic dumbbells (two monomers
+    of radius beta at their rest length r0) around it, the setting of the
+    reference's thermal test (test_sim_dumbbells_thermal.py).  RPY pair scalars,
+    so the grand mobility is positive definite and the noise exact."""
+    rng = np.random.default_rng(seed)
+    grid = _Grid(2 * beta)
+    grid.add(np.zeros(3), 1.0)
+    xs = []
+    while len(xs) < 2 * n_db:
+        c = rng.uniform(-6.0, 6.0, size=3)
+        if c @ c < 9.0:
+            continue
+        u = _unit(rng)
+        p0, p1 = c - 0.5 * r0 * u, c + 0.5 * r0 * u
+        if grid.clear(p0, beta, 2.5 * beta) and grid.clear(p1, beta, 2.5 * beta):
+            grid.add(p0, beta)
+            grid.add(p1, beta)
+            xs += [p0, p1]
+    x = np.vstack([np.array(xs), np.zeros((1, 3))])
+    params = make_params(Nm=2 * n_db, Nc=1, Npoly=n_db, Nmono_per_chain=2, beta=beta, kT=1.0, kbond=kbond, r0=r0,
+                         Lmax=10 * r0, dt=dt, mm_HI=mm_HI, chain_HI=0, fene=0, ktrap=ktrap, tstart=0.0, trun=1e9,
+                         aa_mode=1, ab_mode=1)
+    return System("dumbbells", params, x)
+
+
 def ensemble(n_rep: int = 256, seed: int = 0, nmin: int = 64, nmax: int = 4096, **kw) -> list[System]:
     rng = np.random.default_rng(seed)
     Ns = np.rint(np.exp(rng.uniform(math.log(nmin), math.log(nmax), size=n_rep))).astype(int)

@@ -67,7 +67,8 @@ static void free_engine(Engine &E)
                     E.d_sv[3], E.d_sv[4], E.d_sbead[0], E.d_sbead[1], E.d_ppart2, E.d_pmr,
                     E.d_pmp[0], E.d_pmp[1], E.d_pmp[2], E.d_pmp[3], E.d_pmp[4], E.d_pmp[5], E.d_pmp[6],
                     E.d_pmp[7], E.d_pmp[8], E.d_pmp[9], E.d_pms[0], E.d_pms[1], E.d_pms[2], E.d_pms[3],
-                    E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8]};
+                    E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8], E.d_obs_acc, E.d_obs_prev,
+                    E.d_obs_ring, E.d_obs_msd, E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.d_obs_msdn};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -469,6 +470,24 @@ int ps_set_aux(ps_ctx *ctx, const double *time, const double *ktrap, const doubl
     if (xpos0 && E.ncoll) PS_CK(cudaMemcpyAsync(E.d_xpos0, xpos0, sizeof(double) * 3 * E.ncoll, cudaMemcpyDefault, st));
     PS_CK(cudaStreamSynchronize(st));
     return PS_OK;
+}
+
+int ps_obs_reset(ps_ctx *ctx, int32_t nbins, double bond_max, double trap_max, int32_t lags)
+{
+    if (!ctx) return PS_ERR_ARG;
+    return ps::obs_reset(ctx->E, nbins, bond_max, trap_max, lags);
+}
+
+int ps_observe(ps_ctx *ctx, void *stream)
+{
+    if (!ctx) return PS_ERR_ARG;
+    return ps::obs_sample(ctx->E, S(stream));
+}
+
+int ps_obs_read(ps_ctx *ctx, ps_obs_out *out, void *stream)
+{
+    if (!ctx || !out) return PS_ERR_ARG;
+    return ps::obs_read(ctx->E, out, S(stream));
 }
 
 int ps_get_replica_steps(ps_ctx *ctx, uint64_t *steps)

@@ -243,6 +243,40 @@ __device__ __forceinline__ void bb_apply(const T e[3], T r, T rinv, bool is_lo, 
     }
 }
 
+// Monomer-colloid translation scalars (x along e, y across) and, for the
+// regularised mode, the rotation-translation scalar yb.  Colloid radius 1,
+// monomer radius beta < 1, units 6 pi eta = 1.
+//   r >= 1 + beta (far):   x = 3/(2r) - (1+b^2)/(2r^3), y = 3/(4r) + (1+b^2)/(4r^3)
+//   1 - beta < r < 1 + beta (overlap, Zuk et al. eq. 3.1/3.3 middle):
+//     t = (1-b)^2 + 3r^2, u = (1-b)^2 - r^2, I = (16 r^3 (1+b) - t^2)/(32 r^3)
+//     y = I/b, x = (I + 3u^2/(32 r^3))/b,
+//     yb = -(3/(8b)) (1-b+r)^2 (b^2 + 2b(1+r) - 3(1-r)^2)/(8 r^2)
+//   r <= 1 - beta (monomer inside the colloid): x = y = 1, yb = -3r/4
+template <class T>
+__device__ __host__ __forceinline__ void ab_trans_scalars(T r, T rinv, T beta, bool reg, T &x, T &y, T &yb)
+{
+    const T b2 = beta * beta;
+    if (!reg || r >= T(1) + beta) {
+        T ri3 = rinv * rinv * rinv;
+        x = T(1.5) * rinv - T(0.5) * (T(1) + b2) * ri3;
+        y = T(0.75) * rinv + T(0.25) * (T(1) + b2) * ri3;
+        return;
+    }
+    if (r > T(1) - beta) {
+        T rd = T(1) - beta, r2 = r * r, r3 = r2 * r;
+        T t = rd * rd + T(3) * r2, u = rd * rd - r2;
+        T I = (T(16) * r3 * (T(1) + beta) - t * t) / (T(32) * r3);
+        y = I / beta;
+        x = (I + T(3) * u * u / (T(32) * r3)) / beta;
+        T poly = (rd + r) * (rd + r) * (b2 + T(2) * beta * (T(1) + r) - T(3) * (T(1) - r) * (T(1) - r)) / (T(8) * r2);
+        yb = -(T(3) / (T(8) * beta)) * poly;
+    } else {
+        x = T(1);
+        y = T(1);
+        yb = T(-0.75) * r;
+    }
+}
+
 // AB scalars (mob.cpp:410-412, 465-466)
 template <class T>
 __device__ __forceinline__ void ab_scalars(T rinv, T beta2, T &yb, T &xg, T &yg)

@@ -106,6 +106,14 @@ struct Engine {
     double *d_pmp[10] = {}, *d_pms[9] = {}, *d_ppart2 = nullptr;
     MinresScal *d_pmr = nullptr;
     bool any_indef = false;          // some replica's far field may be indefinite: pair-space MINRES
+
+    // trajectory observables (observe.cu)
+    double *d_obs_acc = nullptr, *d_obs_prev = nullptr, *d_obs_ring = nullptr, *d_obs_msd = nullptr;
+    int *d_obs_hasprev = nullptr;
+    unsigned long long *d_obs_hb = nullptr, *d_obs_ht = nullptr, *d_obs_msdn = nullptr;
+    int obs_nbins = 0, obs_lags = 0;
+    double obs_bmax = 0.0, obs_tmax = 0.0;
+    long obs_n = 0;
     RedTable red_bead;               // over beads (pair-space sums by lower bead)
 
     // Krylov workspace
@@ -144,6 +152,13 @@ struct Engine {
 // true when p is host memory (pageable or pinned): the C-ABI accepts host
 // pointers for state and noise arguments and copies them itself
 bool is_host_ptr(const void *p);
+
+// observe.cu: OBS_K doubles per bead -- bond count, sum b (3), sum |b|, sum |b|^2,
+// increment count, sum db (3); trap count, sum d (3), sum |d|, sum |d|^2, sum d_a^2 (3); pad
+constexpr int OBS_K = 20;
+int obs_reset(Engine &E, int nbins, double bond_max, double trap_max, int lags);
+int obs_sample(Engine &E, cudaStream_t st);
+int obs_read(Engine &E, ps_obs_out *out, cudaStream_t st);
 
 // rpy.cu
 // done: optional per-replica int flags (base pointer + byte stride); replicas

@@ -154,7 +154,7 @@ __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const 
                                            float2 fd, float nx0, float nx1, float ny0, float ny1, float tb2,
                                            float2 &tx, float2 &ty, float2 &tz)
 {
-#pragma unroll 4
+#pragma unroll 8
     for (int k = 0; k < nj; k++) {
         const float4 A = sA[k], B = sB[k];
         const float2 C = sC[k];
@@ -310,10 +310,9 @@ k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
         T G[15];
         gt_flat<T>(e, xg, yg, G);
         T TT[9];
-        if (mode == PS_AB_RPY) {
-            T ri3 = rinv * rinv * rinv;
-            T xa = T(1.5) * rinv - T(0.5) * (T(1) + beta2) * ri3;
-            T ya = T(0.75) * rinv + T(0.25) * (T(1) + beta2) * ri3;
+        if (mode == PS_AB_RPY || mode == PS_AB_RPY_REG) {
+            T xa, ya;
+            ab_trans_scalars<T>(r2 * rinv, rinv, T(sg.beta), mode == PS_AB_RPY_REG, xa, ya, yb);
             for (int a = 0; a < 3; a++)
                 for (int b = 0; b < 3; b++) TT[a * 3 + b] = xa * e[a] * e[b] + ya * ((a == b ? T(1) : T(0)) - e[a] * e[b]);
         } else if (shell) {

@@ -610,13 +610,13 @@ __global__ void k_schur(const Seg *__restrict__ segs, const int *__restrict__ re
                 double ri = 1.0 / dr;
                 double yb, xg, yg;
                 ab_scalars<double>(ri, s.beta * s.beta, yb, xg, yg);
+                double xa = 0.0, ya = 0.0;
+                if (s.ab_mode == PS_AB_RPY || s.ab_mode == PS_AB_RPY_REG)
+                    ab_trans_scalars<double>(dr, ri, s.beta, s.ab_mode == PS_AB_RPY_REG, xa, ya, yb);
                 for (int d = 0; d < 3; d++) {
                     double v;
                     if (q < 3) {
-                        if (s.ab_mode == PS_AB_RPY) {
-                            double ri3 = ri * ri * ri;
-                            double xa = 1.5 * ri - 0.5 * (1 + s.beta * s.beta) * ri3;
-                            double ya = 0.75 * ri + 0.25 * (1 + s.beta * s.beta) * ri3;
+                        if (s.ab_mode == PS_AB_RPY || s.ab_mode == PS_AB_RPY_REG) {
                             v = xa * e[d] * e[q] + ya * ((d == q) - e[d] * e[q]);
                         } else v = 0.0;
                     } else if (q < 6) {

@@ -116,6 +116,26 @@ class Batch:
         check(lib().ps_get_aux(self.h, _ptr(t), _ptr(k), _ptr(xp), self.stream), "ps_get_aux")
         return t, k, xp[: 3 * self.ncoll]
 
+    # observables -----------------------------------------------------------
+    def obs_reset(self, nbins: int = 64, bond_max: float = 4.0, trap_max: float = 2.0, lags: int = 64):
+        self._obs = (nbins, lags)
+        check(lib().ps_obs_reset(self.h, nbins, bond_max, trap_max, lags), "ps_obs_reset")
+
+    def observe(self):
+        check(lib().ps_observe(self.h, self.stream), "ps_observe")
+
+    def observables(self) -> dict:
+        """Per-replica accumulators (see ps_obs_out in the C header)."""
+        nbins, lags = self._obs
+        R = self.R
+        out = {"bond": np.zeros((R, 10)), "bond_hist": np.zeros((R, nbins), np.uint64),
+               "trap": np.zeros((R, 9)), "trap_hist": np.zeros((R, nbins), np.uint64),
+               "msd": np.zeros((R, lags, 6)), "msd_count": np.zeros((R, lags), np.uint64)}
+        o = _capi.PsObsOut(*[C.c_void_p(out[k].ctypes.data) for k in
+                             ("bond", "bond_hist", "trap", "trap_hist", "msd", "msd_count")])
+        check(lib().ps_obs_read(self.h, C.byref(o), self.stream), "ps_obs_read")
+        return out
+
     def set_aux(self, time=None, ktrap=None, xpos0=None):
         check(lib().ps_set_aux(self.h, _ptr(time), _ptr(ktrap), _ptr(xpos0), self.stream), "ps_set_aux")
 

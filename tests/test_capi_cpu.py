@@ -28,7 +28,8 @@ def test_struct_layouts_match_header(tmp_path):
     the header's struct."""
     structs = {"ps_desc": _capi.PsDesc, "ps_ksp_opts": _capi.PsKspOpts, "ps_ksp_result": _capi.PsKspResult,
                "ps_sqrt_opts": _capi.PsSqrtOpts, "ps_sqrt_result": _capi.PsSqrtResult,
-               "ps_step_inputs": _capi.PsStepInputs, "ps_step_result": _capi.PsStepResult}
+               "ps_step_inputs": _capi.PsStepInputs, "ps_step_result": _capi.PsStepResult,
+               "ps_obs_out": _capi.PsObsOut}
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{os.path.abspath(_capi.HEADER)}"',
              "int main(void) {"]
     for cname, py in structs.items():

@@ -33,6 +33,8 @@ CASES = {
     "shell_rpy": lambda: configs.small_mixed(seed=4, mm_HI=0, ab_mode=1),
     "colloids": lambda: configs.suspension(n=96, phi=0.1, seed=0),
     "brush_small": lambda: configs.brush(nchain=8, nper=8, seed=0),
+    # regularised unequal-radii monomer-colloid coupling, one monomer overlapping, one inside the colloid
+    "rpy_reg_overlap": lambda: __import__("test_oracle").overlapping_system(2),
 }
 
 
@@ -73,7 +75,7 @@ def test_minres_parity(case):
     b.close()
 
 
-@pytest.mark.parametrize("case", ["shell_C1", "mmhi_mixed", "colloids", "brush_small", "mmhi_rpy"])
+@pytest.mark.parametrize("case", ["shell_C1", "mmhi_mixed", "colloids", "brush_small", "mmhi_rpy", "rpy_reg_overlap"])
 def test_structured_solve_parity(case):
     """Exact block elimination of the constraint (PS_SOLVE_STRUCTURED) against the
     oracle's MINRES at rtol 1e-13; the colloid case (96 colloids) exercises the

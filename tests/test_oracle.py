@@ -165,3 +165,48 @@ def test_step_with_noise_runs():
     assert np.all(np.isfinite(x)) and np.all(np.isfinite(o["udiff"]))
     assert np.allclose(np.linalg.norm(q.reshape(-1, 4), axis=1), 1.0)
     assert all(i > 0 for i in o["iters"])
+
+
+# ---------------------------------------------------------------------------
+# regularised unequal-radii monomer-colloid coupling (ab_mode 2)
+def overlapping_system(ab_mode):
+    """One colloid, chains around it; monomer 0 overlaps the colloid (r = 1.1),
+    monomer 5 sits inside it (r = 0.5); beta = 0.3."""
+    sysm = configs.small_mixed(seed=12, Nm_chain=(3, 4), Nc=1, mm_HI=1, aa_mode=1, ab_mode=ab_mode)
+    x = sysm.x.copy()
+    c = x[-1]
+    x[0] = c + np.array([1.1, 0.0, 0.0])
+    x[5] = c + np.array([0.0, 0.5, 0.0])
+    return configs.System(sysm.name, sysm.params, x)
+
+
+def test_ab_regularised_scalars_continuous():
+    for beta in (0.2, 1.0 / 3.0, 0.5):
+        for rb, eps in ((1 + beta, 1e-9), (1 - beta, 1e-9)):
+            lo = np.array(po.ab_reg_scalars(rb - eps, beta))
+            hi = np.array(po.ab_reg_scalars(rb + eps, beta))
+            assert np.abs(lo - hi).max() < 1e-7
+        # far field: the PS_AB_RPY scalars
+        r = 3.0
+        x, y, yb = po.ab_reg_scalars(r, beta)
+        assert x == pytest.approx(1.5 / r - 0.5 * (1 + beta ** 2) / r ** 3)
+        assert y == pytest.approx(0.75 / r + 0.25 * (1 + beta ** 2) / r ** 3)
+        assert yb == pytest.approx(-0.75 / r ** 2)
+        # engulfed: the colloid's self mobility
+        assert po.ab_reg_scalars(0.3 * (1 - beta), beta)[:2] == (1.0, 1.0)
+
+
+def test_ab_regularised_keeps_force_torque_mobility_definite():
+    # the translation / rotation block (forces and torques -> velocities): the far-field
+    # 1/r^k terms make it indefinite once a monomer penetrates the colloid; the
+    # regularised branches keep it positive definite.  The stresslet coupling stays
+    # far-field, as in the reference (mob.cpp:455-470), so the full FTS matrix is not.
+    lam = {}
+    for mode in (1, 2):
+        s = oracle_for(overlapping_system(mode))
+        s.stage()
+        M = s.dense_mobility()
+        assert np.abs(M - M.T).max() < 1e-13 * np.abs(M).max()
+        n6 = s.nm3nc6
+        lam[mode] = np.linalg.eigvalsh(M[:n6, :n6]).min()
+    assert lam[1] < 0 < lam[2]
