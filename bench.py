@@ -319,6 +319,8 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    b.stage()
+    aa_cols, aa_tune_ms = b.autotune(5)      # far-field chunk width for this GPU and workload
     for _ in range(args.warmup):
         b.step(rtol=args.rtol, solver=solver)
     barrier()
@@ -416,6 +418,7 @@ def run_b200(args):
                "config": {"workload": name, "replicas_per_rank": len(systems), "beads_job": job_beads,
                           "rtol": args.rtol,
                           "precision": args.precision, "solver": args.solver,
+                          "aa_chunk_cols": aa_cols, "autotune_ms_per_launch": aa_tune_ms,
                           "l2": "flushed (256 MB write) before every timed step",
                           "parallelism": f"independent replicas on {world} GPU(s) ({args.scaling} scaling), "
                                          "no collective in the step"},

@@ -245,6 +245,13 @@ int ps_time_kernel(ps_ctx *ctx, int32_t which, int32_t reps, const double *u, do
 int ps_fma_peak(int32_t fp64, double *tflops, void *stream);
 /* number of kernels the library has launched since it was loaded */
 uint64_t ps_kernel_launches(void);
+/* Autotuner (no counterpart in the reference): times the monomer far-field
+ * kernel of this context for each column-chunk width in {128, 256, 512, 1024}
+ * (reps launches each, CUDA events) and keeps the fastest for this context and
+ * for every context created afterwards in the process.  The width is
+ * process-wide so that a replica's arithmetic stays independent of its batch.
+ * best_cols / ms (4 timings, candidate order) may be NULL. */
+int ps_autotune(ps_ctx *ctx, int32_t reps, int32_t *best_cols, double *ms, void *stream);
 
 #ifdef __cplusplus
 }

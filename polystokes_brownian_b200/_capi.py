@@ -105,6 +105,7 @@ def lib():
     L.ps_set_replica_seeds.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.ps_get_replica_steps.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.ps_get_aux.argtypes = [vp, P, P, P, vp]
+    L.ps_autotune.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double), vp]
     L.ps_obs_reset.argtypes = [vp, C.c_int32, C.c_double, C.c_double, C.c_int32]
     L.ps_observe.argtypes = [vp, vp]
     L.ps_obs_read.argtypes = [vp, C.POINTER(PsObsOut), vp]

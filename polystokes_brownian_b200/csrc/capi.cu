@@ -128,7 +128,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         s.lub_bonded = d.lub_bonded;
         s.nper = d.Nmono_per_chain > 0 ? d.Nmono_per_chain : 1;
         s.ss_off = -1;
-        s.nch_aa = std::max(1, (d.Nm + AA_CHUNK_COLS - 1) / AA_CHUNK_COLS);
+        s.nch_aa = std::max(1, (d.Nm + ps::g_aa_chunk_cols - 1) / ps::g_aa_chunk_cols);
         s.nch_bb = std::max(1, (d.Nc + BB_CHUNK_COLS - 1) / BB_CHUNK_COLS);
         if (d.aa_mode == PS_AA_RPY) {
             double b = d.beta, b2 = b * b;
@@ -630,6 +630,32 @@ int ps_time_kernel(ps_ctx *ctx, int32_t which, int32_t reps, const double *u, do
 }
 
 uint64_t ps_kernel_launches(void) { return (uint64_t)ps_launch_count; }
+
+
+int ps_autotune(ps_ctx *ctx, int32_t reps, int32_t *best_cols, double *ms, void *stream)
+{
+    if (!ctx) return PS_ERR_ARG;
+    ps::Engine &E = ctx->E;
+    const int cand[4] = {128, 256, 512, 1024};
+    double t[4] = {0, 0, 0, 0};
+    double *u = nullptr;
+    PS_CK(cudaMalloc(&u, sizeof(double) * std::max<long>(E.ntop, 1)));
+    PS_CK(cudaMemset(u, 0, sizeof(double) * std::max<long>(E.ntop, 1)));
+    int best = ps::g_aa_chunk_cols, rc = PS_OK;
+    double tbest = 1e300;
+    for (int k = 0; k < 4 && rc == PS_OK; k++) {
+        if ((rc = ps::set_aa_chunking(E, cand[k]))) break;
+        rc = ps::time_pairs(E, 0, reps > 0 ? reps : 5, u, &t[k], S(stream));
+        if (rc == PS_OK && t[k] < tbest) { tbest = t[k]; best = cand[k]; }
+    }
+    cudaFree(u);
+    if (rc) return rc;
+    ps::g_aa_chunk_cols = best;
+    if ((rc = ps::set_aa_chunking(E, best))) return rc;
+    if (best_cols) *best_cols = best;
+    if (ms) for (int k = 0; k < 4; k++) ms[k] = t[k];
+    return PS_OK;
+}
 
 int ps_fma_peak(int32_t fp64, double *tflops, void *stream)
 {

@@ -48,7 +48,7 @@ struct Seg {
 };
 
 // Column chunk widths of the far-field pair kernels.
-constexpr int AA_CHUNK_COLS = 256;
+constexpr int AA_CHUNK_COLS = 256;        // default; ps_autotune may pick another, process-wide
 constexpr int BB_CHUNK_COLS = 64;
 
 // Row tile of the far-field pair kernels.

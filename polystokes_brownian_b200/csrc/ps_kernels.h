@@ -149,6 +149,12 @@ struct Engine {
     cudaStream_t internal = nullptr;
 };
 
+// monomer column chunk width of the far-field AA kernels: process-wide (every
+// context of the process chunks a replica the same way, which keeps a replica's
+// arithmetic independent of its batch); set by ps_autotune
+extern int g_aa_chunk_cols;
+int set_aa_chunking(Engine &E, int cols);
+
 // true when p is host memory (pageable or pinned): the C-ABI accepts host
 // pointers for state and noise arguments and copies them itself
 bool is_host_ptr(const void *p);

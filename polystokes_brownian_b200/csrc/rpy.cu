@@ -552,6 +552,25 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
 }
 
 
+int g_aa_chunk_cols = AA_CHUNK_COLS;
+
+// re-chunk the monomer far field of a context: per-replica chunk counts, the
+// grid extent and the partial buffer
+int set_aa_chunking(Engine &E, int cols)
+{
+    E.nch_aa = 1;
+    for (auto &s : E.segs) {
+        s.nch_aa = std::max(1, (s.Nm + cols - 1) / cols);
+        E.nch_aa = std::max(E.nch_aa, s.nch_aa);
+    }
+    PS_CK(cudaDeviceSynchronize());
+    cudaFree(E.d_partAA);
+    E.d_partAA = nullptr;
+    PS_CK(cudaMalloc(&E.d_partAA, sizeof(double) * std::max<long>(E.ntop, 1) * E.nch_aa));
+    PS_CK(cudaMemcpy(E.d_segs, E.segs.data(), sizeof(Seg) * E.segs.size(), cudaMemcpyHostToDevice));
+    return PS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // diagnostics: average duration (CUDA events on `st`) of one far-field kernel
 // which: 0 AA pair kernel, 1 AB/BA kernel, 2 BB kernel, 3 whole mobility apply

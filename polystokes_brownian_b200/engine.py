@@ -116,6 +116,14 @@ class Batch:
         check(lib().ps_get_aux(self.h, _ptr(t), _ptr(k), _ptr(xp), self.stream), "ps_get_aux")
         return t, k, xp[: 3 * self.ncoll]
 
+    def autotune(self, reps: int = 5):
+        """Pick the monomer far-field column-chunk width for this process (ps_autotune);
+        returns (width, {width: ms per launch})."""
+        best = C.c_int32(0)
+        ms = (C.c_double * 4)()
+        check(lib().ps_autotune(self.h, reps, C.byref(best), ms, self.stream), "ps_autotune")
+        return int(best.value), dict(zip((128, 256, 512, 1024), list(ms)))
+
     # observables -----------------------------------------------------------
     def obs_reset(self, nbins: int = 64, bond_max: float = 4.0, trap_max: float = 2.0, lags: int = 64):
         self._obs = (nbins, lags)

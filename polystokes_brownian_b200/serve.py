@@ -102,6 +102,8 @@ def make_trace(n_req: int, rate: float, seed: int = 0, nmin: int = 64, nmax: int
 
 
 class Server:
+    _tuned = False
+
     def __init__(self, precision: int = _capi.PS_PREC_MIXED, budget_bytes: float = 150e9, max_slots: int = 256,
                  rtol: float = 1e-6, solver: int = _capi.PS_SOLVE_STRUCTURED, rebuild_every: int = 1,
                  device: str = "cuda:0", lub_table: np.ndarray | None = None):
@@ -141,6 +143,11 @@ class Server:
         xp = torch.from_numpy(np.concatenate(xp)).to(dev) if xp else None
         b.set_aux(t, k, xp)
         b.set_replica_seeds([s.req.seed for s in slots], [s.rng_steps for s in slots])
+        if not Server._tuned:
+            # one process-wide choice, so every later context chunks replicas the same way
+            b.stage()
+            self.aa_chunk_cols, _ = b.autotune(3)
+            Server._tuned = True
         self.rebuilds += 1
         return b
 
