@@ -64,7 +64,36 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="N > 1: weak = one seeded ensemble per rank; strong = one ensemble split across ranks (LPT)")
+    ap.add_argument("--profile-kernel", type=int, default=0, metavar="K",
+                    help="profiler driver: build the workload, stage it once, launch only the monomer pair kernel "
+                         "K times (default chunk width, no autotuning, no steps) and exit; prints no bench line")
     return ap.parse_args()
+
+
+def profile_kernel(args):
+    """A short, fixed launch sequence for profiler captures of the dominant kernel:
+    the packing and pair-list kernels of one staging, then K launches of the
+    monomer pair kernel through ps_time_kernel (one untimed warm launch + K)."""
+    import ctypes as C
+
+    import torch
+    from polystokes_brownian_b200 import _capi
+    from polystokes_brownian_b200.engine import Batch, _ptr
+
+    torch.cuda.set_device(0)
+    systems, name = workload(args)
+    prec = _capi.PS_PREC_MIXED if args.precision == "mixed" else _capi.PS_PREC_FP64
+    b = Batch(systems, precision=prec)
+    b.stage()
+    u = torch.randn(b.ntop, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    ms = C.c_double(0)
+    _capi.check(_capi.lib().ps_time_kernel(b.h, 0, args.profile_kernel, _ptr(u), C.byref(ms), b.stream),
+                "ps_time_kernel")
+    free, total = torch.cuda.mem_get_info()
+    print(json.dumps({"profile_kernel": "k_rpy_aa_f2" if prec == _capi.PS_PREC_MIXED else "k_rpy_aa",
+                      "workload": name, "launches": args.profile_kernel + 1, "ms_per_launch": ms.value,
+                      "device_gb_in_use": (total - free) / 1e9}))
+    b.close()
 
 
 def workload(args, rank=0, world=1):
@@ -439,7 +468,9 @@ def run_b200(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.profile_kernel:
+        profile_kernel(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_b200(a)

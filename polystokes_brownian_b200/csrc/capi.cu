@@ -51,7 +51,7 @@ static int upload(T *&dst, const std::vector<T> &v)
 static void free_engine(Engine &E)
 {
     void *ptrs[] = {E.d_segs, E.d_vec_offs, E.d_top_offs, E.d_vel_offs, E.d_bead_offs, E.d_x, E.d_q, E.d_xpos0,
-                    E.d_xn, E.d_pos64, E.d_pos32, E.d_pos32lo, E.d_chain, E.d_coll_rep, E.d_time, E.d_ktrap, E.d_trapinfo,
+                    E.d_xn, E.d_pos64, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_chain, E.d_coll_rep, E.d_time, E.d_ktrap, E.d_trapinfo,
                     E.d_aa_tiles, E.d_ab_tiles, E.d_bb_tiles, E.d_partAA, E.d_partAB, E.d_partBB, E.d_partBA,
                     E.d_tab, E.d_stale, E.d_aa_last, E.d_delta, E.d_schurQ, E.d_schurL, E.d_schur_reps, E.d_ss_reps,
                     E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_cell, E.d_cell_start, E.d_cell_sorted,
@@ -284,6 +284,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_pos64, sizeof(double4) * bead);
     TRY_ALLOC(E.d_pos32, sizeof(float4) * bead);
     TRY_ALLOC(E.d_pos32lo, sizeof(float4) * bead);
+    TRY_ALLOC(E.d_aa_te2, sizeof(float) * std::max<long>(R, 1));
     // pair partials
     TRY_ALLOC(E.d_partAA, sizeof(double) * top * E.nch_aa);
     TRY_ALLOC(E.d_partAB, sizeof(double) * top);

@@ -51,6 +51,7 @@ struct Engine {
     double *d_x = nullptr, *d_q = nullptr, *d_xpos0 = nullptr, *d_xn = nullptr;
     double4 *d_pos64 = nullptr;
     float4 *d_pos32 = nullptr, *d_pos32lo = nullptr;   // FP32 positions as hi + lo
+    float *d_aa_te2 = nullptr;   // per replica: squared exact radius of the FP32 monomer kernel
     double *d_chain = nullptr;      // chain id per bead (monomers), -1-c for colloid c
     int *d_coll_rep = nullptr;      // replica of each colloid
     double *d_time = nullptr;       // per replica time

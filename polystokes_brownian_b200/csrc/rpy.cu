@@ -133,10 +133,15 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
 // AA in FP32 with packed FP32x2 arithmetic (sm_100 FFMA2/FADD2/FMUL2): each
 // thread owns two rows (i and i + 64 of a 128-row tile) held in the two lanes of
 // float2 registers, so one packed instruction advances two pairs against the
-// same shared-memory column.  Positions are hi + lo floats, separations
-// d = (hi_i - hi_j) + (lo_i - lo_j).  Self pairs and skipped same-chain pairs
-// get rinv = 0, which zeroes their contribution without a branch; the near-
-// overlap form (r <= 2 beta) is applied only when some lane of the warp needs it.
+// same shared-memory column.  Positions are hi + lo floats.  Separations start
+// as d = hi_i - hi_j, whose error is at most 2^-23 X for a replica whose
+// coordinates stay below X in magnitude; within the replica's exact radius
+// (r <= max(2.1 beta, X / 16), so the hi-only relative error stays below 2^-19
+// where it is used) the warp adds the low parts, d = (hi_i - hi_j) + (lo_i - lo_j),
+// the same rounding as a full hi + lo difference.  Self pairs and skipped
+// same-chain pairs get rinv = 0, which zeroes their contribution without a
+// branch; the near-overlap form (r <= 2 beta) lies inside the exact radius and is
+// applied only when some lane of the warp needs it.
 constexpr int AAF_THREADS = 64;
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
@@ -144,36 +149,51 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 // one staged column tile against the thread's two rows; CHECK: the tile may
 // hold the rows themselves or (chain_HI) same-chain partners, which get rinv = 0.
 // Far form in factored scalars: y = ri (c + d ri^2), (x - y)/r^2 = ri^3 (a + b ri^2),
-// a = c0 - c2, b = c1 - c3, c = c2, d = c3; the near form (r^2 <= (2 beta)^2, taken
-// only when some lane of the warp needs it) overwrites both.
+// a = c0 - c2, b = c1 - c3, c = c2, d = c3; the near form (r^2 <= (2 beta)^2)
+// overwrites both.  Shared columns: sA (hi x, y, z, u0), sB (lo x, y, z, chain),
+// sC (u1, u2); sB is read only inside the exact radius or by CHECK tiles.
 template <bool CHECK>
 __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const float4 *__restrict__ sB,
                                            const float2 *__restrict__ sC, int jt, int nj, int i0, int i1,
                                            bool chain_hi, float w0, float w1, float2 px, float2 py, float2 pz,
-                                           float2 lx, float2 ly, float2 lz, float2 fa, float2 fb, float2 fc,
-                                           float2 fd, float nx0, float nx1, float ny0, float ny1, float tb2,
-                                           float2 &tx, float2 &ty, float2 &tz)
+                                           const float4 *__restrict__ plo, int b0, int b1, float2 fa, float2 fb,
+                                           float2 fc, float2 fd, const Seg &sg, float te2, float2 &tx, float2 &ty,
+                                           float2 &tz)
 {
-#pragma unroll 8
+#pragma unroll 4
     for (int k = 0; k < nj; k++) {
-        const float4 A = sA[k], B = sB[k];
+        const float4 A = sA[k];
         const float2 C = sC[k];
-        float2 dx = __fadd2_rn(__fadd2_rn(px, f2(-A.x)), __fadd2_rn(lx, f2(-B.x)));
-        float2 dy = __fadd2_rn(__fadd2_rn(py, f2(-A.y)), __fadd2_rn(ly, f2(-B.y)));
-        float2 dz = __fadd2_rn(__fadd2_rn(pz, f2(-A.z)), __fadd2_rn(lz, f2(-B.z)));
+        float2 dx = __fadd2_rn(px, f2(-A.x));
+        float2 dy = __fadd2_rn(py, f2(-A.y));
+        float2 dz = __fadd2_rn(pz, f2(-A.z));
         float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         bool e0 = false, e1 = false;
         if constexpr (CHECK) {
             const int j = jt + k;
-            e0 = (j == i0) || (chain_hi && w0 == A.w);
-            e1 = (j == i1) || (chain_hi && w1 == A.w);
+            const float cw = sB[k].w;
+            e0 = (j == i0) || (chain_hi && w0 == cw);
+            e1 = (j == i1) || (chain_hi && w1 == cw);
+        }
+        const bool inner = __any_sync(0xffffffffu, r2.x <= te2 || r2.y <= te2);
+        if (inner) {
+            // row low parts re-read from L1 here rather than held in registers
+            const float4 B = sB[k], L0 = __ldg(plo + b0), L1 = __ldg(plo + b1);
+            const float2 lx = make_float2(L0.x, L1.x), ly = make_float2(L0.y, L1.y), lz = make_float2(L0.z, L1.z);
+            dx = __fadd2_rn(dx, __fadd2_rn(lx, f2(-B.x)));
+            dy = __fadd2_rn(dy, __fadd2_rn(ly, f2(-B.y)));
+            dz = __fadd2_rn(dz, __fadd2_rn(lz, f2(-B.z)));
+            r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         }
         float2 ri = make_float2(e0 ? 0.f : rsqrtf(r2.x), e1 ? 0.f : rsqrtf(r2.y));
         float2 ri2 = __fmul2_rn(ri, ri);
         float2 yv = __fmul2_rn(__ffma2_rn(fd, ri2, fc), ri);                     // y
         float2 g = __fmul2_rn(__ffma2_rn(fb, ri2, fa), __fmul2_rn(ri2, ri));    // (x - y) / r^2
-        const bool n0 = !e0 && r2.x <= tb2, n1 = !e1 && r2.y <= tb2;
-        if (__any_sync(0xffffffffu, n0 || n1)) {
+        if (inner) {
+            // overlap constants re-read here: they are needed only inside the exact radius
+            const float tb2 = (float)(4.0 * sg.beta * sg.beta);
+            const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
+            const bool n0 = !e0 && r2.x <= tb2, n1 = !e1 && r2.y <= tb2;
             if (n0) {
                 float r = r2.x * ri.x, x = nx0 + nx1 * r;
                 yv.x = ny0 + ny1 * r;
@@ -186,9 +206,9 @@ __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const 
             }
         }
         // mob_a u = y u + (x - y)(d.u) d / r^2
-        float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(B.w))));
+        float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(A.w))));
         float2 f = __fmul2_rn(g, du);
-        tx = __ffma2_rn(f, dx, __ffma2_rn(yv, f2(B.w), tx));
+        tx = __ffma2_rn(f, dx, __ffma2_rn(yv, f2(A.w), tx));
         ty = __ffma2_rn(f, dy, __ffma2_rn(yv, f2(C.x), ty));
         tz = __ffma2_rn(f, dz, __ffma2_rn(yv, f2(C.y), tz));
     }
@@ -196,12 +216,12 @@ __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const 
 
 __global__ void __launch_bounds__(AAF_THREADS, 16)
 k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const float4 *__restrict__ pos,
-            const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
-            long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
+            const float4 *__restrict__ plo, const float *__restrict__ aa_te2, const double *__restrict__ u, int in_top,
+            double *__restrict__ part, long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
 {
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
-    __shared__ float4 sA[128];   // hi x, y, z, chain
-    __shared__ float4 sB[128];   // lo x, y, z, u0
+    __shared__ float4 sA[128];   // hi x, y, z, u0
+    __shared__ float4 sB[128];   // lo x, y, z, chain
     __shared__ float2 sC[128];   // u1, u2
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
@@ -214,23 +234,24 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
     const bool a0 = threadIdx.x < tl.nrow, a1 = threadIdx.x + AAF_THREADS < tl.nrow;
     const int uoff = in_top ? sg.top_off : sg.vec_off;
     const float4 P0 = pos[sg.bead_off + (a0 ? i0 : tl.row0)], P1 = pos[sg.bead_off + (a1 ? i1 : tl.row0)];
-    const float4 L0 = plo[sg.bead_off + (a0 ? i0 : tl.row0)], L1 = plo[sg.bead_off + (a1 ? i1 : tl.row0)];
+    const int b0 = sg.bead_off + (a0 ? i0 : tl.row0), b1 = sg.bead_off + (a1 ? i1 : tl.row0);
     const float2 px = make_float2(P0.x, P1.x), py = make_float2(P0.y, P1.y), pz = make_float2(P0.z, P1.z);
-    const float2 lx = make_float2(L0.x, L1.x), ly = make_float2(L0.y, L1.y), lz = make_float2(L0.z, L1.z);
     const bool chain_hi = sg.chain_HI != 0;
     const float2 fa = f2(sg.aa_c[0] - sg.aa_c[2]), fb = f2(sg.aa_c[1] - sg.aa_c[3]);
     const float2 fc = f2(sg.aa_c[2]), fd = f2(sg.aa_c[3]);
-    const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
-    const float tb2 = (float)(4.0 * sg.beta * sg.beta);
-    float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), kx = f2(0.f), ky = f2(0.f), kz = f2(0.f);
+    const float te2 = aa_te2[tl.rep];
+    // Kahan sums across column tiles (sum, compensation per row and axis) live in
+    // shared memory, thread-private, so the pair loop keeps their registers
+    __shared__ float2 sKs[6][AAF_THREADS];
+    for (int q = 0; q < 6; q++) sKs[q][threadIdx.x] = f2(0.f);
     for (int jt = j0; jt < j1; jt += 128) {
         const int nj = min(128, j1 - jt);
         __syncthreads();
         for (int t = threadIdx.x; t < nj; t += AAF_THREADS) {
             const int j = jt + t;
             const float4 A = pos[sg.bead_off + j], B = plo[sg.bead_off + j];
-            sA[t] = A;
-            sB[t] = make_float4(B.x, B.y, B.z, (float)u[uoff + 3 * j]);
+            sA[t] = make_float4(A.x, A.y, A.z, (float)u[uoff + 3 * j]);
+            sB[t] = make_float4(B.x, B.y, B.z, A.w);
             sC[t] = make_float2((float)u[uoff + 3 * j + 1], (float)u[uoff + 3 * j + 2]);
         }
         __syncthreads();
@@ -238,20 +259,22 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
         // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
         const bool check = chain_hi || (jt < tl.row0 + 2 * AAF_THREADS && jt + nj > tl.row0);
         if (check)
-            aa_f2_cols<true>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, fa, fb, fc,
-                             fd, nx0, nx1, ny0, ny1, tb2, tx, ty, tz);
+            aa_f2_cols<true>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, plo, b0, b1, fa,
+                             fb, fc, fd, sg, te2, tx, ty, tz);
         else
-            aa_f2_cols<false>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, lx, ly, lz, fa, fb, fc,
-                              fd, nx0, nx1, ny0, ny1, tb2, tx, ty, tz);
+            aa_f2_cols<false>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, plo, b0, b1, fa,
+                              fb, fc, fd, sg, te2, tx, ty, tz);
         // Kahan across column tiles
-        float2 yy, tt;
-        yy = __fadd2_rn(tx, make_float2(-kx.x, -kx.y)); tt = __fadd2_rn(sx, yy);
-        kx = __fadd2_rn(__fadd2_rn(tt, make_float2(-sx.x, -sx.y)), make_float2(-yy.x, -yy.y)); sx = tt;
-        yy = __fadd2_rn(ty, make_float2(-ky.x, -ky.y)); tt = __fadd2_rn(sy, yy);
-        ky = __fadd2_rn(__fadd2_rn(tt, make_float2(-sy.x, -sy.y)), make_float2(-yy.x, -yy.y)); sy = tt;
-        yy = __fadd2_rn(tz, make_float2(-kz.x, -kz.y)); tt = __fadd2_rn(sz, yy);
-        kz = __fadd2_rn(__fadd2_rn(tt, make_float2(-sz.x, -sz.y)), make_float2(-yy.x, -yy.y)); sz = tt;
+        const float2 t3[3] = {tx, ty, tz};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const float2 sq = sKs[q][threadIdx.x], kq = sKs[3 + q][threadIdx.x];
+            const float2 yy = __fadd2_rn(t3[q], make_float2(-kq.x, -kq.y)), tt = __fadd2_rn(sq, yy);
+            sKs[3 + q][threadIdx.x] = __fadd2_rn(__fadd2_rn(tt, make_float2(-sq.x, -sq.y)), make_float2(-yy.x, -yy.y));
+            sKs[q][threadIdx.x] = tt;
+        }
     }
+    const float2 sx = sKs[0][threadIdx.x], sy = sKs[1][threadIdx.x], sz = sKs[2][threadIdx.x];
     double *o = part + (long)c * part_stride + sg.top_off;
     if (a0) { o[3 * i0] = sx.x; o[3 * i0 + 1] = sy.x; o[3 * i0 + 2] = sz.x; }
     if (a1) { o[3 * i1] = sx.y; o[3 * i1 + 1] = sy.y; o[3 * i1 + 2] = sz.y; }
@@ -514,7 +537,7 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
     if (E.n_aa_tiles && !skip_aa) {
         if constexpr (sizeof(T) == 4)
             ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
-                E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
+                E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
         else
             ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(
                 E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
@@ -583,7 +606,7 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     cudaEventCreate(&b);
     auto launch = [&]() {
         if (which == 0 && E.n_aa_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+            if (fp32) ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
             else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
         } else if (which == 1 && E.n_ab_tiles) {
             if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);

@@ -55,10 +55,36 @@ __global__ void k_pack(long ntot, const double *__restrict__ x, const double *__
     p32lo[b] = make_float4((float)(cx - (double)hx), (float)(cy - (double)hy), (float)(cz - (double)hz), 0.f);
 }
 
+// Exact radius of the FP32 monomer kernel, one block per replica: with X the
+// largest monomer coordinate magnitude of the replica, hi-only separations carry
+// an error of at most 2^-23 X, so beyond r = X / 16 their relative error stays
+// below 2^-19; inside max(2.1 beta, X / 16) the kernel adds the low parts.  The
+// radius covers the overlap form (r <= 2 beta).  Stored squared, as a float.
+// A max over the replica's own beads: independent of the other replicas.
+__global__ void k_aa_radius(const Seg *__restrict__ segs, const double *__restrict__ x, float *__restrict__ te2)
+{
+    const Seg &s = segs[blockIdx.x];
+    __shared__ double red[256];
+    double m = 0.0;
+    for (long i = threadIdx.x; i < 3L * s.Nm; i += blockDim.x) m = fmax(m, fabs(x[3L * s.bead_off + i]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double t = fmax(2.1 * s.beta, red[0] * (1.0 / 16.0));
+        te2[blockIdx.x] = isfinite(t) ? (float)fmin(t * t, 3.0e38) : 3.0e38f;
+    }
+}
+
 int stage_pack(Engine &E, cudaStream_t st)
 {
     int thr = 256;
     ::ps_launch_count++, k_pack<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_x, E.d_chain, E.d_pos64, E.d_pos32, E.d_pos32lo);
+    if (E.n_aa_tiles)
+        ::ps_launch_count++, k_aa_radius<<<E.R, 256, 0, st>>>(E.d_segs, E.d_x, E.d_aa_te2);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

@@ -32,3 +32,22 @@ def test_mixed_operator_and_solve_error(n_rep):
     assert _rel(X32, X64) < 1e-6
     b64.close()
     b32.close()
+
+
+@pytest.mark.parametrize("shift", [0.0, 1000.0])
+def test_mixed_far_from_origin(shift):
+    """The FP32 monomer kernel adds the low parts of positions within an exact
+    radius that grows with the replica's largest coordinate: a replica moved
+    1000 units from the origin, where hi-only separations would be off by
+    ~1e-4, keeps the 1e-6 bound on the mobility apply."""
+    s = configs.ensemble(1, seed=5, nmin=1500, nmax=1500)[0]
+    s.x = s.x + np.array([shift, -0.5 * shift, 0.25 * shift])
+    b64 = Batch([s], precision=0)
+    b32 = Batch([s], precision=1)
+    b64.stage()
+    b32.stage()
+    g = torch.Generator("cuda").manual_seed(2)
+    u = torch.randn(b64.ntop, dtype=torch.float64, device="cuda", generator=g)
+    assert _rel(b32.mobility_apply(u), b64.mobility_apply(u)) < 1e-6
+    b64.close()
+    b32.close()
