@@ -447,7 +447,7 @@ def run_b200(args):
                "config": {"workload": name, "replicas_per_rank": len(systems), "beads_job": job_beads,
                           "rtol": args.rtol,
                           "precision": args.precision, "solver": args.solver,
-                          "aa_chunk_cols": aa_cols, "autotune_ms_per_launch": aa_tune_ms,
+                          "aa_chunk_cols": aa_cols, "autotune_ms_per_apply": aa_tune_ms,
                           "l2": "flushed (256 MB write) before every timed step",
                           "parallelism": f"independent replicas on {world} GPU(s) ({args.scaling} scaling), "
                                          "no collective in the step"},

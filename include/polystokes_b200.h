@@ -240,14 +240,17 @@ int ps_mobility_apply_noalloc(const double *x, const double *u, double *y, int32
  * launches of one far-field kernel on mobility-layout input u; which: 0 the
  * monomer-monomer pair kernel, 1 monomer-colloid, 2 colloid-colloid, 3 the whole
  * mobility apply.  ps_fma_peak: measured FMA throughput (TFLOP/s) of the current
- * device, FP64 when fp64 != 0, else FP32. */
+ * device, FP64 when fp64 != 0, else FP32 (the larger of scalar and packed FP32x2
+ * FMA chains). */
 int ps_time_kernel(ps_ctx *ctx, int32_t which, int32_t reps, const double *u, double *ms, void *stream);
 int ps_fma_peak(int32_t fp64, double *tflops, void *stream);
 /* number of kernels the library has launched since it was loaded */
 uint64_t ps_kernel_launches(void);
-/* Autotuner (no counterpart in the reference): times the monomer far-field
- * kernel of this context for each column-chunk width in {128, 256, 512, 1024}
- * (reps launches each, CUDA events) and keeps the fastest for this context and
+/* Autotuner (no counterpart in the reference): times the whole mobility apply
+ * of this context (the monomer far-field kernel, whose column-chunk width is
+ * tuned, plus the combine that reads one partial sum per chunk) for each width
+ * in {128, 256, 512, 1024} (reps applies each, CUDA events) and keeps the
+ * fastest for this context and
  * for every context created afterwards in the process.  The width is
  * process-wide so that a replica's arithmetic stays independent of its batch.
  * best_cols / ms (4 timings, candidate order) may be NULL. */

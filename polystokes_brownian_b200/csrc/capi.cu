@@ -412,6 +412,7 @@ int ps_set_lub_table(ps_ctx *ctx, const double *tab, int32_t nrow, int32_t ncol)
         for (int c = 0; c < 11; c++) t[(size_t)i * 11 + c] = tab[(size_t)i * ncol + c];
     if (E.d_lubtab) cudaFree(E.d_lubtab);
     E.d_lubtab = nullptr;
+    E.ps_setup_valid = false;
     int rc = upload(E.d_lubtab, t);
     if (rc) return rc;
     E.lub_nrow = nrow;
@@ -646,7 +647,7 @@ int ps_autotune(ps_ctx *ctx, int32_t reps, int32_t *best_cols, double *ms, void 
     double tbest = 1e300;
     for (int k = 0; k < 4 && rc == PS_OK; k++) {
         if ((rc = ps::set_aa_chunking(E, cand[k]))) break;
-        rc = ps::time_pairs(E, 0, reps > 0 ? reps : 5, u, &t[k], S(stream));
+        rc = ps::time_pairs(E, 3, reps > 0 ? reps : 5, u, &t[k], S(stream));   // apply incl. combine
         if (rc == PS_OK && t[k] < tbest) { tbest = t[k]; best = cand[k]; }
     }
     cudaFree(u);

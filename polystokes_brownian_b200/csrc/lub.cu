@@ -188,6 +188,7 @@ __global__ void k_canon_fill(long ntot, const int *__restrict__ sptr, const int 
 // build the symmetric partner list (which 3) and from it the canonical i<j list
 int lub_build(Engine &E, cudaStream_t st)
 {
+    E.ps_setup_valid = false;     // new pair list
     long np = 0;
     int rc = build_list(E, 3, &np, st);
     if (rc) return rc;

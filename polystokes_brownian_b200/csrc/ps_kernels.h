@@ -101,6 +101,9 @@ struct Engine {
     // pair-space lubricated solve: per pair K^{1/2} and preconditioner blocks (12x12), CG vectors (12 per pair)
     double *d_pS = nullptr, *d_pP = nullptr, *d_py_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double *d_ppart = nullptr; long pair_cap = 0;
+    // pair blocks d_pS / d_pP hold the setup of the current staged positions
+    // (cleared by every packing, table change and reallocation)
+    bool ps_setup_valid = false;
     // stresslet unknowns of replicas without a dense stresslet inverse (mobility layout), per-bead partials
     double *d_sv[5] = {nullptr, nullptr, nullptr, nullptr, nullptr}, *d_sbead[2] = {nullptr, nullptr};
     // pair-space MINRES: 10 pair-storage vectors (3 r, 3 w, v, z, x, Az), 9 stresslet-storage vectors, scalars

@@ -965,6 +965,7 @@ static int ensure_pair_space(Engine &E)
 {
     long need = std::max<long>(E.lub_npairs, 1);
     if (need <= E.pair_cap) return PS_OK;
+    E.ps_setup_valid = false;
     cudaFree(E.d_pS); cudaFree(E.d_pP); cudaFree(E.d_ppart); cudaFree(E.d_ppart2);
     for (auto &p : E.d_py_) cudaFree(p);
     for (auto &p : E.d_pmp) cudaFree(p);
@@ -1085,10 +1086,14 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     PS_CK(cudaMemsetAsync(E.d_pu2, 0, sizeof(double) * E.ntop, st));
     PS_CK(cudaMemsetAsync(E.d_py2, 0, sizeof(double) * E.ntop, st));
     ::ps_launch_count++, k_pcg_start<<<E.red.nblk, RB_THREADS, 0, st>>>(E.red, E.d_segs, b, E.d_D, E.d_pcg, o->rtol);
-    if (npair)
+    // the pair blocks depend on the staged positions and the table only: solves
+    // that share a staging (the deterministic and the noise solve) set them up once
+    if (npair && !E.ps_setup_valid) {
         ::ps_launch_count++, k_ps_setup<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                                  E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.d_pS,
                                                                  E.d_pP);
+        E.ps_setup_valid = true;
+    }
     if (E.n_ss_reps) {
         ::ps_launch_count++, k_ss_inverse<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, E.d_ssinv);
         // g: u2 = [0 ; M_SS^{-1} b_S]

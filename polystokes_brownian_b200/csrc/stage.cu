@@ -82,6 +82,7 @@ __global__ void k_aa_radius(const Seg *__restrict__ segs, const double *__restri
 int stage_pack(Engine &E, cudaStream_t st)
 {
     int thr = 256;
+    E.ps_setup_valid = false;     // positions change: the pair-space blocks are stale
     ::ps_launch_count++, k_pack<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_x, E.d_chain, E.d_pos64, E.d_pos32, E.d_pos32lo);
     if (E.n_aa_tiles)
         ::ps_launch_count++, k_aa_radius<<<E.R, 256, 0, st>>>(E.d_segs, E.d_x, E.d_aa_te2);

@@ -118,7 +118,7 @@ class Batch:
 
     def autotune(self, reps: int = 5):
         """Pick the monomer far-field column-chunk width for this process (ps_autotune);
-        returns (width, {width: ms per launch})."""
+        returns (width, {width: ms per mobility apply, combine included})."""
         best = C.c_int32(0)
         ms = (C.c_double * 4)()
         check(lib().ps_autotune(self.h, reps, C.byref(best), ms, self.stream), "ps_autotune")
