@@ -130,154 +130,183 @@ k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
 }
 
 // ---------------------------------------------------------------------------
-// AA in FP32 with packed FP32x2 arithmetic (sm_100 FFMA2/FADD2/FMUL2): each
-// thread owns two rows (i and i + 64 of a 128-row tile) held in the two lanes of
-// float2 registers, so one packed instruction advances two pairs against the
-// same shared-memory column.  Positions are hi + lo floats.  Separations start
-// as d = hi_i - hi_j, whose error is at most 2^-23 X for a replica whose
-// coordinates stay below X in magnitude; within the replica's exact radius
-// (r <= max(2.1 beta, X / 16), so the hi-only relative error stays below 2^-19
-// where it is used) the warp adds the low parts, d = (hi_i - hi_j) + (lo_i - lo_j),
-// the same rounding as a full hi + lo difference.  Self pairs and skipped
-// same-chain pairs get rinv = 0, which zeroes their contribution without a
-// branch; the near-overlap form (r <= 2 beta) lies inside the exact radius and is
-// applied only when some lane of the warp needs it.
+// AA in FP32 with packed FP32x2 arithmetic (sm_100 FFMA2/FADD2/FMUL2), column
+// pairs in the two lanes: a thread owns rows i and i + 64 of a 128-row tile,
+// each held as a broadcast pair (loop-invariant), and advances both against
+// columns (j, j + 1) per step, four pairs per step.  Shared columns are stored
+// pairwise, so the loads deliver every operand pair as it is consumed, with no
+// per-column broadcast: sXY (-x_j, -x_j+1, -y_j, -y_j+1), sZU (-z_j, -z_j+1,
+// u0_j, u0_j+1), sUU (u1_j, u1_j+1, u2_j, u2_j+1); sLA (lo x_j, x_j+1, lo y_j,
+// y_j+1) and sLB (lo z_j, z_j+1, chain_j, chain_j+1) are read inside the exact
+// radius or by CHECK tiles.  An odd tile is padded with a column at 1e18
+// carrying u = 0.  Each row's two lane sums are added once per column tile,
+// then Kahan-summed across tiles.
+//
+// Positions are hi + lo floats.  Separations start as d = hi_i - hi_j, whose
+// error is at most 2^-23 X for a replica whose coordinates stay below X in
+// magnitude; within the replica's exact radius (r <= max(2.1 beta, X / 16), so
+// the hi-only relative error stays below 2^-19 where it is used) the warp adds
+// the low parts, d = (hi_i - hi_j) + (lo_i - lo_j), the same rounding as a full
+// hi + lo difference.  Self pairs and skipped same-chain pairs get rinv = 0,
+// which zeroes their contribution without a branch; the near-overlap form
+// (r <= 2 beta) lies inside the exact radius.  Far form in factored scalars:
+// y = ri (c + d ri^2), (x - y)/r^2 = ri^3 (a + b ri^2), a = c0 - c2, b = c1 - c3,
+// c = c2, d = c3; the near form (r^2 <= (2 beta)^2) overwrites both.
 constexpr int AAF_THREADS = 64;
+constexpr float AAC_PAD = 1e18f;
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-// one staged column tile against the thread's two rows; CHECK: the tile may
-// hold the rows themselves or (chain_HI) same-chain partners, which get rinv = 0.
-// Far form in factored scalars: y = ri (c + d ri^2), (x - y)/r^2 = ri^3 (a + b ri^2),
-// a = c0 - c2, b = c1 - c3, c = c2, d = c3; the near form (r^2 <= (2 beta)^2)
-// overwrites both.  Shared columns: sA (hi x, y, z, u0), sB (lo x, y, z, chain),
-// sC (u1, u2); sB is read only inside the exact radius or by CHECK tiles.
-template <bool CHECK>
-__device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sA, const float4 *__restrict__ sB,
-                                           const float2 *__restrict__ sC, int jt, int nj, int i0, int i1,
-                                           bool chain_hi, float w0, float w1, float2 px, float2 py, float2 pz,
-                                           const float4 *__restrict__ plo, int b0, int b1, float2 fa, float2 fb,
-                                           float2 fc, float2 fd, const Seg &sg, float te2, float2 &tx, float2 &ty,
-                                           float2 &tz)
+__device__ __forceinline__ void aa_near_lane(bool n, float r2, float ri, float ri2, float nx0, float nx1, float ny0,
+                                             float ny1, float &yv, float &g)
 {
-#pragma unroll 4
-    for (int k = 0; k < nj; k++) {
-        const float4 A = sA[k];
-        const float2 C = sC[k];
-        float2 dx = __fadd2_rn(px, f2(-A.x));
-        float2 dy = __fadd2_rn(py, f2(-A.y));
-        float2 dz = __fadd2_rn(pz, f2(-A.z));
-        float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-        bool e0 = false, e1 = false;
-        if constexpr (CHECK) {
-            const int j = jt + k;
-            const float cw = sB[k].w;
-            e0 = (j == i0) || (chain_hi && w0 == cw);
-            e1 = (j == i1) || (chain_hi && w1 == cw);
-        }
-        const bool inner = __any_sync(0xffffffffu, r2.x <= te2 || r2.y <= te2);
-        if (inner) {
-            // row low parts re-read from L1 here rather than held in registers
-            const float4 B = sB[k], L0 = __ldg(plo + b0), L1 = __ldg(plo + b1);
-            const float2 lx = make_float2(L0.x, L1.x), ly = make_float2(L0.y, L1.y), lz = make_float2(L0.z, L1.z);
-            dx = __fadd2_rn(dx, __fadd2_rn(lx, f2(-B.x)));
-            dy = __fadd2_rn(dy, __fadd2_rn(ly, f2(-B.y)));
-            dz = __fadd2_rn(dz, __fadd2_rn(lz, f2(-B.z)));
-            r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-        }
-        float2 ri = make_float2(e0 ? 0.f : rsqrtf(r2.x), e1 ? 0.f : rsqrtf(r2.y));
-        float2 ri2 = __fmul2_rn(ri, ri);
-        float2 yv = __fmul2_rn(__ffma2_rn(fd, ri2, fc), ri);                     // y
-        float2 g = __fmul2_rn(__ffma2_rn(fb, ri2, fa), __fmul2_rn(ri2, ri));    // (x - y) / r^2
-        if (inner) {
-            // overlap constants re-read here: they are needed only inside the exact radius
-            const float tb2 = (float)(4.0 * sg.beta * sg.beta);
-            const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
-            const bool n0 = !e0 && r2.x <= tb2, n1 = !e1 && r2.y <= tb2;
-            if (n0) {
-                float r = r2.x * ri.x, x = nx0 + nx1 * r;
-                yv.x = ny0 + ny1 * r;
-                g.x = (x - yv.x) * ri2.x;
-            }
-            if (n1) {
-                float r = r2.y * ri.y, x = nx0 + nx1 * r;
-                yv.y = ny0 + ny1 * r;
-                g.y = (x - yv.y) * ri2.y;
-            }
-        }
-        // mob_a u = y u + (x - y)(d.u) d / r^2
-        float2 du = __ffma2_rn(dz, f2(C.y), __ffma2_rn(dy, f2(C.x), __fmul2_rn(dx, f2(A.w))));
-        float2 f = __fmul2_rn(g, du);
-        tx = __ffma2_rn(f, dx, __ffma2_rn(yv, f2(A.w), tx));
-        ty = __ffma2_rn(f, dy, __ffma2_rn(yv, f2(C.x), ty));
-        tz = __ffma2_rn(f, dz, __ffma2_rn(yv, f2(C.y), tz));
+    if (n) {
+        const float r = r2 * ri, x = nx0 + nx1 * r;
+        yv = ny0 + ny1 * r;
+        g = (x - yv) * ri2;
     }
 }
 
-__global__ void __launch_bounds__(AAF_THREADS, 16)
+template <bool CHECK>
+__device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sXY, const float4 *__restrict__ sZU,
+                                           const float4 *__restrict__ sUU, const float4 *__restrict__ sLA,
+                                           const float4 *__restrict__ sLB, int jt, int np, int iA, int iB,
+                                           bool chain_hi, float wA, float wB, float2 ax, float2 ay, float2 az,
+                                           float2 bx, float2 by, float2 bz, const float4 *__restrict__ plo, int bA,
+                                           int bB, float2 fa, float2 fb, float2 fc, float2 fd, const Seg &sg,
+                                           float te2, float2 (&t)[6])
+{
+#pragma unroll 1
+    for (int k = 0; k < np; k++) {
+        const float4 XY = sXY[k], ZU = sZU[k], UU = sUU[k];
+        float2 dA[3], dB[3];
+        dA[0] = __fadd2_rn(ax, make_float2(XY.x, XY.y)); dA[1] = __fadd2_rn(ay, make_float2(XY.z, XY.w));
+        dA[2] = __fadd2_rn(az, make_float2(ZU.x, ZU.y));
+        dB[0] = __fadd2_rn(bx, make_float2(XY.x, XY.y)); dB[1] = __fadd2_rn(by, make_float2(XY.z, XY.w));
+        dB[2] = __fadd2_rn(bz, make_float2(ZU.x, ZU.y));
+        float2 r2A = __ffma2_rn(dA[2], dA[2], __ffma2_rn(dA[1], dA[1], __fmul2_rn(dA[0], dA[0])));
+        float2 r2B = __ffma2_rn(dB[2], dB[2], __ffma2_rn(dB[1], dB[1], __fmul2_rn(dB[0], dB[0])));
+        bool eA0 = false, eA1 = false, eB0 = false, eB1 = false;
+        if constexpr (CHECK) {
+            const int j = jt + 2 * k;
+            const float4 LB = sLB[k];
+            eA0 = (j == iA) || (chain_hi && wA == LB.z);
+            eA1 = (j + 1 == iA) || (chain_hi && wA == LB.w);
+            eB0 = (j == iB) || (chain_hi && wB == LB.z);
+            eB1 = (j + 1 == iB) || (chain_hi && wB == LB.w);
+        }
+        const bool inner = __any_sync(0xffffffffu, fminf(fminf(r2A.x, r2A.y), fminf(r2B.x, r2B.y)) <= te2);
+        if (inner) {
+            const float4 LA = sLA[k], LB = sLB[k], RA = __ldg(plo + bA), RB = __ldg(plo + bB);
+            const float2 cx = make_float2(-LA.x, -LA.y), cy = make_float2(-LA.z, -LA.w), cz = make_float2(-LB.x, -LB.y);
+            dA[0] = __fadd2_rn(dA[0], __fadd2_rn(f2(RA.x), cx)); dA[1] = __fadd2_rn(dA[1], __fadd2_rn(f2(RA.y), cy));
+            dA[2] = __fadd2_rn(dA[2], __fadd2_rn(f2(RA.z), cz));
+            dB[0] = __fadd2_rn(dB[0], __fadd2_rn(f2(RB.x), cx)); dB[1] = __fadd2_rn(dB[1], __fadd2_rn(f2(RB.y), cy));
+            dB[2] = __fadd2_rn(dB[2], __fadd2_rn(f2(RB.z), cz));
+            r2A = __ffma2_rn(dA[2], dA[2], __ffma2_rn(dA[1], dA[1], __fmul2_rn(dA[0], dA[0])));
+            r2B = __ffma2_rn(dB[2], dB[2], __ffma2_rn(dB[1], dB[1], __fmul2_rn(dB[0], dB[0])));
+        }
+        const float2 riA = make_float2(eA0 ? 0.f : rsqrtf(r2A.x), eA1 ? 0.f : rsqrtf(r2A.y));
+        const float2 riB = make_float2(eB0 ? 0.f : rsqrtf(r2B.x), eB1 ? 0.f : rsqrtf(r2B.y));
+        const float2 ri2A = __fmul2_rn(riA, riA), ri2B = __fmul2_rn(riB, riB);
+        float2 yA = __fmul2_rn(__ffma2_rn(fd, ri2A, fc), riA), yB = __fmul2_rn(__ffma2_rn(fd, ri2B, fc), riB);
+        float2 gA = __fmul2_rn(__ffma2_rn(fb, ri2A, fa), __fmul2_rn(ri2A, riA));
+        float2 gB = __fmul2_rn(__ffma2_rn(fb, ri2B, fa), __fmul2_rn(ri2B, riB));
+        if (inner) {
+            const float tb2 = (float)(4.0 * sg.beta * sg.beta);
+            const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
+            aa_near_lane(!eA0 && r2A.x <= tb2, r2A.x, riA.x, ri2A.x, nx0, nx1, ny0, ny1, yA.x, gA.x);
+            aa_near_lane(!eA1 && r2A.y <= tb2, r2A.y, riA.y, ri2A.y, nx0, nx1, ny0, ny1, yA.y, gA.y);
+            aa_near_lane(!eB0 && r2B.x <= tb2, r2B.x, riB.x, ri2B.x, nx0, nx1, ny0, ny1, yB.x, gB.x);
+            aa_near_lane(!eB1 && r2B.y <= tb2, r2B.y, riB.y, ri2B.y, nx0, nx1, ny0, ny1, yB.y, gB.y);
+        }
+        // mob_a u = y u + (x - y)(d.u) d / r^2
+        const float2 u0 = make_float2(ZU.z, ZU.w), u1 = make_float2(UU.x, UU.y), u2 = make_float2(UU.z, UU.w);
+        const float2 hA = __fmul2_rn(gA, __ffma2_rn(dA[2], u2, __ffma2_rn(dA[1], u1, __fmul2_rn(dA[0], u0))));
+        const float2 hB = __fmul2_rn(gB, __ffma2_rn(dB[2], u2, __ffma2_rn(dB[1], u1, __fmul2_rn(dB[0], u0))));
+        t[0] = __ffma2_rn(hA, dA[0], __ffma2_rn(yA, u0, t[0]));
+        t[1] = __ffma2_rn(hA, dA[1], __ffma2_rn(yA, u1, t[1]));
+        t[2] = __ffma2_rn(hA, dA[2], __ffma2_rn(yA, u2, t[2]));
+        t[3] = __ffma2_rn(hB, dB[0], __ffma2_rn(yB, u0, t[3]));
+        t[4] = __ffma2_rn(hB, dB[1], __ffma2_rn(yB, u1, t[4]));
+        t[5] = __ffma2_rn(hB, dB[2], __ffma2_rn(yB, u2, t[5]));
+    }
+}
+
+__global__ void __launch_bounds__(AAF_THREADS, 12)
 k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const float4 *__restrict__ pos,
             const float4 *__restrict__ plo, const float *__restrict__ aa_te2, const double *__restrict__ u, int in_top,
             double *__restrict__ part, long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
 {
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
-    __shared__ float4 sA[128];   // hi x, y, z, u0
-    __shared__ float4 sB[128];   // lo x, y, z, chain
-    __shared__ float2 sC[128];   // u1, u2
+    __shared__ float4 sXY[64], sZU[64], sUU[64], sLA[64], sLB[64];
+    __shared__ float sK[12][AAF_THREADS];     // Kahan sums [0, 6) and compensations [6, 12), thread-private
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
     const int c = blockIdx.y;
     nchunk = sg.nch_aa;               // per-replica chunk count: a function of Nm alone
     if (c >= nchunk) return;
-    const int Nm = sg.Nm;
+    const int Nm = sg.Nm, tid = threadIdx.x;
     const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
-    const int i0 = tl.row0 + threadIdx.x, i1 = i0 + AAF_THREADS;
-    const bool a0 = threadIdx.x < tl.nrow, a1 = threadIdx.x + AAF_THREADS < tl.nrow;
+    const int iA = tl.row0 + tid, iB = iA + AAF_THREADS;
+    const bool actA = tid < tl.nrow, actB = tid + AAF_THREADS < tl.nrow;
     const int uoff = in_top ? sg.top_off : sg.vec_off;
-    const float4 P0 = pos[sg.bead_off + (a0 ? i0 : tl.row0)], P1 = pos[sg.bead_off + (a1 ? i1 : tl.row0)];
-    const int b0 = sg.bead_off + (a0 ? i0 : tl.row0), b1 = sg.bead_off + (a1 ? i1 : tl.row0);
-    const float2 px = make_float2(P0.x, P1.x), py = make_float2(P0.y, P1.y), pz = make_float2(P0.z, P1.z);
+    const int bA = sg.bead_off + (actA ? iA : tl.row0), bB = sg.bead_off + (actB ? iB : tl.row0);
+    const float4 PA = pos[bA], PB = pos[bB];
+    const float2 ax = f2(PA.x), ay = f2(PA.y), az = f2(PA.z), bx = f2(PB.x), by = f2(PB.y), bz = f2(PB.z);
     const bool chain_hi = sg.chain_HI != 0;
     const float2 fa = f2(sg.aa_c[0] - sg.aa_c[2]), fb = f2(sg.aa_c[1] - sg.aa_c[3]);
     const float2 fc = f2(sg.aa_c[2]), fd = f2(sg.aa_c[3]);
     const float te2 = aa_te2[tl.rep];
-    // Kahan sums across column tiles (sum, compensation per row and axis) live in
-    // shared memory, thread-private, so the pair loop keeps their registers
-    __shared__ float2 sKs[6][AAF_THREADS];
-    for (int q = 0; q < 6; q++) sKs[q][threadIdx.x] = f2(0.f);
+#pragma unroll
+    for (int q = 0; q < 12; q++) sK[q][tid] = 0.f;
     for (int jt = j0; jt < j1; jt += 128) {
-        const int nj = min(128, j1 - jt);
+        const int nj = min(128, j1 - jt), np = (nj + 1) >> 1;
         __syncthreads();
-        for (int t = threadIdx.x; t < nj; t += AAF_THREADS) {
-            const int j = jt + t;
-            const float4 A = pos[sg.bead_off + j], B = plo[sg.bead_off + j];
-            sA[t] = make_float4(A.x, A.y, A.z, (float)u[uoff + 3 * j]);
-            sB[t] = make_float4(B.x, B.y, B.z, A.w);
-            sC[t] = make_float2((float)u[uoff + 3 * j + 1], (float)u[uoff + 3 * j + 2]);
+        // one column pair per thread (64 pairs = 128 columns)
+        if (tid < np) {
+            float4 A[2], B[2];
+            float v[2][3];
+            for (int h = 0; h < 2; h++) {
+                const int jl = 2 * tid + h, j = jt + jl;
+                if (jl < nj) {
+                    A[h] = pos[sg.bead_off + j]; B[h] = plo[sg.bead_off + j];
+                    for (int a = 0; a < 3; a++) v[h][a] = (float)u[uoff + 3 * j + a];
+                } else {
+                    A[h] = make_float4(AAC_PAD, AAC_PAD, AAC_PAD, __int_as_float(0x7fc00000));
+                    B[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    v[h][0] = v[h][1] = v[h][2] = 0.f;
+                }
+            }
+            sXY[tid] = make_float4(-A[0].x, -A[1].x, -A[0].y, -A[1].y);
+            sZU[tid] = make_float4(-A[0].z, -A[1].z, v[0][0], v[1][0]);
+            sUU[tid] = make_float4(v[0][1], v[1][1], v[0][2], v[1][2]);
+            sLA[tid] = make_float4(B[0].x, B[1].x, B[0].y, B[1].y);
+            sLB[tid] = make_float4(B[0].z, B[1].z, A[0].w, A[1].w);
         }
         __syncthreads();
-        float2 tx = f2(0.f), ty = f2(0.f), tz = f2(0.f);
+        float2 t[6] = {f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f), f2(0.f)};
         // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
         const bool check = chain_hi || (jt < tl.row0 + 2 * AAF_THREADS && jt + nj > tl.row0);
         if (check)
-            aa_f2_cols<true>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, plo, b0, b1, fa,
-                             fb, fc, fd, sg, te2, tx, ty, tz);
+            aa_f2_cols<true>(sXY, sZU, sUU, sLA, sLB, jt, np, iA, iB, chain_hi, PA.w, PB.w, ax, ay, az, bx, by, bz,
+                             plo, bA, bB, fa, fb, fc, fd, sg, te2, t);
         else
-            aa_f2_cols<false>(sA, sB, sC, jt, nj, i0, i1, chain_hi, P0.w, P1.w, px, py, pz, plo, b0, b1, fa,
-                              fb, fc, fd, sg, te2, tx, ty, tz);
-        // Kahan across column tiles
-        const float2 t3[3] = {tx, ty, tz};
+            aa_f2_cols<false>(sXY, sZU, sUU, sLA, sLB, jt, np, iA, iB, chain_hi, PA.w, PB.w, ax, ay, az, bx, by, bz,
+                              plo, bA, bB, fa, fb, fc, fd, sg, te2, t);
+        // fold the two column lanes, then Kahan across column tiles
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const float2 sq = sKs[q][threadIdx.x], kq = sKs[3 + q][threadIdx.x];
-            const float2 yy = __fadd2_rn(t3[q], make_float2(-kq.x, -kq.y)), tt = __fadd2_rn(sq, yy);
-            sKs[3 + q][threadIdx.x] = __fadd2_rn(__fadd2_rn(tt, make_float2(-sq.x, -sq.y)), make_float2(-yy.x, -yy.y));
-            sKs[q][threadIdx.x] = tt;
+        for (int q = 0; q < 6; q++) {
+            const float x = t[q].x + t[q].y;
+            const float sq = sK[q][tid], kq = sK[6 + q][tid];
+            const float yy = x - kq, tt = sq + yy;
+            sK[6 + q][tid] = (tt - sq) - yy;
+            sK[q][tid] = tt;
         }
     }
-    const float2 sx = sKs[0][threadIdx.x], sy = sKs[1][threadIdx.x], sz = sKs[2][threadIdx.x];
     double *o = part + (long)c * part_stride + sg.top_off;
-    if (a0) { o[3 * i0] = sx.x; o[3 * i0 + 1] = sy.x; o[3 * i0 + 2] = sz.x; }
-    if (a1) { o[3 * i1] = sx.y; o[3 * i1 + 1] = sy.y; o[3 * i1 + 2] = sz.y; }
+    if (actA) { o[3 * iA] = sK[0][tid]; o[3 * iA + 1] = sK[1][tid]; o[3 * iA + 2] = sK[2][tid]; }
+    if (actB) { o[3 * iB] = sK[3][tid]; o[3 * iB + 1] = sK[4][tid]; o[3 * iB + 2] = sK[5][tid]; }
 }
 
 // ---------------------------------------------------------------------------
