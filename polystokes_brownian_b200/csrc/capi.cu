@@ -56,7 +56,7 @@ static void free_engine(Engine &E)
                     E.d_tab, E.d_stale, E.d_aa_last, E.d_delta, E.d_schurQ, E.d_schurL, E.d_schur_reps, E.d_ss_reps,
                     E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_cell, E.d_cell_start, E.d_cell_sorted,
                     E.d_cell_count, E.d_cellgeo, E.d_cell_offs, E.d_nbr_ptr, E.d_nbr, E.d_nbr_count, E.d_lubtab,
-                    E.d_luby, E.d_lub_diag, E.d_lub_ptr, E.d_lub_nbr, E.d_tmp_vel, E.d_tmp_vel2, E.d_zlub, E.d_D, E.d_z, E.d_v, E.d_xw, E.d_Rr[0],
+                    E.d_luby, E.d_lub_diag, E.d_lub_ptr, E.d_lub_nbr, E.d_lub_cidx, E.d_tmp_vel, E.d_tmp_vel2, E.d_zlub, E.d_D, E.d_z, E.d_v, E.d_xw, E.d_Rr[0],
                     E.d_Rr[1], E.d_Rr[2], E.d_W[0], E.d_W[1], E.d_W[2], E.d_mr, E.d_sinv, E.d_nactive,
                     E.d_rhs, E.d_X, E.d_Xd, E.d_Xdet, E.d_Wn, E.d_vdn, E.d_vdc, E.d_vb, E.d_up, E.d_ud,
                     E.d_drift, E.d_sb, E.d_fext, E.d_fb, E.d_wr, E.d_tmp_top, E.d_tmp_top2, E.d_lzV, E.d_lzT,

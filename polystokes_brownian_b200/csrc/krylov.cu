@@ -334,12 +334,35 @@ __global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, co
     const RBlk B = T.d_blk[blockIdx.x];
     const bool act = !lz[B.rep].done;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int i = 0; i <= j; i++) {
-        double v = 0.0;
-        if (act)
-            for (int e = threadIdx.x; e < B.len; e += RB_THREADS) v += V[(long)i * ldv + B.start + e] * q[B.start + e];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) sh[wid][i] = v;
+    // q held in registers (a block spans at most RB_EPT elements per thread);
+    // eight basis vectors per pass keep 8 x RB_EPT loads in flight.  Each dot is
+    // summed in element order and reduced by the same shuffle tree as one at a time.
+    double qv[RB_EPT];
+#pragma unroll
+    for (int k = 0; k < RB_EPT; k++) {
+        const int e = threadIdx.x + k * RB_THREADS;
+        qv[k] = (act && e < B.len) ? q[B.start + e] : 0.0;
+    }
+    for (int i0 = 0; i0 <= j; i0 += 8) {
+        double v[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            v[c] = 0.0;
+            if (act && i0 + c <= j) {
+                const double *Vi = V + (long)(i0 + c) * ldv + B.start;
+#pragma unroll
+                for (int k = 0; k < RB_EPT; k++) {
+                    const int e = threadIdx.x + k * RB_THREADS;
+                    if (e < B.len) v[c] += Vi[e] * qv[k];
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            double t = v[c];
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (lane == 0 && i0 + c <= j) sh[wid][i0 + c] = t;
+        }
     }
     __syncthreads();
     // block partial for i stored at d_part[(LZ_KMAX+1) * blk + i]
@@ -374,10 +397,28 @@ __global__ void k_lz_sub(RedTable T, const double *__restrict__ V, long ldv, dou
     const RBlk B = T.d_blk[blockIdx.x];
     if (lz[B.rep].done) return;
     const double *hr = h + (long)(LZ_KMAX + 1) * B.rep;
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        double acc = q[B.start + e];
-        for (int i = 0; i <= j; i++) acc -= hr[i] * V[(long)i * ldv + B.start + e];
-        q[B.start + e] = acc;
+    // the thread's RB_EPT elements advance together, so each basis vector's
+    // loads are independent; per element the subtraction order is i = 0..j
+    double acc[RB_EPT];
+#pragma unroll
+    for (int k = 0; k < RB_EPT; k++) {
+        const int e = threadIdx.x + k * RB_THREADS;
+        acc[k] = e < B.len ? q[B.start + e] : 0.0;
+    }
+#pragma unroll 4
+    for (int i = 0; i <= j; i++) {
+        const double hi = hr[i];
+        const double *Vi = V + (long)i * ldv + B.start;
+#pragma unroll
+        for (int k = 0; k < RB_EPT; k++) {
+            const int e = threadIdx.x + k * RB_THREADS;
+            if (e < B.len) acc[k] -= hi * Vi[e];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < RB_EPT; k++) {
+        const int e = threadIdx.x + k * RB_THREADS;
+        if (e < B.len) q[B.start + e] = acc[k];
     }
     if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start))
         alpha[(long)LZ_KMAX * B.rep + j] = (first ? 0.0 : alpha[(long)LZ_KMAX * B.rep + j]) + hr[j];

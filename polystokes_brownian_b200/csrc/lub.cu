@@ -186,6 +186,27 @@ __global__ void k_canon_fill(long ntot, const int *__restrict__ sptr, const int 
 }
 
 // build the symmetric partner list (which 3) and from it the canonical i<j list
+// canonical index of every symmetric-list entry (b, j): the position of
+// (min, max) in min's ascending canonical list, found once per list build so
+// the per-iteration gathers need no search; -1 if absent (lists disagree)
+__global__ void k_canon_map(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr,
+                            const int *__restrict__ cptr, const int *__restrict__ cnbr, int *__restrict__ cidx)
+{
+    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    for (int t = sptr[b]; t < sptr[b + 1]; t++) {
+        const long j = snbr[t];
+        const long lo = b < j ? b : j, hi = b < j ? j : b;
+        int qa = cptr[lo], qb = cptr[lo + 1];
+        const int qend = qb;
+        while (qb - qa > 1) {
+            int mid = (qa + qb) >> 1;
+            if (cnbr[mid] <= hi) qa = mid; else qb = mid;
+        }
+        cidx[t] = (qa < qend && cnbr[qa] == hi) ? qa : -1;
+    }
+}
+
 int lub_build(Engine &E, cudaStream_t st)
 {
     E.ps_setup_valid = false;     // new pair list
@@ -195,8 +216,10 @@ int lub_build(Engine &E, cudaStream_t st)
     // keep the symmetric list in the lubrication buffers
     if (np + 1 > E.lub_cap) {
         cudaFree(E.d_lub_nbr);
+        cudaFree(E.d_lub_cidx);
         E.lub_cap = np * 3 / 2 + 1024;
         PS_CK(cudaMalloc(&E.d_lub_nbr, sizeof(int) * E.lub_cap));
+        PS_CK(cudaMalloc(&E.d_lub_cidx, sizeof(int) * E.lub_cap));
     }
     PS_CK(cudaMemcpyAsync(E.d_lub_ptr, E.d_nbr_ptr, sizeof(int) * (E.ntot + 1), cudaMemcpyDeviceToDevice, st));
     if (np) PS_CK(cudaMemcpyAsync(E.d_lub_nbr, E.d_nbr, sizeof(int) * np, cudaMemcpyDeviceToDevice, st));
@@ -217,6 +240,8 @@ int lub_build(Engine &E, cudaStream_t st)
     if ((rc = exclusive_scan(E, E.d_nbr_count, E.d_lubc_ptr, E.ntot, st))) return rc;
     ::ps_launch_count++, k_canon_fill<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
                                                        E.d_lub_pairs);
+    ::ps_launch_count++, k_canon_map<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
+                                                      E.d_lub_cidx);
     E.lub_npairs = nc;
     PS_CK(cudaGetLastError());
     return PS_OK;

@@ -97,6 +97,7 @@ struct Engine {
     double *d_luby = nullptr, *d_lub_diag = nullptr, *d_tmp_vel = nullptr, *d_tmp_vel2 = nullptr;
     double *d_zlub = nullptr; long zlub_cap = 0;
     int *d_lub_ptr = nullptr, *d_lub_nbr = nullptr; long lub_cap = 0; long lub_npairs = 0;
+    int *d_lub_cidx = nullptr;       // per symmetric-list entry: its canonical pair index (-1: none)
     int *d_lubc_ptr = nullptr, *d_lubc_nbr = nullptr; int2 *d_lub_pairs = nullptr; long lubc_cap = 0;  // canonical
     // pair-space lubricated solve: per pair K^{1/2} and preconditioner blocks (12x12), CG vectors (12 per pair)
     double *d_pS = nullptr, *d_pP = nullptr, *d_py_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include "ps_internal.h"
 #include "ps_kernels.h"
+#include "ps_reduce.cuh"
 
 namespace ps {
 
@@ -501,60 +502,65 @@ __device__ __forceinline__ int find_rep(const int *__restrict__ offs, int R, lon
     return lo;
 }
 
-__global__ void k_combine(const Seg *__restrict__ segs, const int *__restrict__ offs, int R, long total, int mode,
-                          const double *__restrict__ x, const double *__restrict__ scale,
-                          const double *__restrict__ partAA, int nchAA, const double *__restrict__ partAB,
-                          const double *__restrict__ partBB, int nchBB, const double *__restrict__ partBA,
-                          const double *__restrict__ delta, const double *__restrict__ lub_y,
-                          long part_stride, double *__restrict__ y, const char *__restrict__ done, int done_stride)
+// One block per entry of the replica-aligned block table of the output layout
+// (saddle vectors for mode 0, mobility vectors for mode 1), so the replica is
+// known without a search and a converged replica's blocks leave at once.
+__global__ void k_combine(const Seg *__restrict__ segs, RedTable T, int mode, const double *__restrict__ x,
+                          const double *__restrict__ scale, const double *__restrict__ partAA, int nchAA,
+                          const double *__restrict__ partAB, const double *__restrict__ partBB, int nchBB,
+                          const double *__restrict__ partBA, const double *__restrict__ delta,
+                          const double *__restrict__ lub_y, long part_stride, double *__restrict__ y,
+                          const char *__restrict__ done, int done_stride)
 {
-    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= total) return;
-    int r = find_rep(offs, R, k);
+    const RBlk B = T.d_blk[blockIdx.x];
+    const int r = B.rep;
     if (done && *(const int *)(done + (long)r * done_stride)) return;   // converged replica: skip
     const Seg &sg = segs[r];
-    int i = (int)(k - offs[r]);
     const int xo = mode == 0 ? sg.vec_off : sg.top_off;
     const double s = scale ? scale[r] : 1.0;
-    double v = 0.0;
-    if (i < sg.nm3nc11) {
-        if (i < sg.nm3) {
-            v = sg.beta_inv * x[xo + i];
-            if (sg.mm_HI)
-                for (int c = 0; c < (nchAA ? sg.nch_aa : 0); c++) v += partAA[(long)c * part_stride + sg.top_off + i];
-            if (sg.Nc > 0) v += partAB[sg.top_off + i];
+    for (int e = threadIdx.x; e < B.len; e += blockDim.x) {
+        const long k = (long)B.start + e;
+        const int i = (int)(k - xo);
+        double v = 0.0;
+        if (i < sg.nm3nc11) {
+            if (i < sg.nm3) {
+                v = sg.beta_inv * x[xo + i];
+                if (sg.mm_HI)
+                    for (int c = 0; c < (nchAA ? sg.nch_aa : 0); c++) v += partAA[(long)c * part_stride + sg.top_off + i];
+                if (sg.Nc > 0) v += partAB[sg.top_off + i];
+            } else {
+                int j = i - sg.nm3;          // colloid-local DOF in [0, nc11)
+                int cidx, q;                 // colloid index, component
+                double self;
+                if (j < sg.nc3) { cidx = j / 3; q = j % 3; self = x[xo + i]; }
+                else if (j < sg.nc6) { cidx = (j - sg.nc3) / 3; q = 3 + (j - sg.nc3) % 3; self = 0.75 * x[xo + i]; }
+                else {
+                    cidx = (j - sg.nc6) / 5; q = 6 + (j - sg.nc6) % 5;
+                    int sb = xo + sg.nm3nc6 + 5 * cidx, p = q - 6;
+                    self = 1.8 * x[sb + p];
+                    if (p == 0) self += 0.9 * x[sb + 4];
+                    if (p == 4) self += 0.9 * x[sb + 0];
+                }
+                v = self;
+                if (sg.Nc >= 2)
+                    for (int c = 0; c < sg.nch_bb; c++) v += partBB[(long)c * part_stride + sg.top_off + i];
+                if (sg.Nm > 0)
+                    for (int t = 0; t < sg.n_mtiles; t++) v += partBA[((long)sg.ba_off + (long)t * sg.Nc + cidx) * 11 + q];
+                if (sg.shell_schur) {
+                    const double *D = delta + sg.schur_off + (long)j * sg.nc11;
+                    double acc = 0.0;
+                    for (int b = 0; b < sg.nc11; b++) acc += D[b] * x[xo + sg.nm3 + b];
+                    v += acc;
+                }
+            }
+            if (mode == 0 && i < sg.nm3nc6) v -= x[xo + sg.nm3nc11 + i];
         } else {
-            int j = i - sg.nm3;          // colloid-local DOF in [0, nc11)
-            int cidx, q;                 // colloid index, component
-            double self;
-            if (j < sg.nc3) { cidx = j / 3; q = j % 3; self = x[xo + i]; }
-            else if (j < sg.nc6) { cidx = (j - sg.nc3) / 3; q = 3 + (j - sg.nc3) % 3; self = 0.75 * x[xo + i]; }
-            else {
-                cidx = (j - sg.nc6) / 5; q = 6 + (j - sg.nc6) % 5;
-                int sb = xo + sg.nm3nc6 + 5 * cidx, p = q - 6;
-                self = 1.8 * x[sb + p];
-                if (p == 0) self += 0.9 * x[sb + 4];
-                if (p == 4) self += 0.9 * x[sb + 0];
-            }
-            v = self;
-            if (sg.Nc >= 2)
-                for (int c = 0; c < sg.nch_bb; c++) v += partBB[(long)c * part_stride + sg.top_off + i];
-            if (sg.Nm > 0)
-                for (int t = 0; t < sg.n_mtiles; t++) v += partBA[((long)sg.ba_off + (long)t * sg.Nc + cidx) * 11 + q];
-            if (sg.shell_schur) {
-                const double *D = delta + sg.schur_off + (long)j * sg.nc11;
-                double acc = 0.0;
-                for (int b = 0; b < sg.nc11; b++) acc += D[b] * x[xo + sg.nm3 + b];
-                v += acc;
-            }
+            int j = i - sg.nm3nc11;
+            v = -x[xo + j];
+            if (sg.lub_on && lub_y) v -= lub_y[sg.vel_off + j];
         }
-        if (mode == 0 && i < sg.nm3nc6) v -= x[xo + sg.nm3nc11 + i];
-    } else {
-        int j = i - sg.nm3nc11;
-        v = -x[xo + j];
-        if (sg.lub_on && lub_y) v -= lub_y[sg.vel_off + j];
+        y[k] = s * v;
     }
-    y[k] = s * v;
 }
 
 // ---------------------------------------------------------------------------
@@ -595,11 +601,9 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
         lub_apply(E, x, E.d_luby, st);
         lub_y = E.d_luby;
     }
-    long total = mode == 0 ? E.nvec : E.ntop;
-    const int *offs = mode == 0 ? E.d_vec_offs : E.d_top_offs;
-    int thr = 256;
-    ::ps_launch_count++, k_combine<<<(unsigned)((total + thr - 1) / thr), thr, 0, st>>>(
-        E.d_segs, offs, E.R, total, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
+    const RedTable &T = mode == 0 ? E.red : E.red_top;
+    ::ps_launch_count++, k_combine<<<(unsigned)T.nblk, RB_THREADS, 0, st>>>(
+        E.d_segs, T, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
         E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
 }
 

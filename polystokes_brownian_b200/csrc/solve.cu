@@ -455,8 +455,8 @@ k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ b
 // nm3nc6 entries of a mobility-layout vector and reduced into ||D^{-1} L y||^2
 // per bead (constraint-row entries of D)
 __global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
-                       const int *__restrict__ sptr, const int *__restrict__ snbr, const int *__restrict__ cptr,
-                       const int *__restrict__ cnbr, const double *__restrict__ S, const double *__restrict__ y,
+                       const int *__restrict__ sptr, const int *__restrict__ snbr, const int *__restrict__ cidx,
+                       const double *__restrict__ S, const double *__restrict__ y,
                        const double *__restrict__ add, double *__restrict__ vel, double *__restrict__ top,
                        const double *__restrict__ D, double *__restrict__ bead_part, const char *__restrict__ done,
                        int dstride)
@@ -470,23 +470,16 @@ __global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, cons
     const bool mono = i < s.Nm;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int t = sptr[b]; t < sptr[b + 1]; t++) {
-        long j = snbr[t];
-        const bool low = b < j;
-        long lo = low ? b : j, hi = low ? j : b;
-        int qa = cptr[lo], qb = cptr[lo + 1];
-        const int qend = qb;
-        while (qb - qa > 1) {
-            int mid = (qa + qb) >> 1;
-            if (cnbr[mid] <= hi) qa = mid; else qb = mid;
-        }
-        if (qa >= qend || cnbr[qa] != hi) continue;    // not in the canonical list (lists disagree)
+        const int qa = cidx[t];
+        if (qa < 0) continue;                           // not in the canonical list (lists disagree)
+        const bool low = b < (long)snbr[t];
         const double *Sq = S + 144L * qa, *yq = y + 12L * qa;
-        const int ng = mono ? 1 : 2;
+        const int ng = mono ? 1 : 2, nd = mono ? 6 : 12;    // monomer pairs: 6 x 6 block, zero elsewhere
         for (int g = 0; g < ng; g++)
             for (int k = 0; k < 3; k++) {
                 const int row = 6 * g + (low ? 0 : 3) + k;
                 double v = 0.0;
-                for (int c = 0; c < 12; c++) v += Sq[row * 12 + c] * yq[c];
+                for (int c = 0; c < nd; c++) v += Sq[row * 12 + c] * yq[c];
                 acc[3 * g + k] += v;
             }
     }
@@ -529,9 +522,11 @@ __global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *_
                (addv ? addv[s.vel_off + dof[k]] : 0.0);
     const double *Sq = S + 144L * q;
     double dot = 0.0;
+    // monomer pairs hold a 6 x 6 block (zero elsewhere): rows and columns past nd add nothing
     for (int a = 0; a < 12; a++) {
         double v = 0.0;
-        for (int c = 0; c < 12; c++) v += Sq[a * 12 + c] * z[c];
+        if (a < nd)
+            for (int c = 0; c < nd; c++) v += Sq[a * 12 + c] * z[c];
         v *= sign;
         if (p) { v += p[12 * q + a]; dot += p[12 * q + a] * v; }
         w[12 * q + a] = v;
@@ -540,17 +535,22 @@ __global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *_
 }
 
 // first iterate: y = 0, r = rhs (in rv), z = P r, p = z, part = r . z
-__global__ void k_ps_init(long npair, const double *__restrict__ P, double *__restrict__ yv,
+__global__ void k_ps_init(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
+                          const Seg *__restrict__ segs, const double *__restrict__ P, double *__restrict__ yv,
                           const double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ pv,
                           double *__restrict__ part)
 {
     long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npair) return;
+    const long lo = pairs[q].x;
+    const Seg &s = segs[rep_of_b(bead_offs, R, lo)];
+    const int nd = (lo - s.bead_off) < s.Nm ? 6 : 12;     // monomer pairs: 6 x 6 block, zero elsewhere
     const double *Pq = P + 144L * q;
     double dot = 0.0;
     for (int a = 0; a < 12; a++) {
         double v = 0.0;
-        for (int c = 0; c < 12; c++) v += Pq[a * 12 + c] * rv[12 * q + c];
+        if (a < nd)
+            for (int c = 0; c < nd; c++) v += Pq[a * 12 + c] * rv[12 * q + c];
         zv[12 * q + a] = v;
         pv[12 * q + a] = v;
         yv[12 * q + a] = 0.0;
@@ -561,25 +561,29 @@ __global__ void k_ps_init(long npair, const double *__restrict__ P, double *__re
 
 // y += alpha p ; r -= alpha Ap ; z = P r ; part = r . z
 __global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
-                            const PcgScal *__restrict__ pc, const double *__restrict__ P, const double *__restrict__ pv,
-                            const double *__restrict__ Ap, double *__restrict__ yv, double *__restrict__ rv,
-                            double *__restrict__ zv, double *__restrict__ part)
+                            const Seg *__restrict__ segs, const PcgScal *__restrict__ pc, const double *__restrict__ P,
+                            const double *__restrict__ pv, const double *__restrict__ Ap, double *__restrict__ yv,
+                            double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ part)
 {
     long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npair) return;
-    const PcgScal sc = pc[rep_of_b(bead_offs, R, pairs[q].x)];
+    const long lo = pairs[q].x;
+    const int r = rep_of_b(bead_offs, R, lo);
+    const PcgScal sc = pc[r];
     if (sc.done) return;
+    // monomer pairs: 6 x 6 blocks, and entries 6..11 of every pair vector stay zero
+    const int nd = (lo - segs[r].bead_off) < segs[r].Nm ? 6 : 12;
     double rq[12];
-    for (int a = 0; a < 12; a++) {
+    for (int a = 0; a < nd; a++) {
         yv[12 * q + a] += sc.alpha * pv[12 * q + a];
         rq[a] = rv[12 * q + a] - sc.alpha * Ap[12 * q + a];
         rv[12 * q + a] = rq[a];
     }
     const double *Pq = P + 144L * q;
     double dot = 0.0;
-    for (int a = 0; a < 12; a++) {
+    for (int a = 0; a < nd; a++) {
         double v = 0.0;
-        for (int c = 0; c < 12; c++) v += Pq[a * 12 + c] * rq[c];
+        for (int c = 0; c < nd; c++) v += Pq[a * 12 + c] * rq[c];
         zv[12 * q + a] = v;
         dot += rq[a] * v;
     }
@@ -1028,7 +1032,7 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
             k++;
             // Az = A z: u = [L z_y ; z_S] (z_S already in u), apply, z_y + L^T (...)_t
             ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                          E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, A.z.pair,
+                                                          E.d_lub_nbr, E.d_lub_cidx, E.d_pS, A.z.pair,
                                                           nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds);
             mr_apply(E, fp32, dn, ds, st);
             if (npair)
@@ -1123,14 +1127,15 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                 ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                                       E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
                                                                       (const char *)dn, ds);
-                ::ps_launch_count++, k_ps_init<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_pP, yv, rv, zv, pv, E.d_ppart);
+                ::ps_launch_count++, k_ps_init<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                                                                        E.d_segs, E.d_pP, yv, rv, zv, pv, E.d_ppart);
             }
         }
         ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
                                                       yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
         // initial residual ||D^{-1} L r||^2 + ||D^{-1} r_S||^2
         ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
-                                                      E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr, nullptr, nullptr,
+                                                      E.d_lub_cidx, E.d_pS, rv, nullptr, nullptr, nullptr,
                                                       E.d_D, bead_part, (const char *)dn, ds);
         ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA, sB,
                                                                       E.d_pcg, 1, maxit, E.d_nactive);
@@ -1142,7 +1147,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
             for (int j = 0; j < check_every && k < maxit; j++, k++) {
                 // Ap = p + L^T Mr L p  (joint replicas: [p_y + L^T (M u)_t ; (M u)_S], u = [L p_y ; p_S])
                 ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                              E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, pv, nullptr,
+                                                              E.d_lub_nbr, E.d_lub_cidx, E.d_pS, pv, nullptr,
                                                               nullptr, E.d_pu, nullptr, nullptr, (const char *)dn, ds);
                 mr_apply(E, fp32, dn, ds, st);
                 if (npair)
@@ -1155,12 +1160,12 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                                                                               nullptr, E.d_pcg, 0, maxit, E.d_nactive);
                 if (npair)
                     ::ps_launch_count++, k_ps_update<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                              E.d_pcg, E.d_pP, pv, Ap, yv, rv, zv,
-                                                                              E.d_ppart);
+                                                                              E.d_segs, E.d_pcg, E.d_pP, pv, Ap, yv, rv,
+                                                                              zv, E.d_ppart);
                 ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
                 ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                              E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, rv, nullptr,
+                                                              E.d_lub_nbr, E.d_lub_cidx, E.d_pS, rv, nullptr,
                                                               nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds);
                 ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA,
                                                                               sB, E.d_pcg, 2, maxit, E.d_nactive);
@@ -1177,7 +1182,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     }
     // F_t = -b_bot + L y (into u_t and the force rows), then U = Mr F_t - g, F_S
     ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
-                                                  E.d_lubc_ptr, E.d_lubc_nbr, E.d_pS, yv, cvel, tmp, E.d_pu, nullptr,
+                                                  E.d_lub_cidx, E.d_pS, yv, cvel, tmp, E.d_pu, nullptr,
                                                   nullptr, nullptr, 0);
     ::ps_launch_count++, k_ps_ft<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, tmp, x);
     ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
