@@ -454,52 +454,50 @@ __global__ void k_lz_init(RedTable T, const Seg *__restrict__ segs, double *__re
 // runs the scalar recurrences, all lanes rotate the eigenvector columns.
 __device__ void warp_tql(double *d, double *e, double *Z, int n)
 {
+    // Every lane runs the same scalar recurrence on the same shared d, e (so all
+    // lanes hold identical rotations without shuffles); lane 0 writes d, e back
+    // and each lane applies the rotations to its own rows of Z.
     const int lane = threadIdx.x & 31;
     for (int k = lane; k < n * n; k += 32) Z[k] = (k / n == k % n) ? 1.0 : 0.0;
     __syncwarp();
     for (int l = 0; l < n; l++) {
         int iter = 0;
         while (true) {
-            int m = l;
-            if (lane == 0) {
-                for (m = l; m < n - 1; m++) {
-                    double dd = fabs(d[m]) + fabs(d[m + 1]);
-                    if (fabs(e[m]) <= 1e-16 * dd) break;
-                }
+            int m;
+            for (m = l; m < n - 1; m++) {
+                double dd = fabs(d[m]) + fabs(d[m + 1]);
+                if (fabs(e[m]) <= 1e-16 * dd) break;
             }
-            m = __shfl_sync(0xffffffffu, m, 0);
             if (m == l || iter++ >= 60) break;
-            double g = 0, r = 0, s = 1, c = 1, p = 0;
-            if (lane == 0) {
-                g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-                r = hypot(g, 1.0);
-                g = d[m] - d[l] + e[l] / (g + copysign(r, g));
-            }
-            int i, brk = 0;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = hypot(g, 1.0);
+            g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+            double s = 1, c = 1, p = 0;
+            int i;
+            bool brk = false;
             for (i = m - 1; i >= l; i--) {
-                if (lane == 0) {
-                    double f = s * e[i], b = c * e[i];
-                    r = hypot(f, g);
-                    e[i + 1] = r;
-                    if (r == 0.0) { d[i + 1] -= p; e[m] = 0.0; brk = 1; }
-                    else {
-                        s = f / r; c = g / r;
-                        g = d[i + 1] - p;
-                        r = (d[i] - g) * s + 2.0 * c * b;
-                        p = s * r;
-                        d[i + 1] = g + p;
-                        g = c * r - b;
-                    }
+                const double ei = e[i], di = d[i], di1 = d[i + 1];
+                double f = s * ei, b = c * ei;
+                r = hypot(f, g);
+                const double rr = r;
+                __syncwarp();               // every lane has read this rotation's d, e
+                if (rr == 0.0) {
+                    if (lane == 0) { e[i + 1] = rr; d[i + 1] = di1 - p; e[m] = 0.0; }
+                    __syncwarp();
+                    brk = true;
+                    break;
                 }
-                brk = __shfl_sync(0xffffffffu, brk, 0);
-                if (brk) break;
-                double ss = __shfl_sync(0xffffffffu, s, 0), cc = __shfl_sync(0xffffffffu, c, 0);
+                s = f / rr; c = g / rr;
+                g = di1 - p;
+                r = (di - g) * s + 2.0 * c * b;
+                p = s * r;
+                if (lane == 0) { e[i + 1] = rr; d[i + 1] = g + p; }
+                g = c * r - b;
                 for (int k = lane; k < n; k += 32) {
-                    double f = Z[k * n + i + 1];
-                    Z[k * n + i + 1] = ss * Z[k * n + i] + cc * f;
-                    Z[k * n + i] = cc * Z[k * n + i] - ss * f;
+                    double fz = Z[k * n + i + 1];
+                    Z[k * n + i + 1] = s * Z[k * n + i] + c * fz;
+                    Z[k * n + i] = c * Z[k * n + i] - s * fz;
                 }
-                __syncwarp();
             }
             if (brk) continue;
             if (lane == 0) { d[l] -= p; e[l] = g; e[m] = 0.0; }

@@ -354,7 +354,9 @@ __device__ void pair_mobility(const Seg &s, const double *__restrict__ x, const 
 }
 
 // per pair: S = K^{1/2} and P = (I + S M_pp S)^{-1} (identity if not positive
-// definite); monomer pairs in closed form, colloid pairs by Jacobi + Cholesky
+// definite); monomer pairs in closed form as compact 6 x 6 blocks (row stride 6),
+// colloid pairs by Jacobi + Cholesky as 12 x 12 blocks; each pair owns a
+// 144-double slot in S and in P
 __global__ void __launch_bounds__(PS_THREADS)
 k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
            const Seg *__restrict__ segs, const double *__restrict__ x, const double *__restrict__ chain,
@@ -384,9 +386,9 @@ k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ b
             double t = 1.0 + l * mob[k];
             pm[k] = t > 0 ? 1.0 / t : 1.0;
         }
-        for (int k = 0; k < 144; k++) { So[k] = 0.0; Po[k] = 0.0; }
-        mono_pair_matrix(d, sq, So, 12);
-        mono_pair_matrix(d, pm, Po, 12);
+        // compact 6 x 6 blocks (row stride 6) at the start of the pair's slot
+        mono_pair_matrix(d, sq, So, 6);
+        mono_pair_matrix(d, pm, Po, 6);
         return;
     }
     const int nd = 12;
@@ -479,7 +481,7 @@ __global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, cons
             for (int k = 0; k < 3; k++) {
                 const int row = 6 * g + (low ? 0 : 3) + k;
                 double v = 0.0;
-                for (int c = 0; c < nd; c++) v += Sq[row * 12 + c] * yq[c];
+                for (int c = 0; c < nd; c++) v += Sq[row * nd + c] * yq[c];
                 acc[3 * g + k] += v;
             }
     }
@@ -526,7 +528,7 @@ __global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *_
     for (int a = 0; a < 12; a++) {
         double v = 0.0;
         if (a < nd)
-            for (int c = 0; c < nd; c++) v += Sq[a * 12 + c] * z[c];
+            for (int c = 0; c < nd; c++) v += Sq[a * nd + c] * z[c];
         v *= sign;
         if (p) { v += p[12 * q + a]; dot += p[12 * q + a] * v; }
         w[12 * q + a] = v;
@@ -550,7 +552,7 @@ __global__ void k_ps_init(long npair, const int2 *__restrict__ pairs, const int 
     for (int a = 0; a < 12; a++) {
         double v = 0.0;
         if (a < nd)
-            for (int c = 0; c < nd; c++) v += Pq[a * 12 + c] * rv[12 * q + c];
+            for (int c = 0; c < nd; c++) v += Pq[a * nd + c] * rv[12 * q + c];
         zv[12 * q + a] = v;
         pv[12 * q + a] = v;
         yv[12 * q + a] = 0.0;
@@ -583,7 +585,7 @@ __global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const in
     double dot = 0.0;
     for (int a = 0; a < nd; a++) {
         double v = 0.0;
-        for (int c = 0; c < nd; c++) v += Pq[a * 12 + c] * rq[c];
+        for (int c = 0; c < nd; c++) v += Pq[a * nd + c] * rq[c];
         zv[12 * q + a] = v;
         dot += rq[a] * v;
     }
@@ -799,10 +801,13 @@ __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs,
     int n;
     double *u_s = nullptr;
     const double *y_s = nullptr;
+    int nd = 12;          // pair blocks: 6 x 6 (row stride 6) for monomer pairs
     if (is_pair) {
         base = 12 * t;
         n = 12;
         bead = pairs[t].x;
+        const Seg &sp = segs[rep_of_b(bead_offs, R, bead)];
+        if (bead - sp.bead_off < sp.Nm) nd = 6;
     } else {
         bead = t - npair;
         const Seg &s0 = segs[rep_of_b(bead_offs, R, bead)];
@@ -828,7 +833,8 @@ __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs,
             const double *Pq = A.P + 144L * t;
             for (int a = 0; a < 12; a++) {
                 double acc = 0.0;
-                for (int c = 0; c < 12; c++) acc += Pq[a * 12 + c] * rv[c];
+                if (a < nd)
+                    for (int c = 0; c < nd; c++) acc += Pq[a * nd + c] * rv[c];
                 zv[a] = acc;
             }
         } else {
@@ -878,7 +884,8 @@ __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs,
             const double *Pq = A.P + 144L * t;
             for (int a = 0; a < 12; a++) {
                 double acc = 0.0;
-                for (int c = 0; c < 12; c++) acc += Pq[a * 12 + c] * rv[c];
+                if (a < nd)
+                    for (int c = 0; c < nd; c++) acc += Pq[a * nd + c] * rv[c];
                 zv[a] = acc;
             }
         } else {
