@@ -124,6 +124,10 @@ def pair_flops(systems):
     return f
 
 
+def colloid_pair_flops(systems):
+    return float(sum(FLOP_BB * s.params["Nc"] * (s.params["Nc"] - 1) for s in systems))
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -394,22 +398,30 @@ def run_b200(args):
     te = shard.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     e2e = job_beads * args.steps / (te * 1e-3)
 
-    # roofline of the dominant kernel (monomer-monomer pair kernel), timed live
+    # roofline of the dominant kernel, timed live: the monomer-monomer pair kernel,
+    # or the colloid-colloid FTS kernel (FP64 in both forms) for colloid-only workloads
     u = torch.randn(b.ntop, dtype=torch.float64, device="cuda")
-    ms_aa, ms_all, peak = C.c_double(0), C.c_double(0), C.c_double(0)
-    _capi.check(L.ps_time_kernel(b.h, 0, 10, _ptr(u), C.byref(ms_aa), b.stream), "ps_time_kernel")
-    _capi.check(L.ps_time_kernel(b.h, 3, 10, _ptr(u), C.byref(ms_all), b.stream), "ps_time_kernel")
-    _capi.check(L.ps_fma_peak(1 if prec == _capi.PS_PREC_FP64 else 0, C.byref(peak), b.stream), "ps_fma_peak")
+    ms_k, ms_all, peak = C.c_double(0), C.c_double(0), C.c_double(0)
     flops = pair_flops(systems)
-    achieved = flops / (ms_aa.value * 1e-3) / 1e12 if ms_aa.value > 0 else 0.0
-    roof = {"bound": "fp64" if prec == _capi.PS_PREC_FP64 else "fp32",
-            "kernel": "k_rpy_aa_f2" if prec == _capi.PS_PREC_MIXED else "k_rpy_aa",
+    if flops > 0:
+        which, fp64_peak = 0, prec == _capi.PS_PREC_FP64
+        kname = "k_rpy_aa_f2" if prec == _capi.PS_PREC_MIXED else "k_rpy_aa"
+        funit = f"{FLOP_AA} per directed monomer pair"
+    else:
+        flops = colloid_pair_flops(systems)
+        which, fp64_peak, kname = 2, True, "k_rpy_bb"
+        funit = f"{FLOP_BB} per directed colloid pair (FTS 11 x 11 block)"
+    _capi.check(L.ps_time_kernel(b.h, which, 10, _ptr(u), C.byref(ms_k), b.stream), "ps_time_kernel")
+    _capi.check(L.ps_time_kernel(b.h, 3, 10, _ptr(u), C.byref(ms_all), b.stream), "ps_time_kernel")
+    _capi.check(L.ps_fma_peak(1 if fp64_peak else 0, C.byref(peak), b.stream), "ps_fma_peak")
+    achieved = flops / (ms_k.value * 1e-3) / 1e12 if ms_k.value > 0 else 0.0
+    roof = {"bound": "fp64" if fp64_peak else "fp32", "kernel": kname,
             "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value if peak.value else None, "traffic": None,
             "peak_source": "measured FMA throughput of this GPU in bench.py (ps_fma_peak); CUDA-core work, "
                            "no tensor-core or HBM denominator applies",
-            "flop_per_launch": flops, "flop_unit": "40 per directed monomer pair",
-            "ms_per_launch": ms_aa.value, "ms_mobility_apply": ms_all.value}
+            "flop_per_launch": flops, "flop_unit": funit,
+            "ms_per_launch": ms_k.value, "ms_mobility_apply": ms_all.value}
     ntot = b.ntot
     b.close()
     del flush
