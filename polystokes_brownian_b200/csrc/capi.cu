@@ -51,7 +51,7 @@ static int upload(T *&dst, const std::vector<T> &v)
 static void free_engine(Engine &E)
 {
     void *ptrs[] = {E.d_segs, E.d_vec_offs, E.d_top_offs, E.d_vel_offs, E.d_bead_offs, E.d_x, E.d_q, E.d_xpos0,
-                    E.d_xn, E.d_pos64, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_chain, E.d_coll_rep, E.d_time, E.d_ktrap, E.d_trapinfo,
+                    E.d_xn, E.d_pos64, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_chain, E.d_coll_rep, E.d_chs, E.d_time, E.d_ktrap, E.d_trapinfo,
                     E.d_aa_tiles, E.d_ab_tiles, E.d_bb_tiles, E.d_partAA, E.d_partAB, E.d_partBB, E.d_partBA,
                     E.d_tab, E.d_stale, E.d_aa_last, E.d_delta, E.d_schurQ, E.d_schurL, E.d_schur_reps, E.d_ss_reps,
                     E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_cell, E.d_cell_start, E.d_cell_sorted,
@@ -166,7 +166,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
             for (int t = 0; t * TR < d.Nc; t++) bb.push_back({r, t * TR, std::min(TR, d.Nc - t * TR), t});
         bead_offs[r] = (int)bead; vec_offs[r] = (int)vec; top_offs[r] = (int)top; vel_offs[r] = (int)vel;
         cell_offs[r] = cells;
-        cells += 2L * d.Nm + 8;
+        cells += CELL_CAP_PER_MONO * d.Nm + CELL_CAP_BASE;
         bead += s.Np; coll += d.Nc; vec += s.n; top += s.nm3nc11; vel += s.nm3nc6;
         E.maxNp = std::max(E.maxNp, s.Np);
         if (d.kT > 0) kTpos++; else kTzero++;
@@ -281,6 +281,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_xn, sizeof(double) * 3 * bead);
     TRY_ALLOC(E.d_q, sizeof(double) * 4 * std::max<long>(coll, 1));
     TRY_ALLOC(E.d_xpos0, sizeof(double) * 3 * std::max<long>(coll, 1));
+    TRY_ALLOC(E.d_chs, sizeof(double) * 3 * std::max<long>(coll, 1));
     TRY_ALLOC(E.d_pos64, sizeof(double4) * bead);
     TRY_ALLOC(E.d_pos32, sizeof(float4) * bead);
     TRY_ALLOC(E.d_pos32lo, sizeof(float4) * bead);

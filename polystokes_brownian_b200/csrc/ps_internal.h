@@ -54,6 +54,11 @@ constexpr int BB_CHUNK_COLS = 64;
 // Row tile of the far-field pair kernels.
 struct Tile { int rep; int row0; int nrow; int mtile; };
 
+// Search-grid cell budget per replica: CELL_CAP_PER_MONO * Nm + CELL_CAP_BASE cells
+// (the longest axis is halved until the grid fits).  About one monomer per cell
+// inside a compact cluster, so a 27-cell stencil visits a few tens of candidates.
+constexpr long CELL_CAP_PER_MONO = 8, CELL_CAP_BASE = 64;
+
 template <class T> struct V4;
 template <> struct V4<double> { typedef double4 t; };
 template <> struct V4<float> { typedef float4 t; };

@@ -54,6 +54,7 @@ struct Engine {
     float *d_aa_te2 = nullptr;   // per replica: squared exact radius of the FP32 monomer kernel
     double *d_chain = nullptr;      // chain id per bead (monomers), -1-c for colloid c
     int *d_coll_rep = nullptr;      // replica of each colloid
+    double *d_chs = nullptr;        // per colloid: its colloid-monomer HS sum (3 doubles)
     double *d_time = nullptr;       // per replica time
     double *d_ktrap = nullptr;      // per replica (weaken_trap mutates it)
     double *d_trapinfo = nullptr;   // per replica: tstop, weaken_trap, unused

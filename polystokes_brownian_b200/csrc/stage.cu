@@ -104,7 +104,7 @@ __device__ __forceinline__ int cell_coord(double v, double org, double size, int
 // reference's because membership is decided by the same `dr < cutoff` test).
 // Geometry per replica: bounding box of the monomers (or the periodic box),
 // cells of edge >= rc (rc = rverl[0] = 0.05 + 2 beta, cell_list.cpp:26), with
-// the cell count capped at 2 Nm + 8 by coarsening the longest axis.
+// the cell count capped at CELL_CAP_PER_MONO Nm + CELL_CAP_BASE by halving the longest axis.
 // cellgeo per replica: org[3], size[3], nc[3], periodic  (10 doubles)
 __global__ void k_cell_geo(const Seg *__restrict__ segs, const double *__restrict__ x, double *__restrict__ geo,
                            const long *__restrict__ cell_off)
@@ -142,7 +142,7 @@ __global__ void k_cell_geo(const Seg *__restrict__ segs, const double *__restric
         }
         // cell counts are computed in double and clamped to [1, 2^20] before any
         // integer conversion, so non-finite or huge coordinates cannot overflow
-        double cap = pass == 0 ? 2.0 * s.Nm + 8.0 : 1e18;
+        double cap = pass == 0 ? (double)CELL_CAP_PER_MONO * s.Nm + (double)CELL_CAP_BASE : 1e18;
         int nc[3];
         double org[3], size[3], ext[3];
         int periodic = 0;
@@ -322,13 +322,52 @@ __device__ __forceinline__ double pair_geom(const Seg &s, const double *__restri
     return dr;
 }
 
+// Colloid-monomer HS sum of one colloid, one warp per colloid: lanes test 32
+// monomers at a time and lane 0 adds the hits in ascending monomer order, the
+// order (and the arithmetic) of a serial sweep over the replica's monomers.
+// Out: chs[3 c] = sum over monomers m of the colloid's hs_pair(m) term.
+__global__ void k_colloid_hs(long ncoll, const int *__restrict__ coll_rep, const Seg *__restrict__ segs,
+                             const double *__restrict__ x, double *__restrict__ chs)
+{
+    const long g = blockIdx.x;
+    if (g >= ncoll) return;
+    const int lane = threadIdx.x;
+    const Seg &s = segs[coll_rep[g]];
+    const long b = (long)s.bead_off + s.Nm + (g - s.coll_off);
+    const double k = s.hs_k, rv = (double)s.rverl[1], sig = (double)s.sig[1];
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    for (int m0 = 0; m0 < s.Nm; m0 += 32) {
+        const int m = m0 + lane;
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+        bool hit = false;
+        if (m < s.Nm) {
+            // pair (lo = monomer, hi = colloid); the colloid is the pair's second bead: sign +1
+            double e[3];
+            const double dr = pair_geom(s, x, (long)s.bead_off + m, b, e);
+            if (dr < rv) {
+                const double fm = hs_mag(dr, sig, k);
+                if (fm != 0.0) { hit = true; c0 = fm * e[0]; c1 = fm * e[1]; c2 = fm * e[2]; }
+            }
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, hit);
+        while (mask) {
+            const int src = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const double a0 = __shfl_sync(0xffffffffu, c0, src), a1 = __shfl_sync(0xffffffffu, c1, src),
+                         a2 = __shfl_sync(0xffffffffu, c2, src);
+            f0 += 1.0 * a0; f1 += 1.0 * a1; f2 += 1.0 * a2;
+        }
+    }
+    if (lane == 0) { chs[3 * g] = f0; chs[3 * g + 1] = f1; chs[3 * g + 2] = f2; }
+}
+
 __global__ void k_forces(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                          const double *__restrict__ x, const double *__restrict__ xpos0,
                          const double *__restrict__ geo, const long *__restrict__ cell_off,
                          const int *__restrict__ cstart, const int *__restrict__ csorted,
                          const int *__restrict__ bptr, const int *__restrict__ bnbr, const double *__restrict__ bsgn,
                          const double *__restrict__ time, double *__restrict__ ktrap, const double *__restrict__ trapinfo,
-                         double *__restrict__ rhs)
+                         const double *__restrict__ chs, double *__restrict__ rhs)
 {
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
@@ -383,7 +422,9 @@ __global__ void k_forces(long ntot, const int *__restrict__ bead_offs, int R, co
             });
         }
     } else {
-        for (int m = 0; m < s.Nm; m++) hs_pair((long)s.bead_off + m, 1);
+        // the sweep over the replica's monomers ran in k_colloid_hs, in the same order
+        const long g = (long)s.coll_off + (i - s.Nm);
+        f[0] = chs[3 * g]; f[1] = chs[3 * g + 1]; f[2] = chs[3 * g + 2];
         for (int c = 0; c < s.Nc; c++)
             if (s.Nm + c != i) hs_pair((long)s.bead_off + s.Nm + c, 2);
     }
@@ -459,10 +500,13 @@ int stage_rhs(Engine &E, int drift, const double *fext, double *rhs, cudaStream_
     ::ps_launch_count++, k_rhs_zero<<<(unsigned)((E.nvec + thr - 1) / thr), thr, 0, st>>>(E.nvec, E.d_vec_offs, E.R, E.d_segs, drift, fext,
                                                                      E.d_vel_offs, rhs);
     if (!drift) {
+        if (E.ncoll)
+            ::ps_launch_count++, k_colloid_hs<<<(unsigned)E.ncoll, 32, 0, st>>>(E.ncoll, E.d_coll_rep, E.d_segs, E.d_x,
+                                                                             E.d_chs);
         ::ps_launch_count++, k_forces<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
             E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_cellgeo, E.d_cell_offs,
             E.d_cell_start, E.d_cell_sorted, E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_time, E.d_ktrap,
-            E.d_trapinfo, rhs);
+            E.d_trapinfo, E.d_chs, rhs);
         ::ps_launch_count++, k_trap_weaken<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_segs, E.d_time, E.d_ktrap, E.d_trapinfo);
     }
     PS_CK(cudaGetLastError());
