@@ -1092,6 +1092,14 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     double *cvel = E.d_pV, *g = E.d_pg, *tmp = E.d_tmp_vel, *bead_part = E.d_pr;
     const void *dn = &E.d_pcg[0].done;
     const int ds = (int)sizeof(PcgScal);
+    // stresslet unknowns join the CG only for replicas beyond the dense stresslet
+    // limit; without such replicas k_ps_S has nothing to do but keep the per-bead
+    // stresslet partials at zero, which one clear at the start does
+    const bool joint = E.n_ss_polish > 0;
+    if (!joint) {
+        PS_CK(cudaMemsetAsync(sA, 0, sizeof(double) * E.ntot, st));
+        PS_CK(cudaMemsetAsync(sB, 0, sizeof(double) * E.ntot, st));
+    }
     PS_CK(cudaMemsetAsync(x, 0, sizeof(double) * E.nvec, st));
     PS_CK(cudaMemsetAsync(E.d_pu, 0, sizeof(double) * E.ntop, st));
     PS_CK(cudaMemsetAsync(E.d_pu2, 0, sizeof(double) * E.ntop, st));
@@ -1138,7 +1146,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                                                                         E.d_segs, E.d_pP, yv, rv, zv, pv, E.d_ppart);
             }
         }
-        ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
+        if (joint)
+            ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
                                                       yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
         // initial residual ||D^{-1} L r||^2 + ||D^{-1} r_S||^2
         ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
@@ -1161,7 +1170,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                     ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                           E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
                                                                           pv, Ap, E.d_ppart, (const char *)dn, ds);
-                ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 1, E.d_pcg, b, E.d_py,
+                if (joint)
+                    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 1, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, nullptr);
                 ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, nullptr, sA,
                                                                               nullptr, E.d_pcg, 0, maxit, E.d_nactive);
@@ -1169,7 +1179,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                     ::ps_launch_count++, k_ps_update<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                               E.d_segs, E.d_pcg, E.d_pP, pv, Ap, yv, rv,
                                                                               zv, E.d_ppart);
-                ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
+                if (joint)
+                    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
                 ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
                                                               E.d_lub_nbr, E.d_lub_cidx, E.d_pS, rv, nullptr,
@@ -1179,7 +1190,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                 if (npair)
                     ::ps_launch_count++, k_ps_dir<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                            E.d_pcg, zv, pv);
-                ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
+                if (joint)
+                    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
             }
             PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1192,7 +1204,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                                                   E.d_lub_cidx, E.d_pS, yv, cvel, tmp, E.d_pu, nullptr,
                                                   nullptr, nullptr, 0);
     ::ps_launch_count++, k_ps_ft<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, tmp, x);
-    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
+    if (joint)
+        ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
                                                   yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
     mr_apply(E, fp32, nullptr, 0, st);
     ::ps_launch_count++, k_ps_fin<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_py, E.d_py2, g, x);
