@@ -43,6 +43,10 @@ from polystokes_brownian_b200 import configs  # noqa: E402
 METRIC = "bead-steps/s"
 FLOP_AA = 40      # algorithmic FLOP per directed monomer-monomer pair (F-F RPY)
 FLOP_BB = 600     # per directed colloid-colloid FTS pair
+# DRAM bytes (read + write) of one launch of the roofline kernel, from one ncu
+# capture on the bench workload (profiles/k_rpy_aa_f2_ensemble256_lub.md:
+# dram__bytes_read.sum 16.47 MB + dram__bytes_write.sum 12.61 MB, chunk width 256)
+NCU_TRAFFIC = {("ensemble256_lub", "k_rpy_aa_f2"): {"bytes": 29.08e6, "chunk_cols": 256}}
 
 
 def parse():
@@ -417,7 +421,11 @@ def run_b200(args):
     achieved = flops / (ms_k.value * 1e-3) / 1e12 if ms_k.value > 0 else 0.0
     roof = {"bound": "fp64" if fp64_peak else "fp32", "kernel": kname,
             "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-            "frac": achieved / peak.value if peak.value else None, "traffic": None,
+            "frac": achieved / peak.value if peak.value else None,
+            "traffic": NCU_TRAFFIC.get((name, kname), {}).get("bytes"),
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at chunk width "
+                               f"{NCU_TRAFFIC[(name, kname)]['chunk_cols']} (compute-bound: the FLOP roofline "
+                               "applies)") if (name, kname) in NCU_TRAFFIC else None,
             "peak_source": "measured FMA throughput of this GPU in bench.py (ps_fma_peak); CUDA-core work, "
                            "no tensor-core or HBM denominator applies",
             "flop_per_launch": flops, "flop_unit": funit,
