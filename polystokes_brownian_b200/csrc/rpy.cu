@@ -40,6 +40,8 @@ template <> struct Acc<float> {
 // ---------------------------------------------------------------------------
 // AA: monomer rows x monomer columns (mm_HI only), 3 -> 3.
 // pos: (x,y,z,chain) per bead.  u: input vector, monomer F at off + 3 m.
+// Launched as k_rpy_aa<double> (the FP64 form); the mixed form runs
+// k_rpy_aa_f2 below, so the FP32 branches here are not instantiated.
 template <class T>
 __global__ void __launch_bounds__(RPY_THREADS, 4)
 k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
