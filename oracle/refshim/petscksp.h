@@ -1,0 +1,2 @@
+/* oracle build of the reference sources: PETSc/SLEPc names come from refshim.h */
+#include "refshim.h"
