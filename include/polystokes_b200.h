@@ -2,9 +2,11 @@
  * polystokes_b200.h -- C-ABI of the B200-native PolyStokes per-timestep hot path.
  *
  * One context holds a batch of independent systems ("replicas"); a single
- * PolyStokes system is a batch of one.  Every vector argument is a DEVICE
- * pointer to the concatenation of the replicas' segments, each laid out exactly
- * as the reference lays out its PETSc vectors:
+ * PolyStokes system is a batch of one.  Vector arguments are DEVICE pointers
+ * to the concatenation of the replicas' segments, except where a declaration
+ * says otherwise (ps_set_state, ps_step_inputs' noise arrays and ps_set_aux also
+ * accept host pointers; ps_obs_read writes host arrays).  Each segment is laid
+ * out exactly as the reference lays out its PETSc vectors:
  *
  *   saddle vector (length n = 6 Nm + 17 Nc per replica):
  *     [ F_m (3Nm) | F_c (3Nc) | T_c (3Nc) | S_c (5Nc) | U_m (3Nm) | U_c (3Nc) | W_c (3Nc) ]
@@ -43,7 +45,10 @@ extern "C" {
 #define PS_ERR_UNSUPPORTED (-5)
 #define PS_ERR_TOO_LARGE (-6)
 
-/* AB translational block mode: reference-faithful or RPY. */
+/* AB (monomer-colloid) translational block mode: the reference's assembly
+ * (mob.cpp:447-453, 845-904: zero in the shell path, the stale last monomer-pair
+ * tensor in the dense path) or the unequal-radii far-field RPY scalars
+ * (mob.cpp:410-411). */
 #define PS_AB_REFERENCE 0
 #define PS_AB_RPY 1
 /* PS_AB_RPY with the overlap and full-overlap branches of the unequal-radii RPY

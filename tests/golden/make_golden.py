@@ -14,7 +14,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: python tests/golden/make_golden.py <reference project path>")
+REF = sys.argv[1]
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
