@@ -90,7 +90,9 @@ typedef struct ps_desc {
     int32_t ab_mode;    /* PS_AB_REFERENCE | PS_AB_RPY | PS_AB_RPY_REG */
     double hs_kpref;    /* HS_KPREF, default 1.0 */
     int32_t hs_kmode;   /* HS_KMODE, default 0 */
-    int32_t lanczos_nc; /* POLYSTOKES_LANCZOS_NC, default 64 */
+    int32_t lanczos_nc; /* POLYSTOKES_LANCZOS_NC (slip_vel.cpp:283-288): shell replicas with
+                           nc11 above it (or above 64, the dense limit here) take the Schur
+                           Lanczos noise; 0 sends every shell replica there; negative = 64 */
     int32_t lub_on;     /* near-field lubrication (not in the reference) */
     double lub_gap;     /* lubricated pairs: gap < lub_gap * radius */
     int32_t aa_mode;    /* PS_AA_REFERENCE | PS_AA_RPY: monomer-monomer scalars */
@@ -195,7 +197,10 @@ int ps_obs_read(ps_ctx *ctx, ps_obs_out *out, void *stream);
 
 /* state --------------------------------------------------------------------- */
 /* x (3 Np per replica), q (4 Nc per replica): device or host pointers; reads
- * into host memory are complete when the call returns. */
+ * into host memory are complete when the call returns.  Host inputs are checked
+ * before any copy or launch: a non-finite coordinate or quaternion component
+ * returns PS_ERR_ARG (ps_last_error names the index) and leaves the state as it
+ * was.  Device inputs are taken as given. */
 int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream);
 int ps_get_state(ps_ctx *ctx, double *x, double *q, void *stream);
 int ps_set_time(ps_ctx *ctx, double t);

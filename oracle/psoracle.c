@@ -768,7 +768,7 @@ void or_schur_sync(or_sim *s)
 {
     if (s->p.mm_HI) return;
     int n = s->nc11, nm3 = s->nm3;
-    int thr = s->p.lanczos_nc > 0 ? s->p.lanczos_nc : 64;
+    int thr = s->p.lanczos_nc >= 0 ? s->p.lanczos_nc : 64;
     if (n > thr || n == 0) return;
     double *S = (double *)malloc(sizeof(double) * n * n);
     for (int a = 0; a < n; a++)
@@ -1268,18 +1268,59 @@ void or_slip_noise(or_sim *s, const double *fb, double *W)
         double acc = 0; for (int k = 0; k < nm3; k++) acc += s->Mcm[a * nm3 + k] * fb[k];
         uc[a] = acc * sqrt(s->p.beta);
     }
-    int thr = s->p.lanczos_nc > 0 ? s->p.lanczos_nc : 64;
+    int thr = s->p.lanczos_nc >= 0 ? s->p.lanczos_nc : 64;
     if (nc > thr) {
-        /* schur_sqrt_lanczos: S q = Mcc q - beta Mcm (Mcm^T q), kmax 40 */
-        double *S = (double *)malloc(sizeof(double) * nc * nc);
-        for (int a = 0; a < nc; a++) for (int b = 0; b < nc; b++) {
-            double acc = 0; for (int k = 0; k < nm3; k++) acc += s->Mcm[a * nm3 + k] * s->Mcm[b * nm3 + k];
-            S[a * nc + b] = s->Mcc_block[a * nc + b] - s->p.beta * acc;
+        /* schur_sqrt_lanczos, slip_vel.cpp:351-477: S q = Mcc q - beta Mcm (Mcm^T q) applied
+         * matrix-free; k <= min(40, nc11) vectors, two-pass reorthogonalisation, stop on an
+         * invariant subspace (||w|| <= 1e-12 ||b||) or the cap; sqrt of the projected
+         * tridiagonal with negative eigenvalues floored at 0. */
+        const double *b = fb + nm3;
+        double b0 = sqrt(dot(b, b, nc));
+        if (b0 > 0.0) {
+            int kmax = nc < 40 ? nc : 40;
+            double *V = (double *)malloc(sizeof(double) * (size_t)nc * kmax);
+            double *w = (double *)malloc(sizeof(double) * nc), *tm = (double *)malloc(sizeof(double) * nm3 + 8);
+            double *al = (double *)calloc(kmax, sizeof(double)), *be = (double *)calloc(kmax, sizeof(double));
+            for (int i = 0; i < nc; i++) V[i] = b[i] / b0;
+            int m = 0;
+            for (int j = 0; j < kmax; j++) {
+                const double *qj = V + (size_t)j * nc;
+                for (int k = 0; k < nm3; k++) {
+                    double acc = 0; for (int a = 0; a < nc; a++) acc += s->Mcm[a * nm3 + k] * qj[a];
+                    tm[k] = acc;
+                }
+                for (int a = 0; a < nc; a++) {
+                    double sq = 0; for (int k = 0; k < nm3; k++) sq += s->Mcm[a * nm3 + k] * tm[k];
+                    double cq = 0; for (int c = 0; c < nc; c++) cq += s->Mcc_block[a * nc + c] * qj[c];
+                    w[a] = cq - s->p.beta * sq;
+                }
+                if (j > 0) for (int a = 0; a < nc; a++) w[a] -= be[j - 1] * V[(size_t)(j - 1) * nc + a];
+                al[j] = dot(qj, w, nc);
+                for (int a = 0; a < nc; a++) w[a] -= al[j] * qj[a];
+                for (int pass = 0; pass < 2; pass++)
+                    for (int i = 0; i <= j; i++) {
+                        double h = dot(V + (size_t)i * nc, w, nc);
+                        for (int a = 0; a < nc; a++) w[a] -= h * V[(size_t)i * nc + a];
+                    }
+                m = j + 1;
+                double bj = sqrt(dot(w, w, nc));
+                if (bj <= 1e-12 * b0 || j == kmax - 1) break;
+                be[j] = bj;
+                for (int a = 0; a < nc; a++) V[(size_t)(j + 1) * nc + a] = w[a] / bj;
+            }
+            double *T = (double *)calloc((size_t)m * m, sizeof(double)), *Q = (double *)malloc(sizeof(double) * m * m);
+            double *lam = (double *)malloc(sizeof(double) * m);
+            for (int a = 0; a < m; a++) T[a * m + a] = al[a];
+            for (int a = 0; a + 1 < m; a++) { T[a * m + a + 1] = be[a]; T[(a + 1) * m + a] = be[a]; }
+            or_jacobi_eig(T, m, lam, Q);
+            for (int a = 0; a < m; a++) {
+                double g = 0;
+                for (int c = 0; c < m; c++) g += Q[a * m + c] * (lam[c] > 0 ? sqrt(lam[c]) : 0.0) * Q[0 * m + c];
+                g *= b0;
+                for (int i = 0; i < nc; i++) uc[i] += g * V[(size_t)a * nc + i];
+            }
+            free(V); free(w); free(tm); free(al); free(be); free(T); free(Q); free(lam);
         }
-        double *t = (double *)malloc(sizeof(double) * nc);
-        or_sqrtm_eig(S, nc, fb + nm3, t);   /* converged Lanczos == eigen sqrt */
-        for (int a = 0; a < nc; a++) uc[a] += t[a];
-        free(S); free(t);
     } else {
         const double *Q = s->schurQ;
         double *yv = (double *)malloc(sizeof(double) * (size_t)(nc > 0 ? nc : 1));

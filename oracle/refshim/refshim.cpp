@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstring>
+#include <ctime>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -96,6 +97,17 @@ PetscErrorCode PetscInitialized(PetscBool *f) { *f = g_init ? PETSC_TRUE : PETSC
 PetscErrorCode PetscFinalized(PetscBool *f) { *f = g_final ? PETSC_TRUE : PETSC_FALSE; return 0; }
 PetscErrorCode PetscLogDefaultBegin(void) { return 0; }
 PetscErrorCode PetscLogView(PetscViewer) { return 0; }
+static double g_first_event = -1.0;
+void refshim_event_begin(PetscLogEvent)
+{
+    if (g_first_event < 0) {
+        struct timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        g_first_event = (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+    }
+}
+extern "C" __attribute__((visibility("default"))) double refshim_first_event_time(void) { return g_first_event; }
+
 PetscErrorCode PetscLogEventRegister(const char *, PetscClassId, PetscLogEvent *ev)
 {
     static int next = 1;
@@ -747,6 +759,51 @@ PetscErrorCode MFNSetFromOptions(MFN) { return 0; }
 PetscErrorCode MFNSetOperator(MFN mfn, Mat A) { mfn->A = A; return 0; }
 PetscErrorCode MFNGetConvergedReason(MFN mfn, MFNConvergedReason *r) { *r = mfn->reason; return 0; }
 
+/* symmetric tridiagonal eigenproblem by implicit QL with Wilkinson shifts (Golub & Van Loan,
+ * sec. 8.3): d (diagonal, n) and e (sub-diagonal, n-1; e[n-1] scratch) in, d = eigenvalues and
+ * Z (n x n, row-major, Z[i*n + c] = component i of eigenvector c) out */
+static void tql(std::vector<double> &d, std::vector<double> &e, std::vector<double> &Z, int n)
+{
+    Z.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) Z[(size_t)i * n + i] = 1.0;
+    e.resize((size_t)n + 1, 0.0);
+    for (int l = 0; l < n; l++) {
+        for (int iter = 0; iter < 60; iter++) {
+            int m;
+            for (m = l; m < n - 1; m++) {
+                double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                if (std::fabs(e[m]) <= 1e-16 * dd) break;
+            }
+            if (m == l) break;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = std::hypot(g, 1.0);
+            g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
+            double s = 1, c = 1, p = 0;
+            int i;
+            bool early = false;
+            for (i = m - 1; i >= l; i--) {
+                double f = s * e[i], b = c * e[i];
+                r = std::hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0) { d[i + 1] -= p; e[m] = 0.0; early = true; break; }
+                s = f / r; c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * s + 2.0 * c * b;
+                p = s * r;
+                d[i + 1] = g + p;
+                g = c * r - b;
+                for (int k = 0; k < n; k++) {
+                    double fz = Z[(size_t)k * n + i + 1];
+                    Z[(size_t)k * n + i + 1] = s * Z[(size_t)k * n + i] + c * fz;
+                    Z[(size_t)k * n + i] = c * Z[(size_t)k * n + i] - s * fz;
+                }
+            }
+            if (early) continue;
+            d[l] -= p; e[l] = g; e[m] = 0.0;
+        }
+    }
+}
+
 PetscErrorCode MFNSolve(MFN mfn, Vec b, Vec x)
 {
     Mat A = mfn->A;
@@ -756,7 +813,10 @@ PetscErrorCode MFNSolve(MFN mfn, Vec b, Vec x)
     std::vector<PetscScalar> out((size_t)n, 0.0);
     mfn->reason = 1;
     if (b0 > 0) {
-        const PetscInt kmax = std::min<PetscInt>(n, 400);
+        /* Lanczos with full reorthogonalisation; every 5 vectors (and at the end) the estimate
+         * b0 Q_m sqrt(T_m) e1 is formed and the run stops when it changed by <= 1e-13
+         * relative, or at once if T_m has a negative eigenvalue (no real square root) */
+        const PetscInt kmax = std::min<PetscInt>(n, 300);
         std::vector<std::vector<PetscScalar>> Q;
         std::vector<PetscReal> al, be, gprev;
         Q.push_back(in);
@@ -779,36 +839,34 @@ PetscErrorCode MFNSolve(MFN mfn, Vec b, Vec x)
                     PetscReal h = dotv(Q[l], w->a);
                     for (PetscInt i = 0; i < n; i++) w->a[i] -= h * Q[l][i];
                 }
-            /* sqrt(T_m) e1 on the current projection */
-            const PetscInt m = j + 1;
-            std::vector<PetscScalar> T((size_t)m * m, 0.0);
-            for (PetscInt i = 0; i < m; i++) T[i + (size_t)i * m] = al[i];
-            for (PetscInt i = 0; i + 1 < m; i++) { T[i + 1 + (size_t)i * m] = be[i]; T[i + (size_t)(i + 1) * m] = be[i]; }
-            std::vector<PetscReal> th((size_t)m);
-            jacobi_eig(m, T.data(), m, th.data(), true);
-            neg = false;
-            g.assign((size_t)m, 0.0);
-            for (PetscInt i = 0; i < m; i++) {
-                PetscReal gi = 0;
-                for (PetscInt l = 0; l < m; l++) {
-                    if (th[l] < 0) neg = true;
-                    gi += T[i + (size_t)l * m] * std::sqrt(std::max(th[l], 0.0)) * T[(size_t)l * m];
-                }
-                g[i] = b0 * gi;
-            }
             PetscReal bj = std::sqrt(dotv(w->a, w->a));
-            bool conv = false;
-            if (!gprev.empty()) {
-                PetscReal dn = 0, gn = 0;
-                for (PetscInt i = 0; i < m; i++) {
-                    PetscReal gp = i < (PetscInt)gprev.size() ? gprev[i] : 0.0;
-                    dn += (g[i] - gp) * (g[i] - gp);
-                    gn += g[i] * g[i];
+            const bool last = bj <= 1e-14 * b0 || j == kmax - 1;
+            if ((j + 1) % 5 == 0 || last) {
+                const int m = (int)j + 1;
+                std::vector<double> d(al.begin(), al.end()), e(be.begin(), be.end()), Z;
+                e.resize((size_t)m, 0.0);
+                tql(d, e, Z, m);
+                neg = false;
+                g.assign((size_t)m, 0.0);
+                for (int c = 0; c < m; c++) {
+                    if (d[c] < 0) { neg = true; continue; }
+                    const double wc = std::sqrt(d[c]) * Z[c];   /* sqrt(theta_c) U[0,c] */
+                    for (int i = 0; i < m; i++) g[i] += Z[(size_t)i * m + c] * wc;
                 }
-                conv = dn <= 1e-26 * gn;
+                for (auto &gi : g) gi *= b0;
+                bool conv = false;
+                if (!gprev.empty()) {
+                    PetscReal dn = 0, gn = 0;
+                    for (int i = 0; i < m; i++) {
+                        PetscReal gp = i < (int)gprev.size() ? gprev[i] : 0.0;
+                        dn += (g[i] - gp) * (g[i] - gp);
+                        gn += g[i] * g[i];
+                    }
+                    conv = dn <= 1e-26 * gn;
+                }
+                gprev = g;
+                if (neg || conv || last) break;
             }
-            gprev = g;
-            if (conv || bj <= 1e-14 * b0 || j == kmax - 1) break;
             be.push_back(bj);
             Q.push_back(w->a);
             for (auto &e : Q.back()) e /= bj;

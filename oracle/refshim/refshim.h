@@ -18,9 +18,10 @@
  *     Matrix Computations, 4th ed., sec. 8.5), eigenvalues ascending,
  *     eigenvectors in the columns.
  *   - SLEPc MFN with FNSQRT: sqrt(M) b by symmetric Lanczos with full
- *     reorthogonalisation, sqrt taken on the projected tridiagonal, stopped when
- *     the estimate changes by less than 1e-13 relative; a negative projected
- *     eigenvalue (M indefinite) reports a negative converged reason.
+ *     reorthogonalisation, sqrt taken on the projected tridiagonal (implicit QL,
+ *     Golub & Van Loan sec. 8.3) every 5 vectors, stopped when the estimate
+ *     changes by less than 1e-13 relative; a negative projected eigenvalue (M
+ *     indefinite: no real square root) stops it with a negative converged reason.
  *   - MPI: one rank; collectives copy.
  * Everything the reference computes in its own code (geometry, tensors,
  * assembly, forces, drift, integrator, Schur floor, output) stays the
@@ -129,7 +130,10 @@ PetscErrorCode PetscPrintf(MPI_Comm comm, const char *fmt, ...);
 PetscErrorCode PetscLogDefaultBegin(void);
 PetscErrorCode PetscLogView(PetscViewer v);
 PetscErrorCode PetscLogEventRegister(const char *name, PetscClassId cls, PetscLogEvent *ev);
-inline PetscErrorCode PetscLogEventBegin(PetscLogEvent, int, int, int, int) { return 0; }
+/* the first event of a run is check_dist() of step 1 (run.cpp:72-73): its time marks the end of
+ * init() and fill_self(); refshim_first_event_time() returns it (CLOCK_MONOTONIC seconds) */
+void refshim_event_begin(PetscLogEvent ev);
+inline PetscErrorCode PetscLogEventBegin(PetscLogEvent ev, int, int, int, int) { refshim_event_begin(ev); return 0; }
 inline PetscErrorCode PetscLogEventEnd(PetscLogEvent, int, int, int, int) { return 0; }
 inline PetscReal PetscRealPart(PetscScalar a) { return a; }
 inline PetscReal PetscAbsScalar(PetscScalar a) { return std::fabs(a); }

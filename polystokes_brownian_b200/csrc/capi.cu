@@ -68,7 +68,8 @@ static void free_engine(Engine &E)
                     E.d_pmp[0], E.d_pmp[1], E.d_pmp[2], E.d_pmp[3], E.d_pmp[4], E.d_pmp[5], E.d_pmp[6],
                     E.d_pmp[7], E.d_pmp[8], E.d_pmp[9], E.d_pms[0], E.d_pms[1], E.d_pms[2], E.d_pms[3],
                     E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8], E.d_obs_acc, E.d_obs_prev,
-                    E.d_obs_ring, E.d_obs_msd, E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.d_obs_msdn};
+                    E.d_obs_ring, E.d_obs_msd, E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.d_obs_msdn,
+                    E.d_sl_reps, E.d_sl_skip, E.d_slV, E.d_slT, E.d_sl_sc, E.d_sl_u, E.d_sl_y, E.d_sl_y2};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -88,7 +89,8 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     std::vector<int> bead_offs(R + 1), vec_offs(R + 1), top_offs(R + 1), vel_offs(R + 1);
     std::vector<long> cell_offs(R + 1);
     std::vector<Tile> aa, ab, bb;
-    std::vector<int> schur_reps, ss_reps;
+    std::vector<int> schur_reps, ss_reps, sl_reps;
+    long slv = 0;
     int ss_polish = 0;
     const int TR = 128;
     int kTpos = 0, kTzero = 0;
@@ -138,11 +140,13 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
             const double c[8] = {0.375, -2.0, 0.75, -0.5, -1.0, 0.375, 1.0, -0.28125};
             for (int k = 0; k < 8; k++) s.aa_c[k] = (float)c[k];
         }
-        int lnc = d.lanczos_nc > 0 ? d.lanczos_nc : 64;
+        // crossover of slip_vel.cpp:283-288 (POLYSTOKES_LANCZOS_NC; 0 forces the Lanczos noise)
+        int lnc = d.lanczos_nc >= 0 ? d.lanczos_nc : 64;
         s.shell_schur = (!d.mm_HI && d.Nc > 0 && s.nc11 <= lnc && s.nc11 <= PS_MAX_NC11_SCHUR);
+        s.sl_slot = -1; s.sl_off = 0;
         if (!d.mm_HI && d.Nc > 0 && !s.shell_schur && d.kT > 0) {
-            ps::set_error("shell path with nc11 above the dense Schur limit needs the Schur Lanczos noise (not built)");
-            return PS_ERR_UNSUPPORTED;
+            s.sl_slot = (int)sl_reps.size(); s.sl_off = (int)slv; sl_reps.push_back(r);
+            slv += (long)(SL_KMAX + 1) * s.nc11;
         }
         if (s.shell_schur) { s.schur_off = (int)schur; schur += (long)s.nc11 * s.nc11; schur_reps.push_back(r); }
         if (d.Nc > 0) {
@@ -210,6 +214,19 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     if ((rc = upload(E.d_schur_reps, schur_reps))) return rc;
     if ((rc = upload(E.d_ss_reps, ss_reps))) return rc;
     E.n_ss_reps = (int)ss_reps.size();
+    E.n_sl_reps = (int)sl_reps.size();
+    if (E.n_sl_reps) {
+        std::vector<int> skip(R, 1);
+        for (int r : sl_reps) skip[r] = 0;
+        if ((rc = upload(E.d_sl_reps, sl_reps))) return rc;
+        if ((rc = upload(E.d_sl_skip, skip))) return rc;
+        TRY_ALLOC(E.d_slV, sizeof(double) * slv);
+        TRY_ALLOC(E.d_slT, sizeof(double) * 2 * SL_KMAX * E.n_sl_reps);
+        TRY_ALLOC(E.d_sl_sc, 32 * E.n_sl_reps);
+        TRY_ALLOC(E.d_sl_u, sizeof(double) * top);
+        TRY_ALLOC(E.d_sl_y, sizeof(double) * top);
+        TRY_ALLOC(E.d_sl_y2, sizeof(double) * top);
+    }
     E.n_ss_polish = ss_polish;
     // per-bead chain ids, colloid -> replica, bonds
     std::vector<double> chain(bead);
@@ -506,6 +523,20 @@ int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
     if (!ctx || !x) return PS_ERR_ARG;
     Engine &E = ctx->E;
     cudaStream_t st = S(stream);
+    // host inputs are scanned before anything is copied or launched: a non-finite
+    // coordinate would otherwise travel through the cell grid and every pair kernel
+    if (ps::is_host_ptr(x))
+        for (long i = 0; i < 3 * E.ntot; i++)
+            if (!std::isfinite(x[i])) {
+                ps::set_error("non-finite position at index " + std::to_string(i));
+                return PS_ERR_ARG;
+            }
+    if (q && ps::is_host_ptr(q))
+        for (long i = 0; i < 4 * E.ncoll; i++)
+            if (!std::isfinite(q[i])) {
+                ps::set_error("non-finite quaternion at index " + std::to_string(i));
+                return PS_ERR_ARG;
+            }
     PS_CK(cudaMemcpyAsync(E.d_x, x, sizeof(double) * 3 * E.ntot, cudaMemcpyDefault, st));
     if (q) PS_CK(cudaMemcpyAsync(E.d_q, q, sizeof(double) * 4 * E.ncoll, cudaMemcpyDefault, st));
     else if (E.ncoll) {

@@ -152,8 +152,9 @@ public:
     void set_warn_neg_eig(bool on) { warn_neg_eig_ = on; }
 
     void set_options(const std::string &precision, const std::string &solver, double rtol, const std::string &noise,
-                     int ab_mode, int aa_mode, int sqrt_kmax, double sqrt_tol)
+                     int ab_mode, int aa_mode, int sqrt_kmax, double sqrt_tol, int maxit, bool strict)
     {
+        if (maxit < 1) throw std::invalid_argument("maxit must be >= 1");
         if (precision != "fp64" && precision != "mixed") throw std::invalid_argument("precision: fp64 | mixed");
         if (solver != "minres" && solver != "structured") throw std::invalid_argument("solver: minres | structured");
         if (noise != "host" && noise != "device") throw std::invalid_argument("noise: host | device");
@@ -163,6 +164,7 @@ public:
         host_noise_ = noise == "host";
         d_.ab_mode = ab_mode; d_.aa_mode = aa_mode;
         sqrt_kmax_ = sqrt_kmax; sqrt_tol_ = sqrt_tol;
+        maxit_ = maxit; strict_ = strict;
     }
 
     void set_lubrication(py::array_t<double, py::array::c_style | py::array::forcecast> table, double gap, bool bonded)
@@ -209,7 +211,7 @@ public:
                 in.wrfd = W.data();
             }
             in.rtol = rtol_;
-            in.maxit = 10000;
+            in.maxit = maxit_;
             in.sqrt_kmax = sqrt_kmax_;
             in.sqrt_tol = sqrt_tol_;
             in.solver = solver_;
@@ -220,8 +222,16 @@ public:
                 rc = ps_step(ctx_, &in, &res, nullptr);
             }
             check(rc, "ps_step");
-            if (res.reason < 0)
+            if (res.reason < 0) {
+                // the reference only reports a failed KSPSolve and carries on (vel.cpp:45-51);
+                // with strict set the run stops with the solver's reason instead
                 std::cout << "Warning: saddle solve did not converge (reason " << res.reason << ") at t=" << t << std::endl;
+                if (strict_) {
+                    t_ = t;
+                    throw std::runtime_error("run: saddle solve did not converge (KSP reason " +
+                                             std::to_string(res.reason) + ") at step " + std::to_string(i + 1));
+                }
+            }
             if (res.lanczos_nneg > 0) {
                 neg_stages++;
                 neg_total += res.lanczos_nneg;
@@ -311,6 +321,8 @@ private:
     bool host_noise_ = true;
     int sqrt_kmax_ = 40;
     double sqrt_tol_ = 1e-6;
+    int maxit_ = 10000;
+    bool strict_ = false;
     std::vector<double> lub_;
     int lub_rows_ = 0, lub_cols_ = 0;
     ps_ctx *ctx_ = nullptr;
@@ -347,9 +359,12 @@ PYBIND11_MODULE(PolyStokes, m)
         // not in the reference
         .def("set_options", &PolyStokes::set_options, py::arg("precision") = "fp64", py::arg("solver") = "structured",
              py::arg("rtol") = 1e-6, py::arg("noise") = "host", py::arg("ab_mode") = 0, py::arg("aa_mode") = 0,
-             py::arg("sqrt_kmax") = 40, py::arg("sqrt_tol") = 1e-6,
+             py::arg("sqrt_kmax") = 40, py::arg("sqrt_tol") = 1e-6, py::arg("maxit") = 10000,
+             py::arg("strict") = false,
              "Engine options: precision fp64|mixed, solver structured|minres, rtol, noise host (the reference's "
-             "mt19937_64 stream) | device (Philox), pair scalars (0 reference, 1 RPY), Lanczos noise cap/tolerance")
+             "mt19937_64 stream) | device (Philox), pair scalars (0 reference, 1 RPY), Lanczos noise cap/tolerance, "
+             "solver iteration cap, strict (raise RuntimeError when a saddle solve does not converge; the "
+             "reference only prints)")
         .def("set_lubrication", &PolyStokes::set_lubrication, py::arg("table"), py::arg("gap") = 0.5,
              py::arg("bonded") = false, "Near-field lubrication from a lubdat/r2babc.dat table")
         .def("positions", &PolyStokes::positions)

@@ -633,4 +633,200 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     }
     return PS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Schur Lanczos noise of the shell (arrowhead) path above the dense Schur limit,
+// schur_sqrt_lanczos (slip_vel.cpp:351-477): sqrt(S) xi_c with
+// S q = Mcc q - beta Mcm (Mcm^T q) applied matrix-free through two mobility
+// applies per vector ([0; q] gives Mcm^T q in the monomer rows and Mcc q in the
+// colloid rows; [Mcm^T q; 0] gives Mcm Mcm^T q in the colloid rows), at most
+// min(40, nc11) vectors, two-pass reorthogonalisation against the whole basis,
+// stop on an invariant subspace (||w|| <= 1e-12 ||xi_c||) or the cap, then the
+// square root of the projected tridiagonal with negative eigenvalues floored at
+// 0.  One block per such replica for the short vectors (length nc11).
+struct SlScal {
+    double b0;
+    int m, done, nneg, pad;
+};
+constexpr int SL_THREADS = 256;
+
+// sum over the block in a fixed order (thread-strided partials, shuffle tree, warp order)
+__device__ double sl_block_sum(double v)
+{
+    __shared__ double ws[SL_THREADS / 32];
+    __shared__ double tot;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) ws[wid] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < SL_THREADS / 32; w++) t += ws[w];
+        tot = t;
+    }
+    __syncthreads();
+    double r = tot;
+    __syncthreads();
+    return r;
+}
+
+__device__ double sl_dot(const double *a, const double *b, int n)
+{
+    double acc = 0;
+    for (int i = threadIdx.x; i < n; i += SL_THREADS) acc += a[i] * b[i];
+    return sl_block_sum(acc);
+}
+
+// V_0 = xi_c / ||xi_c||
+__global__ void k_sl_init(const Seg *__restrict__ segs, const int *__restrict__ reps, const double *__restrict__ fb,
+                          double *__restrict__ V, SlScal *__restrict__ sc, int *__restrict__ skip)
+{
+    const int slot = blockIdx.x, r = reps[slot];
+    const Seg &s = segs[r];
+    const int n = s.nc11;
+    const double *b = fb + s.top_off + s.nm3;
+    const double b0 = sqrt(sl_dot(b, b, n));
+    double *V0 = V + s.sl_off;
+    const double inv = b0 > 0 ? 1.0 / b0 : 0.0;
+    for (int i = threadIdx.x; i < n; i += SL_THREADS) V0[i] = b[i] * inv;
+    if (threadIdx.x == 0) {
+        sc[slot].b0 = b0; sc[slot].m = 0; sc[slot].nneg = 0; sc[slot].done = (b0 == 0.0);
+        skip[r] = (b0 == 0.0);
+    }
+}
+
+// u = [0 ; V_j] (stage 0) or u = [y_m ; 0] (stage 1) on the Lanczos replicas, 0 elsewhere
+__global__ void k_sl_load(long ntop, const int *__restrict__ top_offs, int R, const Seg *__restrict__ segs,
+                          const double *__restrict__ V, const SlScal *__restrict__ sc, int j, int stage,
+                          const double *__restrict__ y, double *__restrict__ u)
+{
+    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ntop) return;
+    int lo = 0, hi = R;
+    while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (top_offs[mid] <= k) lo = mid; else hi = mid; }
+    const Seg &s = segs[lo];
+    const int i = (int)(k - s.top_off);
+    double v = 0.0;
+    if (s.sl_slot >= 0 && !sc[s.sl_slot].done) {
+        if (stage == 0) { if (i >= s.nm3) v = V[s.sl_off + (long)j * s.nc11 + (i - s.nm3)]; }
+        else if (i < s.nm3) v = y[k];
+    }
+    u[k] = v;
+}
+
+// one Lanczos vector: w = S V_j - beta_{j-1} V_{j-1}, alpha_j, two reorthogonalisation passes,
+// beta_j and V_{j+1} (row j+1 of the basis holds w while it is formed)
+__global__ void k_sl_iter(const Seg *__restrict__ segs, const int *__restrict__ reps, double *__restrict__ V,
+                          double *__restrict__ ab, SlScal *__restrict__ sc, int *__restrict__ skip,
+                          const double *__restrict__ y, const double *__restrict__ y2, int j)
+{
+    const int slot = blockIdx.x, r = reps[slot];
+    if (sc[slot].done) return;
+    const Seg &s = segs[r];
+    const int n = s.nc11;
+    double *Vb = V + s.sl_off;
+    double *w = Vb + (long)(j + 1) * n;
+    double *alpha = ab + (long)2 * SL_KMAX * slot, *betad = alpha + SL_KMAX;
+    const double *yc = y + s.top_off + s.nm3, *y2c = y2 + s.top_off + s.nm3;
+    for (int i = threadIdx.x; i < n; i += SL_THREADS) {
+        double v = yc[i] - s.beta * y2c[i];
+        if (j > 0) v -= betad[j - 1] * Vb[(long)(j - 1) * n + i];
+        w[i] = v;
+    }
+    __syncthreads();
+    const double *Vj = Vb + (long)j * n;
+    const double aj = sl_dot(Vj, w, n);
+    for (int i = threadIdx.x; i < n; i += SL_THREADS) w[i] -= aj * Vj[i];
+    __syncthreads();
+    for (int pass = 0; pass < 2; pass++)
+        for (int l = 0; l <= j; l++) {
+            const double *Vl = Vb + (long)l * n;
+            const double h = sl_dot(Vl, w, n);
+            for (int i = threadIdx.x; i < n; i += SL_THREADS) w[i] -= h * Vl[i];
+            __syncthreads();
+        }
+    const double bj = sqrt(sl_dot(w, w, n));
+    const int kmax = n < SL_KMAX ? n : SL_KMAX;
+    const bool stop = (bj <= 1e-12 * sc[slot].b0) || (j == kmax - 1);
+    if (!stop) {
+        const double inv = 1.0 / bj;
+        for (int i = threadIdx.x; i < n; i += SL_THREADS) w[i] *= inv;
+    }
+    if (threadIdx.x == 0) {
+        alpha[j] = aj;
+        sc[slot].m = j + 1;
+        if (stop) { sc[slot].done = 1; skip[r] = 1; }
+        else betad[j] = bj;
+    }
+}
+
+// W_m = sqrt(beta_inv) xi_m; W_c = sqrt(beta) (Mcm xi_m) + b0 V U sqrt(max(theta, 0)) U^T e1
+__global__ void k_sl_finish(const Seg *__restrict__ segs, const int *__restrict__ reps, const double *__restrict__ V,
+                            const double *__restrict__ ab, SlScal *__restrict__ sc, const double *__restrict__ fb,
+                            const double *__restrict__ ymcm, double *__restrict__ W)
+{
+    __shared__ double d[SL_KMAX], e[SL_KMAX], Z[SL_KMAX * SL_KMAX], g[SL_KMAX];
+    const int slot = blockIdx.x, r = reps[slot];
+    const Seg &s = segs[r];
+    const int n = s.nc11, m = sc[slot].m;
+    const double b0 = sc[slot].b0;
+    for (int i = threadIdx.x; i < s.nm3; i += blockDim.x) W[s.top_off + i] = sqrt(s.beta_inv) * fb[s.top_off + i];
+    const double *alpha = ab + (long)2 * SL_KMAX * slot, *betad = alpha + SL_KMAX;
+    if (m > 0 && threadIdx.x < 32) {
+        for (int i = threadIdx.x; i < m; i += 32) { d[i] = alpha[i]; e[i] = (i < m - 1) ? betad[i] : 0.0; }
+        __syncwarp();
+        warp_tql(d, e, Z, m);
+        __syncwarp();
+        int nneg = 0;
+        for (int i = threadIdx.x; i < m; i += 32) {
+            double gi = 0;
+            for (int c = 0; c < m; c++) gi += Z[i * m + c] * (d[c] > 0 ? sqrt(d[c]) : 0.0) * Z[c];
+            g[i] = b0 * gi;
+            nneg += d[i] < 0.0;
+        }
+        for (int o = 16; o > 0; o >>= 1) nneg += __shfl_down_sync(0xffffffffu, nneg, o);
+        if (threadIdx.x == 0) sc[slot].nneg = nneg;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double acc = sqrt(s.beta) * ymcm[s.top_off + s.nm3 + i];
+        for (int c = 0; c < m; c++) acc += g[c] * V[s.sl_off + (long)c * n + i];
+        W[s.top_off + s.nm3 + i] = acc;
+    }
+}
+
+int schur_lanczos_noise(Engine &E, const double *fb, const double *ymcm, double *W, int *nneg, cudaStream_t st)
+{
+    if (!E.n_sl_reps) return PS_OK;
+    SlScal *sc = (SlScal *)E.d_sl_sc;
+    const int ns = E.n_sl_reps;
+    int kmax = 0;
+    for (auto &s : E.segs)
+        if (s.sl_slot >= 0) kmax = std::max(kmax, std::min(s.nc11, SL_KMAX));
+    ::ps_launch_count++, k_sl_init<<<ns, SL_THREADS, 0, st>>>(E.d_segs, E.d_sl_reps, fb, E.d_slV, sc, E.d_sl_skip);
+    const int thr = 256;
+    const unsigned gb = (unsigned)((E.ntop + thr - 1) / thr);
+    for (int j = 0; j < kmax; j++) {
+        ::ps_launch_count++, k_sl_load<<<gb, thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 0,
+                                                           nullptr, E.d_sl_u);
+        apply_operator(E, 1, E.d_sl_u, E.d_sl_y, nullptr, false, st, E.d_sl_skip, (int)sizeof(int));
+        ::ps_launch_count++, k_sl_load<<<gb, thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 1,
+                                                           E.d_sl_y, E.d_sl_u);
+        apply_operator(E, 1, E.d_sl_u, E.d_sl_y2, nullptr, false, st, E.d_sl_skip, (int)sizeof(int));
+        ::ps_launch_count++, k_sl_iter<<<ns, SL_THREADS, 0, st>>>(E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc,
+                                                                  E.d_sl_skip, E.d_sl_y, E.d_sl_y2, j);
+    }
+    ::ps_launch_count++, k_sl_finish<<<ns, SL_THREADS, 0, st>>>(E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc, fb, ymcm, W);
+    // the operator applies of the next noise draw start from the Lanczos set again
+    std::vector<int> skip(E.R, 1);
+    for (auto &s : E.segs)
+        if (s.sl_slot >= 0) skip[&s - &E.segs[0]] = 0;
+    PS_CK(cudaMemcpyAsync(E.d_sl_skip, skip.data(), sizeof(int) * E.R, cudaMemcpyHostToDevice, st));
+    std::vector<SlScal> hs(ns);
+    PS_CK(cudaMemcpyAsync(hs.data(), sc, sizeof(SlScal) * ns, cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaStreamSynchronize(st));
+    PS_CK(cudaGetLastError());
+    if (nneg) { *nneg = 0; for (auto &h : hs) *nneg += h.nneg; }
+    return PS_OK;
+}
 }  // namespace ps

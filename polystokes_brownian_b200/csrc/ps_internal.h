@@ -13,6 +13,7 @@
 #include "../../include/polystokes_b200.h"
 
 #define PS_MAX_NC11_SCHUR 64   // dense Schur path limit (slip_vel.cpp:97)
+#define SL_KMAX 40             // Schur Lanczos noise: basis cap (slip_vel.cpp:300, kmax = 40)
 
 // number of kernels this library has launched (host-side counter)
 extern unsigned long long ps_launch_count;
@@ -29,6 +30,8 @@ struct Seg {
     int mm_HI, chain_HI, ab_mode, box_on, fene, mono_ev, lub_on, tether, aa_mode;
     int shell_schur;   // shell path with the dense Schur floor (nc11 <= lanczos_nc)
     int schur_off;     // offset into the per-replica nc11^2 buffers
+    int sl_slot;       // shell path above the Schur limit: slot of its Schur Lanczos noise state, else -1
+    int sl_off;        // offset of its Lanczos basis ((SL_KMAX + 1) nc11 doubles)
     int ba_off;        // offset (in 11-vectors) of this replica's BA partials
     int n_mtiles;      // monomer row tiles of this replica
     int bond_off, nbonds;

@@ -75,6 +75,14 @@ struct Engine {
     double *d_delta = nullptr, *d_schurQ = nullptr, *d_schurL = nullptr;
     int *d_schur_reps = nullptr; int n_schur_reps = 0;
     int *d_ss_reps = nullptr; int n_ss_reps = 0;   // replicas whose stresslet block is solved densely
+    // Schur Lanczos noise of shell replicas above the dense Schur limit (slip_vel.cpp:283-288, 351-477)
+    int n_sl_reps = 0;
+    int *d_sl_reps = nullptr;        // slot -> replica
+    int *d_sl_skip = nullptr;        // per replica: 1 = skip in the operator applies of the Lanczos loop
+    double *d_slV = nullptr;         // per slot: basis, (SL_KMAX + 1) x nc11 (the last row is the residual)
+    double *d_slT = nullptr;         // per slot: alpha[SL_KMAX], beta[SL_KMAX]
+    void *d_sl_sc = nullptr;         // per slot: scalars (b0, m, done, nneg)
+    double *d_sl_u = nullptr, *d_sl_y = nullptr, *d_sl_y2 = nullptr;   // mobility-layout work vectors
     int n_ss_polish = 0;                           // replicas with colloids beyond the dense limit
 
     // bonds (per-bead CSR: partner, sign)
@@ -204,6 +212,7 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
 // solve.cu
 int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps_ksp_result *res,
                      cudaStream_t st);
+int schur_lanczos_noise(Engine &E, const double *fb, const double *ymcm, double *W, int *nneg, cudaStream_t st);
 int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st);
 int build_red_table(Engine &E, RedTable &T, int layout);   // 0 saddle, 1 top, 2 velocity, 3 beads
 void free_red_table(RedTable &T);

@@ -391,18 +391,40 @@ __global__ void k_forces(long ntot, const int *__restrict__ bead_offs, int R, co
     };
     if (mono) {
         if (s.mm_HI && s.mono_ev) {
-            // AA Verlet partners via the cell list, gathered then applied in ascending order
-            int cnt = 0;
-            int nb[64];
-            for_cell_neighbours(s, r, b, x, geo, cell_off, cstart, csorted, [&](int j) {
+            // AA Verlet partners via the cell list, applied in ascending order.  Up to 64 are
+            // gathered and sorted in registers; a bead with more (overlapping, diverging
+            // configurations) takes them by repeated ascending selection over its cells, so no
+            // partner is ever dropped and the order stays the reference's.
+            const double rv = (double)s.rverl[0];
+            auto is_partner = [&](int j) {
                 double dx = x[3 * b] - x[3 * (long)j], dy = x[3 * b + 1] - x[3 * (long)j + 1], dz = x[3 * b + 2] - x[3 * (long)j + 2];
                 min_image(s, dx, dy, dz);
                 double d2 = dx * dx + dy * dy + dz * dz;
-                double rv = (double)s.rverl[0];
-                if (d2 < rv * rv * 1.0000001 && cnt < 64) nb[cnt++] = j;
+                return d2 < rv * rv * 1.0000001;
+            };
+            int cnt = 0, tot = 0;
+            int nb[64];
+            for_cell_neighbours(s, r, b, x, geo, cell_off, cstart, csorted, [&](int j) {
+                if (!is_partner(j)) return;
+                if (cnt < 64) nb[cnt++] = j;
+                tot++;
             });
-            for (int a = 1; a < cnt; a++) { int v = nb[a], c = a - 1; while (c >= 0 && nb[c] > v) { nb[c + 1] = nb[c]; c--; } nb[c + 1] = v; }
-            for (int a = 0; a < cnt; a++) hs_pair(nb[a], 0);
+            if (tot <= 64) {
+                for (int a = 1; a < cnt; a++) { int v = nb[a], c = a - 1; while (c >= 0 && nb[c] > v) { nb[c + 1] = nb[c]; c--; } nb[c + 1] = v; }
+                for (int a = 0; a < cnt; a++) hs_pair(nb[a], 0);
+            } else {
+                // each pass applies the smallest partner above the last one: tot passes at most
+                int last = -1;
+                for (int pass = 0; pass < tot; pass++) {
+                    int best = 0x7fffffff;
+                    for_cell_neighbours(s, r, b, x, geo, cell_off, cstart, csorted, [&](int j) {
+                        if (j > last && j < best && is_partner(j)) best = j;
+                    });
+                    if (best == 0x7fffffff) break;
+                    hs_pair(best, 0);
+                    last = best;
+                }
+            }
         }
         for (int c = 0; c < s.Nc; c++) hs_pair((long)s.bead_off + s.Nm + c, 1);
         if (!s.mm_HI && s.mono_ev) {

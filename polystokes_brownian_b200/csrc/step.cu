@@ -67,13 +67,21 @@ int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps
         int rc = lanczos_sqrt(E, fb, W, o, &r0, st);
         if (rc) return rc;
     }
-    if (E.n_schur_reps) {
+    if (E.n_schur_reps || E.n_sl_reps) {
         int thr = 256;
         ::ps_launch_count++, k_zero_colloid_dofs<<<(unsigned)((E.ntop + thr - 1) / thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs,
                                                                                   fb, E.d_tmp_top);
         apply_operator(E, 1, E.d_tmp_top, E.d_tmp_top2, nullptr, false, st);
-        ::ps_launch_count++, k_shell_noise<<<E.n_schur_reps, 128, 0, st>>>(E.d_segs, E.d_schur_reps, fb, E.d_tmp_top2, E.d_schurQ,
-                                                       E.d_schurL, W);
+        if (E.n_schur_reps)
+            ::ps_launch_count++, k_shell_noise<<<E.n_schur_reps, 128, 0, st>>>(E.d_segs, E.d_schur_reps, fb, E.d_tmp_top2,
+                                                                               E.d_schurQ, E.d_schurL, W);
+        if (E.n_sl_reps) {
+            // above the dense Schur limit: Lanczos on the colloid Schur complement
+            int nneg = 0;
+            int rc = schur_lanczos_noise(E, fb, E.d_tmp_top2, W, &nneg, st);
+            if (rc) return rc;
+            r0.nneg += nneg;
+        }
     }
     PS_CK(cudaGetLastError());
     if (res) *res = r0;

@@ -6,7 +6,11 @@ Heun step per launch sequence (one engine context over the active set).  New
 arrivals are admitted, and finished trajectories retired, between steps:
 
   * admission is first-come-first-served against an HBM budget (the engine's
-    per-replica footprint, ``footprint_bytes``) and a slot limit;
+    per-replica footprint, ``footprint_bytes``) and a slot limit; a request whose
+    footprint alone exceeds the budget is refused with an error result;
+  * thermal (kT > 0) and athermal (kT = 0) trajectories advance in separate
+    contexts (an engine context takes one kind: the step either draws noise and
+    runs the RFD probes for every replica or for none), stepped back to back;
   * when the active set changes the context is rebuilt over the new set and the
     continuing trajectories carry their state across: positions, quaternions,
     time, trap constant and centres, and their own noise stream (seed and step
@@ -55,6 +59,7 @@ class Result:
     arrival: float
     admitted: float
     finished: float
+    error: str | None = None      # set when the request was refused (no trajectory)
 
 
 @dataclasses.dataclass
@@ -129,7 +134,16 @@ class Server:
         xpos0 = x[3 * Nm:].copy()          # fresh start: trap centres at the colloids
         return _Slot(req, x, q, float(p.get("t0", 0.0)), float(p.get("ktrap", 0.0)), xpos0, admitted=now)
 
-    def _build(self, slots: list[_Slot]) -> Batch:
+    def _build(self, slots: list[_Slot]) -> list[tuple[list[_Slot], Batch]]:
+        """One context per kT class present in the active set, in (thermal, athermal) order."""
+        groups = []
+        for thermal in (True, False):
+            grp = [s for s in slots if (s.req.system.params["kT"] > 0) == thermal]
+            if grp:
+                groups.append((grp, self._build_one(grp)))
+        return groups
+
+    def _build_one(self, slots: list[_Slot]) -> Batch:
         systems = [s.req.system for s in slots]
         b = Batch(systems, precision=self.precision, device=self.device, lub_table=self.lub_table)
         dev = b.device
@@ -171,7 +185,7 @@ class Server:
         active: list[_Slot] = []
         results: list[Result] = []
         used = 0.0
-        batch: Batch | None = None
+        groups: list[tuple[list[_Slot], Batch]] = []
         since_rebuild = 0
         t0 = time.perf_counter()
         vnow = 0.0
@@ -183,18 +197,23 @@ class Server:
             live = [s for s in active if s.result is None]
             finished = [s for s in active if s.result is not None]
             arrivals = bool(pending) and pending[0].arrival <= now()
-            must = batch is None or not live
+            must = not groups or not live
             if must or (since_rebuild >= self.rebuild_every and (finished or arrivals)):
-                if batch is not None:
-                    self._export(batch, active)
-                    batch.close()
-                    batch = None
+                for grp, b in groups:
+                    self._export(b, grp)
+                    b.close()
+                groups = []
                 for s in finished:
                     used -= footprint_bytes(s.req.system, self.precision)
                 active = live
                 while pending and pending[0].arrival <= now() and len(active) < self.max_slots:
                     fb = footprint_bytes(pending[0].system, self.precision)
-                    if used + fb > self.budget and active:
+                    if fb > self.budget:
+                        req = pending.popleft()
+                        results.append(Result(req.rid, np.zeros(0), np.zeros(0), 0, req.arrival, now(), now(),
+                                              error=f"footprint {fb:.3e} B exceeds the HBM budget {self.budget:.3e} B"))
+                        continue
+                    if used + fb > self.budget:
                         break
                     req = pending.popleft()
                     used += fb
@@ -207,13 +226,14 @@ class Server:
                         else:
                             vnow = pending[0].arrival
                     continue
-                batch = self._build(active)
+                groups = self._build(active)
                 since_rebuild = 0
-            # one step of the whole active set
+            # one step of the whole active set (one context per kT class, back to back)
             st = torch.cuda.current_stream()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
-            batch.step(rtol=self.rtol, solver=self.solver)
+            for _, b in groups:
+                b.step(rtol=self.rtol, solver=self.solver)
             e1.record(st)
             e1.synchronize()
             ms = e0.elapsed_time(e1)
@@ -221,31 +241,33 @@ class Server:
             self.batch_sizes.append(len(active))
             vnow += ms * 1e-3
             since_rebuild += 1
-            done_now = []
-            for s in active:
-                if s.result is None:
-                    s.done_steps += 1
-                    self.bead_steps += s.req.system.Np
-                    if s.done_steps == s.req.steps:
-                        done_now.append(s)
-            if done_now:
-                x, q = batch.state()
+            for grp, b in groups:
+                done_now = []
+                for s in grp:
+                    if s.result is None:
+                        s.done_steps += 1
+                        self.bead_steps += s.req.system.Np
+                        if s.done_steps == s.req.steps:
+                            done_now.append(s)
+                if not done_now:
+                    continue
+                x, q = b.state()
                 x, q = x.cpu(), q.cpu()
                 for s in done_now:
-                    r = active.index(s)
+                    r = grp.index(s)
                     Nc = s.req.system.params["Nc"]
-                    co = batch.off[r]["coll"]
-                    s.result = Result(s.req.rid, batch.seg(x, r, "bead").numpy().copy(),
+                    co = b.off[r]["coll"]
+                    s.result = Result(s.req.rid, b.seg(x, r, "bead").numpy().copy(),
                                       q[4 * co:4 * co + 4 * Nc].numpy().copy(), s.done_steps, s.req.arrival,
                                       s.admitted, now())
                     results.append(s.result)
-        if batch is not None:
-            batch.close()
+        for _, b in groups:
+            b.close()
         return sorted(results, key=lambda r: r.rid)
 
     def stats(self, results: list[Result], wall_s: float) -> dict:
         lat = sorted(self.step_ms)
-        req = sorted(r.finished - r.arrival for r in results)
+        req = sorted(r.finished - r.arrival for r in results if r.error is None)
 
         def pct(v, p):
             return v[min(len(v) - 1, int(p * len(v)))] if v else None
@@ -254,7 +276,7 @@ class Server:
                 "step_ms": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99), "n": len(lat)},
                 "request_s": {"p50": pct(req, 0.5), "p99": pct(req, 0.99), "n": len(req)},
                 "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
-                "rebuilds": self.rebuilds}
+                "rebuilds": self.rebuilds, "refused": sum(r.error is not None for r in results)}
 
 
 def main():

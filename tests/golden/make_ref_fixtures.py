@@ -72,6 +72,13 @@ def cases():
         s = cf.small_mixed(seed=2, Nm_chain=(4, 10), Nc=1, mm_HI=0, beta=1.0 / 3.0, spread=8.0)
         return s, dict(steps=3, kT=1.0, seed=3, dump_mat=False)
 
+    def shell_lanczos():
+        # the same path with the crossover at 0 (POLYSTOKES_LANCZOS_NC=0, slip_vel.cpp:283-288):
+        # the colloid noise comes from schur_sqrt_lanczos (slip_vel.cpp:351-477) and Mcc carries
+        # no eigenvalue-floor correction (sync_mcc_schur_correction returns early)
+        s = cf.small_mixed(seed=2, Nm_chain=(4, 10), Nc=1, mm_HI=0, beta=1.0 / 3.0, spread=8.0, lanczos_nc=0)
+        return s, dict(steps=3, kT=1.0, seed=4, dump_mat=False, env={"POLYSTOKES_LANCZOS_NC": "0"})
+
     def probe_c1():
         # the polymer-plus-probe workload (11 chains x 20 beads, a_c = 3) with one probe: the
         # reference's shell path cannot take two (its colloid-colloid blocks are written into
@@ -88,7 +95,8 @@ def cases():
         return s, dict(steps=1, kT=1.0, seed=2, dump_mat=False)
 
     return {"dense_spd": dense_spd, "dense_spd_nc2": dense_spd_nc2, "dense_kt0": dense_kt0,
-            "shell_probe": shell_probe, "probe_c1": probe_c1, "replica1000": replica1000}
+            "shell_probe": shell_probe, "shell_lanczos": shell_lanczos, "probe_c1": probe_c1,
+            "replica1000": replica1000}
 
 
 def run_case(name: str, out: str) -> None:
@@ -169,7 +177,7 @@ def make(name: str) -> str:
         out = os.path.join(td, "out")
         os.makedirs(out)
         dump = os.path.join(td, "dump.bin")
-        env = dict(os.environ, ORACLE_KSP_RTOL="1e-13", ORACLE_REF_DUMP=dump)
+        env = dict(os.environ, ORACLE_KSP_RTOL="1e-13", ORACLE_REF_DUMP=dump, **o.get("env", {}))
         if o["dump_mat"]:
             env["ORACLE_REF_DUMP_MAT"] = "1"
         log = subprocess.run([sys.executable, os.path.abspath(__file__), "--run-case", name, out], env=env,

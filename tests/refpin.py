@@ -11,7 +11,7 @@ import numpy as np
 from polystokes_brownian_b200 import configs
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-SMALL = ["dense_spd", "dense_spd_nc2", "dense_kt0", "shell_probe", "probe_c1"]
+SMALL = ["dense_spd", "dense_spd_nc2", "dense_kt0", "shell_probe", "shell_lanczos", "probe_c1"]
 ALL = SMALL + ["replica1000"]
 
 

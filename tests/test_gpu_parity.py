@@ -146,6 +146,8 @@ STEP_CASES = {
     # dense path, deterministic (kT = 0), FENE chains around a colloid
     "brush_kT0": lambda: configs.System("brush", dict(configs.brush(nchain=8, nper=8, seed=0).params, kT=0.0),
                                         configs.brush(nchain=8, nper=8, seed=0).x),
+    # shell path above the dense Schur limit: 8 colloids (nc11 = 88 > 64), Schur Lanczos noise
+    "shell_lanczos8": lambda: configs.small_mixed(seed=6, Nm_chain=(4, 6), Nc=8, mm_HI=0, spread=12.0),
 }
 
 
@@ -175,6 +177,22 @@ def test_step_parity(case, solver):
     b.close()
 
 
+@pytest.mark.parametrize("lnc", [64, 0])
+def test_schur_lanczos_noise(lnc):
+    """Shell-path slip noise through the Schur Lanczos branch (slip_vel.cpp:351-477): 8
+    colloids (nc11 = 88 above the crossover of 64), or the crossover set to 0, which sends
+    every shell replica there (the reference's POLYSTOKES_LANCZOS_NC=0)."""
+    sysm = configs.small_mixed(seed=6, Nm_chain=(4, 6), Nc=8 if lnc else 2, mm_HI=0, spread=12.0, lanczos_nc=lnc)
+    o = oracle_for(sysm)
+    o.stage()
+    z = np.random.default_rng(8).normal(size=o.nm3nc11)
+    b = Batch([sysm])
+    b.stage()
+    w, r = b.sqrtm(torch.from_numpy(z).cuda())
+    assert rel(w.cpu().numpy(), o.slip_noise(z)) < 1e-10
+    b.close()
+
+
 def test_batch_matches_single():
     systems = [CASES["mmhi_mixed"](), CASES["colloids"](), CASES["shell_C1"]()]
     xs = [np.random.default_rng(i).normal(size=6 * s.params["Nm"] + 17 * s.params["Nc"]) for i, s in enumerate(systems)]
@@ -188,4 +206,24 @@ def test_batch_matches_single():
         o = b.off[i]["vec"]
         assert rel(yb[o:o + len(xs[i])], y1) < 1e-13
         one.close()
+    b.close()
+
+
+def test_hs_partner_overflow():
+    """Monomers piled inside one Verlet radius (about 99 hard-sphere partners each, beyond
+    the 64 gathered in registers): the forces still take every partner, in ascending order,
+    as the oracle's Verlet sweep does."""
+    rng = np.random.default_rng(5)
+    Nm = 100
+    x = rng.uniform(-0.15, 0.15, size=(Nm, 3))
+    p = configs.make_params(Nm=Nm, Nc=0, Npoly=20, Nmono_per_chain=5, beta=0.3, kT=0.0, kbond=10.0, r0=0.1,
+                            Lmax=1.0, mm_HI=1, mono_ev=1)
+    sysm = configs.System("pile", p, x)
+    o = oracle_for(sysm)
+    rhs_o = o.stage()
+    pi, pj = o.verlet_pairs()
+    assert np.bincount(np.concatenate([pi, pj]), minlength=Nm).min() > 64
+    b = Batch([sysm])
+    rhs_g = b.stage().cpu().numpy()
+    assert rel(rhs_g, rhs_o) < 1e-13
     b.close()

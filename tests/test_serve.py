@@ -60,3 +60,31 @@ def test_admission_respects_budget():
     res = srv.run(trace, clock="virtual")
     assert len(res) == len(trace)
     assert max(srv.batch_sizes) <= 2
+
+
+def test_oversize_request_refused():
+    """A request whose footprint alone is beyond the HBM budget gets an error result; the
+    loop never builds a context for it (host only, runs without a GPU)."""
+    trace = small_trace(5)[:1]
+    fp = serve.footprint_bytes(trace[0].system)
+    srv = serve.Server(budget_bytes=0.5 * fp)
+    res = srv.run(trace, clock="virtual")
+    assert len(res) == 1 and res[0].error is not None and "budget" in res[0].error
+    assert res[0].x.size == 0 and srv.rebuilds == 0
+
+
+@pytest.mark.gpu
+def test_mixed_kT_trace():
+    """kT = 0 and kT > 0 requests in one trace run in two contexts side by side; each
+    trajectory equals its run alone."""
+    from polystokes_brownian_b200 import configs
+    trace = small_trace(6)
+    r1 = trace[1]
+    cold = configs.System(r1.system.name, dict(r1.system.params, kT=0.0), r1.system.x)
+    trace[1] = serve.Request(r1.rid, cold, r1.steps, r1.seed, r1.arrival)
+    mixed = serve.Server(precision=_capi.PS_PREC_FP64, rebuild_every=1).run(trace, clock="virtual")
+    assert [r.rid for r in mixed] == [r.rid for r in trace] and all(r.error is None for r in mixed)
+    for req in (trace[0], trace[1]):
+        alone = serve.Server(precision=_capi.PS_PREC_FP64).run(
+            [serve.Request(req.rid, req.system, req.steps, req.seed, 0.0)], clock="virtual")[0]
+        assert np.array_equal(alone.x, mixed[req.rid].x)
