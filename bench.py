@@ -17,9 +17,10 @@ and the mixed form's velocity error against FP64.
 
 For N > 1 it is launched under torchrun; every rank advances its own seeded
 ensemble (weak scaling, no collective in the step) and rank 0 prints the line.
-The reference arm (--impl reference) times the CPU restatement of the
-reference (oracle/, the reference itself needs PETSc/SLEPc and cannot be built
-here) on a bounded, stratified sample of the same workload.
+The reference arm (--impl reference) times the reference's own code
+(oracle/_ref: its sources built against the PETSc/SLEPc stand-in; the CPU
+restatement in oracle/ where that build is absent) on all host cores, on a
+bounded, stratified sample of the same workload's replicas.
 """
 from __future__ import annotations
 
@@ -65,6 +66,7 @@ def parse():
                     help="replicas timed one by one in the plain FP64 drop-in form (0: skip)")
     ap.add_argument("--err-sample", type=int, default=16, help="replicas of the mixed-vs-FP64 error check (0: skip)")
     ap.add_argument("--no-fp64-batched", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the bounded runs of the other configurations")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="N > 1: weak = one seeded ensemble per rank; strong = one ensemble split across ranks (LPT)")
@@ -252,6 +254,96 @@ def _oracle_step_seconds(s, rtol):
     return s.Np, time.perf_counter() - t0
 
 
+def _ref_step_seconds(params, x, rtol):
+    """One step of the reference's own module on one system (fresh worker process)."""
+    from oracle import refrun
+    return refrun.step_seconds(params, np.ascontiguousarray(x, dtype=np.float64).ravel(), rtol)
+
+
+def ref_pool(cores):
+    """Fresh spawned process per task (the reference keeps global state); a worker that dies
+    raises BrokenProcessPool instead of stalling the arm."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    return cf.ProcessPoolExecutor(cores, mp_context=mp.get_context("spawn"), max_tasks_per_child=1)
+
+
+def power_fit(n, t):
+    """t = a N^p by least squares in log-log; returns (a, p, relative rms residual)."""
+    n, t = np.asarray(n, float), np.asarray(t, float)
+    p, la = np.polyfit(np.log(n), np.log(t), 1)
+    pred = np.exp(la) * n ** p
+    return float(np.exp(la)), float(p), float(np.sqrt(np.mean(((pred - t) / t) ** 2)))
+
+
+def ref_sample(systems, nmax, k, offset=0):
+    """k replicas of the workload with N <= nmax and at least one colloid, spread evenly over
+    that range (rotated by offset).  The reference cannot run a system without a colloid
+    (initial_configuration reads the trap centre of colloid 0)."""
+    Ns = np.array([s.Np for s in systems])
+    small = [systems[int(i)] for i in np.argsort(Ns) if systems[int(i)].Np <= nmax and systems[int(i)].params["Nc"] > 0]
+    if not small:
+        small = [systems[int(np.argmin(Ns))]]
+    m = len(small)
+    return [small[(int(round(i * (m - 1) / max(1, k - 1))) + offset) % m] for i in range(k)]
+
+
+def reference_cpu(systems, rtol, cores, steps, nmax=300, pool=None):
+    """The reference's own code (oracle/_ref) stepping replicas of the workload on `cores`
+    host cores: per bench step, `cores` replicas (N <= nmax, rotated through the range)
+    run one reference step each, concurrently in fresh processes, so every time carries a
+    loaded host's contention.  The per-replica step time is fitted as a N^p over all
+    samples and the whole batch is scheduled longest-first on the cores.  The reference
+    runs its own model on the same positions: its own pair scalars, no lubrication (it
+    has none), MINRES + Jacobi at the workload's rtol."""
+    own = pool is None
+    if own:
+        pool = ref_pool(cores)
+    n, t = [], []
+    try:
+        for k in range(steps):
+            pick = ref_sample(systems, nmax, cores, offset=k)
+            res = list(pool.map(_ref_step_seconds, [s.params for s in pick], [s.x for s in pick],
+                                [rtol] * len(pick)))
+            n += [r[0] for r in res]
+            t += [r[1] for r in res]
+    finally:
+        if own:
+            pool.shutdown()
+    a, pw, resid = power_fit(n, t)
+    Ns = np.array([s.Np for s in systems])
+    makespan = lpt_makespan([a * N ** pw for N in Ns], cores)
+    desc = (f"the reference's own code (sources built against the PETSc/SLEPc stand-in) on {cores} cores: "
+            f"{len(n)} one-step runs of workload replicas with N in [{min(n)},{max(n)}], {cores} at a time; "
+            f"step time fitted as a*N^p (p = {pw:.2f}, rms residual {resid:.2f}), the batch scheduled "
+            f"longest-first on the {cores} cores; its own model (reference pair scalars, no lubrication)")
+    return {"value": float(Ns.sum()) / makespan, "unit": METRIC, "cores": cores, "kind": "reference",
+            "sample": desc, "sample_seconds": float(sum(t)), "fit": {"a_s": a, "p": pw, "rms_rel_residual": resid,
+                                                                      "N": n, "s": t}}
+
+
+def cpu_baseline_ref(systems, rtol, k=6, nmax=250):
+    """The reference's own code (oracle/_ref) on one core: one step each of k workload
+    replicas with N <= nmax, one after another; step time fitted as a N^p and summed over
+    the workload."""
+    pool = ref_pool(1)
+    try:
+        pick = ref_sample(systems, nmax, k)
+        res = list(pool.map(_ref_step_seconds, [s.params for s in pick], [s.x for s in pick], [rtol] * len(pick)))
+    finally:
+        pool.shutdown()
+    n, t = [r[0] for r in res], [r[1] for r in res]
+    a, pw, resid = power_fit(n, t)
+    Ns = np.array([s.Np for s in systems])
+    total = float(sum(a * N ** pw for N in Ns))
+    desc = (f"the reference's own code (sources built against the PETSc/SLEPc stand-in), 1 core, one step each "
+            f"of {len(n)} workload replicas with N in [{min(n)},{max(n)}]; step time fitted as a*N^p "
+            f"(p = {pw:.2f}, rms residual {resid:.2f}) and summed over the workload; its own model (reference "
+            f"pair scalars, no lubrication)")
+    return {"value": float(Ns.sum()) / total, "unit": METRIC, "cores": 1, "kind": "reference", "sample": desc,
+            "sample_seconds": float(sum(t)), "fit": {"a_s": a, "p": pw, "rms_rel_residual": resid, "N": n, "s": t}}
+
+
 def lpt_makespan(times, cores):
     """Longest-processing-time-first schedule of independent jobs on `cores` workers."""
     loads = [0.0] * max(1, cores)
@@ -293,45 +385,77 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import refrun
     systems, name = workload(args, 0)
     vals = []
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     single = len(systems) == 1
+    use_ref = refrun.available() and not single
     pool = None
-    if not single:
+    if use_ref:
+        pool = ref_pool(cores)
+    elif not single:
         import multiprocessing as mp
         pool = mp.get_context("spawn").Pool(cores)     # spawned once; no GPU in this arm
     try:
-        for k in range(args.warmup + args.steps):
-            if single:
-                # one system: the port has no parallelism inside a system
-                ss, sd = scaled_instances(args) if systems[0].Np > 700 else (None, None)
-                cb = cpu_baseline(systems, steps_budget_s=6.0, rtol=args.rtol, sample_systems=ss, sample_desc=sd)
-            else:
-                cb = cpu_baseline_parallel(systems, args.rtol, cores, pool)
-            if k >= args.warmup:
-                vals.append(cb["value"])
+        if use_ref:
+            # the fit uses every timed sample; the warm-up steps prime the page cache and processes
+            reference_cpu(systems, args.rtol, cores, args.warmup, pool=pool)
+            cb = reference_cpu(systems, args.rtol, cores, args.steps, pool=pool)
+            vals = [cb["value"]]
+        else:
+            for k in range(args.warmup + args.steps):
+                if single:
+                    # one system: the port has no parallelism inside a system
+                    ss, sd = scaled_instances(args) if systems[0].Np > 700 else (None, None)
+                    cb = cpu_baseline(systems, steps_budget_s=6.0, rtol=args.rtol, sample_systems=ss, sample_desc=sd)
+                else:
+                    cb = cpu_baseline_parallel(systems, args.rtol, cores, pool)
+                if k >= args.warmup:
+                    vals.append(cb["value"])
     finally:
-        if pool is not None:
+        if use_ref:
+            pool.shutdown()
+        elif pool is not None:
             pool.close()
             pool.join()
     v = float(np.median(vals))
     out = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": name, "replicas": len(systems), "beads": int(sum(s.Np for s in systems)),
-                      "rtol": args.rtol},
-           "cpu_baseline": {"value": v, "unit": METRIC, "cores": cb["cores"], "kind": "port", "sample": cb["sample"]},
+           "config": {"workload": name, "replicas_per_rank": len(systems),
+                      "beads_job": int(sum(s.Np for s in systems)), "rtol": args.rtol},
+           "cpu_baseline": {"value": v, "unit": METRIC, "cores": cb["cores"], "kind": cb["kind"],
+                            "sample": cb["sample"]},
            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if "fit" in cb:
+        out["cpu_baseline"]["fit"] = cb["fit"]
     print(json.dumps(out), flush=True)
 
 
-def plain_fp64(systems, args, budget_s=60.0):
+def _fit_project(n, ms, Ns):
+    """Per-replica step time fitted as a + b N + c N^2 over a sample, summed over Ns;
+    returns (total ms, rms relative residual of the fit)."""
+    n = np.asarray(n, float)
+    ms = np.asarray(ms, float)
+    A = np.stack([np.ones_like(n), n, n * n], 1)
+    coef, *_ = np.linalg.lstsq(A, ms, rcond=None)
+    if len(n) < 3 or np.any(A @ coef <= 0):
+        coef = np.array([0.0, 0.0, float(np.sum(ms) / np.sum(n * n))])
+    pred = A @ coef
+    resid = float(np.sqrt(np.mean(((pred - ms) / ms) ** 2)))
+    return float(sum(max(coef[0] + coef[1] * N + coef[2] * N * N, 1e-3) for N in Ns)), resid
+
+
+def plain_fp64(systems, args, budget_s=90.0):
     """The plain FP64 GPU drop-in: each replica in its own context, one at a time,
     FP64 operator and Jacobi-preconditioned MINRES -- the reference's MatShell +
-    KSPSolve path moved to the GPU.  A stratified sample of replicas is stepped
-    (1 warm-up + 1 timed step each, CUDA events); the per-replica step time is
-    fitted as a + b N + c N^2 and summed over the whole workload."""
+    KSPSolve path moved to the GPU.  The same replicas are also stepped one at a time
+    with the structured solve, which splits the headline ratio into algorithm
+    (MINRES -> structured, one replica at a time), batching (one at a time -> batched,
+    FP64) and precision (FP64 -> mixed, batched).  A stratified sample that includes
+    the three largest replicas is stepped (one timed step each, CUDA events); the
+    per-replica step time is fitted as a + b N + c N^2 and summed over the workload."""
     import torch
     from polystokes_brownian_b200 import _capi
     from polystokes_brownian_b200.engine import Batch
@@ -339,47 +463,59 @@ def plain_fp64(systems, args, budget_s=60.0):
     order = np.argsort(Ns)
     k = min(args.plain_sample, len(systems))
     pick = [int(order[int(round(i * (len(order) - 1) / max(1, k - 1)))]) for i in range(k)]
+    pick += [int(i) for i in order[-3:]]
     pick = sorted(set(pick), key=lambda i: Ns[i])
-    n, ms, iters = [], [], []
-    t_start = time.perf_counter()
-    for idx in pick:
-        b = Batch([systems[idx]], precision=_capi.PS_PREC_FP64)
-        if len(systems) > 1:      # single large systems: one step, no warm-up (bounded time)
-            b.step(rtol=args.rtol, maxit=50000, solver=_capi.PS_SOLVE_MINRES)
-        st = torch.cuda.current_stream()
+    st = torch.cuda.current_stream()
+
+    def timed_step(b, solver):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        r = b.step(rtol=args.rtol, maxit=50000, solver=_capi.PS_SOLVE_MINRES)
+        r = b.step(rtol=args.rtol, maxit=50000, solver=solver)
         e1.record(st)
         e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
+        return e0.elapsed_time(e1), r
+
+    n, ms, ms_struct, iters = [], [], [], []
+    t_start = time.perf_counter()
+    for idx in pick:
+        for solver in (_capi.PS_SOLVE_STRUCTURED, _capi.PS_SOLVE_MINRES):
+            b = Batch([systems[idx]], precision=_capi.PS_PREC_FP64)
+            if solver == _capi.PS_SOLVE_STRUCTURED or Ns[idx] < 1000:
+                b.step(rtol=args.rtol, maxit=50000, solver=solver)     # warm-up (skipped for the long MINRES runs)
+            t, r = timed_step(b, solver)
+            b.close()
+            if solver == _capi.PS_SOLVE_MINRES:
+                ms.append(t)
+                iters.append(max(r.iters))
+            else:
+                ms_struct.append(t)
         n.append(systems[idx].Np)
-        iters.append(max(r.iters))
-        b.close()
         if time.perf_counter() - t_start > budget_s:
             break
-    n = np.array(n, float)
-    A = np.stack([np.ones_like(n), n, n * n], 1)
-    coef, *_ = np.linalg.lstsq(A, np.array(ms), rcond=None)
-    if len(n) < 3 or np.any(A @ coef <= 0):
-        coef = np.array([0.0, 0.0, float(np.sum(ms) / np.sum(n * n))])
-    total_ms = float(sum(max(coef[0] + coef[1] * N + coef[2] * N * N, 1e-3) for N in Ns))
+    total_ms, resid = _fit_project(n, ms, Ns)
+    total_struct, resid_s = _fit_project(n, ms_struct, Ns)
     return {"value": float(Ns.sum()) / (total_ms * 1e-3), "unit": METRIC, "ms_per_step_projected": total_ms,
             "sample_N": [int(v) for v in n], "sample_ms": ms, "sample_max_minres_iters": iters,
+            "fit_rms_rel_residual": resid,
             "form": "FP64, one replica per context, Jacobi-preconditioned MINRES (the reference's KSPSolve), "
                     "rtol as the batched run",
-            "projection": "per-replica step time fitted as a + b N + c N^2 over the sample, summed over all replicas"}
+            "projection": "per-replica step time fitted as a + b N + c N^2 over the sample, summed over all replicas",
+            "structured_single": {"value": float(Ns.sum()) / (total_struct * 1e-3), "unit": METRIC,
+                                  "ms_per_step_projected": total_struct, "sample_ms": ms_struct,
+                                  "fit_rms_rel_residual": resid_s,
+                                  "form": "FP64, one replica per context, structured solve"}}
 
 
-def velocity_error(systems, args):
+def velocity_error(systems, args, precision=None):
     """Relative velocity error of one step of the benchmarked form against FP64
     at rtol 1e-10 on the same state and the same injected noise (first
     err_sample replicas)."""
     import torch
     from polystokes_brownian_b200 import _capi
     from polystokes_brownian_b200.engine import Batch
-    sub = systems[: args.err_sample]
-    prec = _capi.PS_PREC_MIXED if args.precision == "mixed" else _capi.PS_PREC_FP64
+    sub = systems[: max(1, args.err_sample)]
+    precision = precision or args.precision
+    prec = _capi.PS_PREC_MIXED if precision == "mixed" else _capi.PS_PREC_FP64
     solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
     out = []
     for pr, rt in ((prec, args.rtol), (_capi.PS_PREC_FP64, 1e-10)):
@@ -392,6 +528,76 @@ def velocity_error(systems, args):
     err = float(np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1]))
     return {"rel_err_up": err, "replicas": len(sub), "against": "FP64 at rtol 1e-10, same state and injected noise",
             "bound": 1e-6, "ok": err <= 1e-6}
+
+
+def time_steps(systems, precision, solver, rtol, steps, warmup=1):
+    """Device time of `steps` steps of one context (CUDA events, after `warmup` steps)."""
+    import torch
+    from polystokes_brownian_b200.engine import Batch
+    b = Batch(systems, precision=precision)
+    st = torch.cuda.current_stream()
+    its = []
+    for _ in range(warmup):
+        b.step(rtol=rtol, maxit=50000, solver=solver)
+    torch.cuda.synchronize()
+    lat = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        r = b.step(rtol=rtol, maxit=50000, solver=solver)
+        e1.record(st)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+        its.append(max(r.iters))
+    x, _ = b.state()
+    finite = bool(torch.isfinite(x).all().item())
+    b.close()
+    beads = sum(s.Np for s in systems)
+    lat_s = sorted(lat)
+    return {"value": beads * steps / (sum(lat) * 1e-3), "unit": METRIC, "ms_per_step": sum(lat) / steps,
+            "p50_ms": lat_s[len(lat) // 2], "p99_ms": lat_s[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "steps": steps, "warmup": warmup, "max_solver_iters": max(its), "state_finite": finite}
+
+
+def config_entries(args):
+    """Bounded runs of the other benchmark configurations, each on its own context:
+    C1 polymer + probes (plain FP64 drop-in: Jacobi MINRES), C2 1024-colloid suspension
+    with lubrication and C3 4097-bead brush (mixed and FP64, with the mixed form's
+    velocity error), C5 a short serving trace (p50/p99 step and request latency)."""
+    from polystokes_brownian_b200 import _capi, serve
+    F64, MIX = _capi.PS_PREC_FP64, _capi.PS_PREC_MIXED
+    ST, MR = _capi.PS_SOLVE_STRUCTURED, _capi.PS_SOLVE_MINRES
+    out = {}
+    c1 = configs.polymer_probe(seed=args.seed)
+    out["C1_polymer_probe222"] = {
+        "plain_fp64_minres": time_steps([c1], F64, MR, args.rtol, steps=20, warmup=2),
+        "fp64_structured": time_steps([c1], F64, ST, args.rtol, steps=20, warmup=2),
+        "config": "2 probes (a_c = 3) + 11 harmonic chains x 20 beads, shell path, dt 1e-3, rtol as the headline"}
+    s2 = configs.suspension(seed=args.seed)
+    s2 = configs.System(s2.name, dict(s2.params, lub_on=1, lub_gap=0.5), s2.x)
+    e2 = argparse.Namespace(**vars(args))
+    e2.err_sample = 1
+    out["C2_suspension1024_lub"] = {
+        "mixed": time_steps([s2], MIX, ST, args.rtol, steps=5, warmup=2),
+        "fp64": time_steps([s2], F64, ST, args.rtol, steps=5, warmup=2),
+        "velocity_error": velocity_error([s2], e2, "mixed"),
+        "config": "1024 colloids, volume fraction 0.2, lubrication for gaps < 0.5 a, dt 1e-4; colloid blocks are "
+                  "FP64 in both forms"}
+    s3 = configs.brush(seed=args.seed)
+    out["C3_brush4097"] = {
+        "mixed": time_steps([s3], MIX, ST, args.rtol, steps=5, warmup=2),
+        "fp64": time_steps([s3], F64, ST, args.rtol, steps=5, warmup=2),
+        "velocity_error": velocity_error([s3], e2, "mixed"),
+        "config": "1 colloid (a_c = 5) + 128 FENE chains x 32 beads, full monomer HI, dt 1e-4"}
+    trace = serve.make_trace(12, rate=4.0, seed=args.seed, nmax=4096, smax=40, lub=True)
+    c5 = {"requests": len(trace), "rate_per_s": 4.0, "N": "log-uniform in [64, 4096]", "steps": "uniform in [10, 40]"}
+    for name, prec in (("mixed", MIX), ("fp64", F64)):
+        srv = serve.Server(precision=prec, rebuild_every=4, rtol=args.rtol)
+        t0 = time.perf_counter()
+        res = srv.run(trace)
+        c5[name] = srv.stats(res, time.perf_counter() - t0)
+    out["C5_serving"] = c5
+    return out
 
 
 def run_b200(args):
@@ -522,10 +728,27 @@ def run_b200(args):
             extra["plain_fp64_drop_in"] = pf
         if args.err_sample > 0:
             extra["velocity_error"] = velocity_error(systems, args)
+        if "fp64_batched" in extra and "plain_fp64_drop_in" in extra:
+            pf, fb = extra["plain_fp64_drop_in"], extra["fp64_batched"]["value"]
+            ss = pf["structured_single"]["value"]
+            extra["decomposition"] = {
+                "algorithm": ss / pf["value"], "batching": fb / ss, "precision": value / fb,
+                "total": value / pf["value"],
+                "note": "algorithm: FP64 one replica at a time, Jacobi MINRES -> structured solve; batching: FP64 "
+                        "structured, one at a time -> all replicas in one context; precision: FP64 batched -> mixed "
+                        "batched (one-at-a-time forms projected from the same sample)"}
+        if args.workload == "ensemble" and not args.no_configs:
+            extra["configs"] = config_entries(args)
 
     if rank == 0:
-        ss, sd = scaled_instances(args) if len(systems) == 1 and systems[0].Np > 700 else (None, None)
-        cb = cpu_baseline(systems, rtol=args.rtol, sample_systems=ss, sample_desc=sd) if world == 1 else None
+        from oracle import refrun
+        cb = None
+        if world == 1:
+            if len(systems) > 1 and refrun.available():
+                cb = cpu_baseline_ref(systems, args.rtol)
+            else:
+                ss, sd = scaled_instances(args) if len(systems) == 1 and systems[0].Np > 700 else (None, None)
+                cb = cpu_baseline(systems, rtol=args.rtol, sample_systems=ss, sample_desc=sd)
         lat_sorted = sorted(lat)
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,

@@ -240,8 +240,14 @@ int ps_step_outputs(ps_ctx *ctx, double *up, double *udiff, double *sb, double *
  * It allocates nothing: its scratch is a fixed 3.4 MB __device__ array held by
  * every GPU that loads this library until exit, so N is limited to 8192
  * (larger N returns PS_ERR_TOO_LARGE).  The first call on a device looks up the
- * array's device address and should come before any stream capture.  Calls
- * share the array, so calls that overlap on the GPU race; serialise them. */
+ * array's device address (cudaGetSymbolAddress) and caches it for the device.
+ * With CUDA's lazy module loading (the CUDA 12 default) that first call may also
+ * be where the library's device code is loaded and the 3.4 MB array placed,
+ * which can synchronise the device or fail under memory pressure: make the first
+ * call at start-up, before any stream capture and before the device fills up.
+ * After cudaDeviceReset the cached address is stale; do not call it again in
+ * that process.  Calls share the array, so calls that overlap on the GPU race;
+ * serialise them. */
 int ps_mobility_apply_noalloc(const double *x, const double *u, double *y, int32_t N, double beta,
                               int32_t chain_HI, int32_t Nmono_per_chain, void *stream);
 

@@ -387,8 +387,15 @@ PetscErrorCode MatDestroy(Mat *A)
 static PetscErrorCode mult_into(Mat A, const PetscScalar *x, PetscScalar *y)
 {
     if (A->kind == MK_DENSE) {
+        /* four columns per sweep of y (a blocked column-oriented gemv) */
         std::fill(y, y + A->m, 0.0);
-        for (PetscInt j = 0; j < A->n; j++) {
+        PetscInt j = 0;
+        for (; j + 4 <= A->n; j += 4) {
+            const PetscScalar x0 = x[j], x1 = x[j + 1], x2 = x[j + 2], x3 = x[j + 3];
+            const PetscScalar *c0 = A->a + (size_t)j * A->lda, *c1 = c0 + A->lda, *c2 = c1 + A->lda, *c3 = c2 + A->lda;
+            for (PetscInt i = 0; i < A->m; i++) y[i] += c0[i] * x0 + c1[i] * x1 + c2[i] * x2 + c3[i] * x3;
+        }
+        for (; j < A->n; j++) {
             const PetscScalar xj = x[j];
             const PetscScalar *col = A->a + (size_t)j * A->lda;
             for (PetscInt i = 0; i < A->m; i++) y[i] += col[i] * xj;
