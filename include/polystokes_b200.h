@@ -260,6 +260,11 @@ int ps_mobility_apply_noalloc(const double *x, const double *u, double *y, int32
  * FMA chains). */
 int ps_time_kernel(ps_ctx *ctx, int32_t which, int32_t reps, const double *u, double *ms, void *stream);
 int ps_fma_peak(int32_t fp64, double *tflops, void *stream);
+/* ps_rsqrt_check (no reference counterpart): the largest distance, in units in the
+ * last place, between the FP64 pair kernel's reciprocal square root (single-
+ * precision seed + second-order binomial correction) and CUDA's rsqrt over the
+ * n device values a. */
+int ps_rsqrt_check(const double *a, int64_t n, uint64_t *max_ulp, void *stream);
 /* number of kernels the library has launched since it was loaded */
 uint64_t ps_kernel_launches(void);
 /* Autotuner (no counterpart in the reference): times the whole mobility apply

@@ -175,6 +175,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         E.maxNp = std::max(E.maxNp, s.Np);
         if (d.kT > 0) kTpos++; else kTzero++;
         if (d.mm_HI) E.any_mmhi = true;
+        if (d.mm_HI && d.Nm >= 2) (d.aa_mode == PS_AA_RPY ? E.any_aa_rpy : E.any_aa_ref) = true;
         E.segs[r] = s;
     }
     if (kTpos && kTzero) {
@@ -695,6 +696,15 @@ int ps_fma_peak(int32_t fp64, double *tflops, void *stream)
 {
     if (!tflops) return PS_ERR_ARG;
     return ps::fma_peak(fp64, tflops, S(stream));
+}
+
+int ps_rsqrt_check(const double *a, int64_t n, uint64_t *max_ulp, void *stream)
+{
+    if ((!a && n > 0) || n < 0 || !max_ulp) return PS_ERR_ARG;
+    unsigned long long m = 0;
+    int rc = ps::rsqrt_check(a, (long)n, &m, S(stream));
+    *max_ulp = (uint64_t)m;
+    return rc;
 }
 
 }  // extern "C"

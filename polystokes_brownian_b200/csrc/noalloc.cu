@@ -74,6 +74,8 @@ k_na_pairs(const double *__restrict__ u, int N, double beta, int chain_hi, int n
             double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             double r2 = dx * dx + dy * dy + dz * dz;
             double rinv = rsqrt(r2), r = r2 * rinv, xx, yy;
+            // near the jump of the reference's scalars at 2 beta, its own distance decides the branch
+            if (fabs(r2 - 4.0 * beta * beta) <= 1e-10 * r2) { r = ref_pair_dist(dx, dy, dz); rinv = 1.0 / r; }
             aa_scalars<double>(r, rinv, 2.0 * beta, xx, yy);
             double u0 = su[3 * k], u1 = su[3 * k + 1], u2 = su[3 * k + 2];
             double f = (xx - yy) * (dx * u0 + dy * u1 + dz * u2) * rinv * rinv;

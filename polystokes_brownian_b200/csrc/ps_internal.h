@@ -71,6 +71,17 @@ template <> __device__ __forceinline__ double rsqrt_t<double>(double v) { return
 template <> __device__ __forceinline__ float rsqrt_t<float>(float v) { return rsqrtf(v); }
 
 // ---------------------------------------------------------------------------
+// The reference's pair distance, dr = sqrt(dx*dx + dy*dy + dz*dz) in double with
+// no fused multiply-add (check_dist.cpp:48-53), which decides the monomer pair
+// branch dr > 2 beta (mob.cpp:123).  The reference's own monomer scalars jump
+// at dr = 2 beta, and chain bonds often sit exactly there, so every kernel that
+// takes that branch decides it with this distance.
+__device__ __forceinline__ double ref_pair_dist(double dx, double dy, double dz)
+{
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+}
+
+// ---------------------------------------------------------------------------
 // AA: reference-specific monomer-monomer scalars (mob.cpp:122-131).
 // mob_a = x ee + y (I - ee)   =>   mob_a u = y u + (x - y)(e.u) e
 template <class T>

@@ -43,6 +43,7 @@ struct Engine {
     long ntot = 0, ncoll = 0, nvec = 0, ntop = 0, nvel = 0;
     int maxNp = 0;
     bool any_lub = false, any_shell_schur = false, any_kT = false, any_mmhi = false;
+    bool any_aa_ref = false, any_aa_rpy = false;   // monomer HI replicas in the reference's / RPY pair scalars
 
     Seg *d_segs = nullptr;
     int *d_vec_offs = nullptr, *d_top_offs = nullptr, *d_vel_offs = nullptr, *d_bead_offs = nullptr;
@@ -189,6 +190,7 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
                     const void *done = nullptr, int done_stride = 0, bool skip_aa = false);
 int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cudaStream_t st);
 int fma_peak(int fp64, double *tflops, cudaStream_t st);
+int rsqrt_check(const double *a, long n, unsigned long long *max_ulp, cudaStream_t st);
 // lub.cu
 void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st);
 void lub_apply_vel(Engine &E, const double *u_vel, double *y_vel, cudaStream_t st);

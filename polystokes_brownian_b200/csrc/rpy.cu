@@ -38,101 +38,6 @@ template <> struct Acc<float> {
 };
 
 // ---------------------------------------------------------------------------
-// AA: monomer rows x monomer columns (mm_HI only), 3 -> 3.
-// pos: (x,y,z,chain) per bead.  u: input vector, monomer F at off + 3 m.
-// Launched as k_rpy_aa<double> (the FP64 form); the mixed form runs
-// k_rpy_aa_f2 below, so the FP32 branches here are not instantiated.
-template <class T>
-__global__ void __launch_bounds__(RPY_THREADS, 4)
-k_rpy_aa(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
-         const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
-         long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
-{
-    if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
-    // FP32: positions are split hi + lo (both float) so that pair separations
-    // keep FP64-level accuracy: d = (hi_i - hi_j) + (lo_i - lo_j).
-    typedef typename V4<T>::t P4;
-    constexpr bool F32 = sizeof(T) == 4;
-    __shared__ P4 sp[RPY_THREADS];
-    __shared__ float4 sl[F32 ? RPY_THREADS : 1];
-    __shared__ T su[RPY_THREADS * 3];
-    const Tile tl = tiles[blockIdx.x];
-    const Seg &sg = segs[tl.rep];
-    const int c = blockIdx.y;
-    nchunk = sg.nch_aa;               // per-replica chunk count: a function of Nm alone
-    if (c >= nchunk) return;
-    const int Nm = sg.Nm;
-    const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
-    const int i = tl.row0 + threadIdx.x;
-    const bool active = threadIdx.x < tl.nrow;
-    const int uoff = in_top ? sg.top_off : sg.vec_off;
-    P4 pi = active ? pos[sg.bead_off + i] : pos[sg.bead_off + tl.row0];
-    float4 li = make_float4(0.f, 0.f, 0.f, 0.f);
-    if constexpr (F32) li = plo[sg.bead_off + (active ? i : tl.row0)];
-    const T two_beta = T(2.0 * sg.beta);
-    const bool chain_hi = sg.chain_HI != 0;
-    // scalars in FP64 from the mode (x = c0/r + c1/r^3, ... as in Seg::aa_c)
-    T c0, c1, c2, c3, c4, c5, c6, c7;
-    if (sg.aa_mode == PS_AA_RPY) {
-        T b = T(sg.beta), b2 = b * b;
-        c0 = T(1.5); c1 = -b2; c2 = T(0.75); c3 = T(0.5) * b2;
-        c4 = T(1) / b; c5 = T(-0.1875) / b2; c6 = T(1) / b; c7 = T(-0.28125) / b2;
-    } else {
-        c0 = T(0.375); c1 = T(-2.0); c2 = T(0.75); c3 = T(-0.5);
-        c4 = T(-1.0); c5 = T(0.375); c6 = T(1.0); c7 = T(-0.28125);
-    }
-    Acc<T> a0, a1, a2;
-    a0.zero(); a1.zero(); a2.zero();
-    for (int jt = j0; jt < j1; jt += RPY_THREADS) {
-        int nj = min(RPY_THREADS, j1 - jt);
-        __syncthreads();
-        if (threadIdx.x < nj) {
-            int j = jt + threadIdx.x;
-            sp[threadIdx.x] = pos[sg.bead_off + j];
-            if constexpr (F32) sl[threadIdx.x] = plo[sg.bead_off + j];
-            su[3 * threadIdx.x + 0] = (T)u[uoff + 3 * j + 0];
-            su[3 * threadIdx.x + 1] = (T)u[uoff + 3 * j + 1];
-            su[3 * threadIdx.x + 2] = (T)u[uoff + 3 * j + 2];
-        }
-        __syncthreads();
-        T t0 = 0, t1 = 0, t2 = 0;
-        for (int k = 0; k < nj; k++) {
-            P4 pj = sp[k];
-            T dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            if constexpr (F32) {
-                float4 lj = sl[k];
-                dx += li.x - lj.x; dy += li.y - lj.y; dz += li.z - lj.z;
-            }
-            T r2 = dx * dx + dy * dy + dz * dz;
-            bool skip = (jt + k == i) || (chain_hi && pi.w == pj.w);
-            if (skip) continue;
-            T rinv = rsqrt_t<T>(r2);
-            T r = r2 * rinv;
-            T x, y;
-            if (r > two_beta) {
-                T ri3 = rinv * rinv * rinv;
-                x = c0 * rinv + c1 * ri3;
-                y = c2 * rinv + c3 * ri3;
-            } else {
-                x = c4 + c5 * r;
-                y = c6 + c7 * r;
-            }
-            T u0 = su[3 * k], u1 = su[3 * k + 1], u2 = su[3 * k + 2];
-            // mob_a u = y u + (x - y)(e.u) e,  e = d / r
-            T f = (x - y) * (dx * u0 + dy * u1 + dz * u2) * rinv * rinv;
-            t0 += y * u0 + f * dx;
-            t1 += y * u1 + f * dy;
-            t2 += y * u2 + f * dz;
-        }
-        a0.add(t0); a1.add(t1); a2.add(t2);
-    }
-    if (active) {
-        double *o = part + (long)c * part_stride + sg.top_off + 3 * i;
-        o[0] = (double)a0.get(); o[1] = (double)a1.get(); o[2] = (double)a2.get();
-    }
-}
-
-// ---------------------------------------------------------------------------
 // AA in FP32 with packed FP32x2 arithmetic (sm_100 FFMA2/FADD2/FMUL2), column
 // pairs in the two lanes: a thread owns rows i and i + 64 of a 128-row tile,
 // each held as a broadcast pair (loop-invariant), and advances both against
@@ -170,14 +75,14 @@ __device__ __forceinline__ void aa_near_lane(bool n, float r2, float ri, float r
     }
 }
 
-template <bool CHECK>
+template <bool CHECK, bool REF>
 __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sXY, const float4 *__restrict__ sZU,
                                            const float4 *__restrict__ sUU, const float4 *__restrict__ sLA,
                                            const float4 *__restrict__ sLB, int jt, int np, int iA, int iB,
                                            bool chain_hi, float wA, float wB, float2 ax, float2 ay, float2 az,
                                            float2 bx, float2 by, float2 bz, const float4 *__restrict__ plo, int bA,
                                            int bB, float2 fa, float2 fb, float2 fc, float2 fd, const Seg &sg,
-                                           float te2, float2 (&t)[6])
+                                           float te2, const double4 *__restrict__ p64, float2 (&t)[6])
 {
 #pragma unroll 1
     for (int k = 0; k < np; k++) {
@@ -218,10 +123,25 @@ __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sXY, const
         if (inner) {
             const float tb2 = (float)(4.0 * sg.beta * sg.beta);
             const float nx0 = sg.aa_c[4], nx1 = sg.aa_c[5], ny0 = sg.aa_c[6], ny1 = sg.aa_c[7];
-            aa_near_lane(!eA0 && r2A.x <= tb2, r2A.x, riA.x, ri2A.x, nx0, nx1, ny0, ny1, yA.x, gA.x);
-            aa_near_lane(!eA1 && r2A.y <= tb2, r2A.y, riA.y, ri2A.y, nx0, nx1, ny0, ny1, yA.y, gA.y);
-            aa_near_lane(!eB0 && r2B.x <= tb2, r2B.x, riB.x, ri2B.x, nx0, nx1, ny0, ny1, yB.x, gB.x);
-            aa_near_lane(!eB1 && r2B.y <= tb2, r2B.y, riB.y, ri2B.y, nx0, nx1, ny0, ny1, yB.y, gB.y);
+            bool nA0 = !eA0 && r2A.x <= tb2, nA1 = !eA1 && r2A.y <= tb2, nB0 = !eB0 && r2B.x <= tb2,
+                 nB1 = !eB1 && r2B.y <= tb2;
+            if constexpr (REF) {
+                // the reference's scalars jump at 2 beta (chain bonds often sit there): within a
+                // band of the FP32 test its own FP64 distance decides (RPY is continuous there)
+                const double tb = 2.0 * sg.beta;
+                const int j = jt + 2 * k;
+                auto decide = [&](bool e, float r2, int bi, int jj, bool &n) {
+                    if (e || fabsf(r2 - tb2) > 1e-5f * tb2) return;
+                    const double4 P = p64[bi], Q = p64[sg.bead_off + jj];
+                    n = !(ref_pair_dist(P.x - Q.x, P.y - Q.y, P.z - Q.z) > tb);
+                };
+                decide(eA0, r2A.x, bA, j, nA0); decide(eA1, r2A.y, bA, j + 1, nA1);
+                decide(eB0, r2B.x, bB, j, nB0); decide(eB1, r2B.y, bB, j + 1, nB1);
+            }
+            aa_near_lane(nA0, r2A.x, riA.x, ri2A.x, nx0, nx1, ny0, ny1, yA.x, gA.x);
+            aa_near_lane(nA1, r2A.y, riA.y, ri2A.y, nx0, nx1, ny0, ny1, yA.y, gA.y);
+            aa_near_lane(nB0, r2B.x, riB.x, ri2B.x, nx0, nx1, ny0, ny1, yB.x, gB.x);
+            aa_near_lane(nB1, r2B.y, riB.y, ri2B.y, nx0, nx1, ny0, ny1, yB.y, gB.y);
         }
         // mob_a u = y u + (x - y)(d.u) d / r^2
         const float2 u0 = make_float2(ZU.z, ZU.w), u1 = make_float2(UU.x, UU.y), u2 = make_float2(UU.z, UU.w);
@@ -236,10 +156,12 @@ __device__ __forceinline__ void aa_f2_cols(const float4 *__restrict__ sXY, const
     }
 }
 
+template <bool REF>
 __global__ void __launch_bounds__(AAF_THREADS, 12)
 k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const float4 *__restrict__ pos,
-            const float4 *__restrict__ plo, const float *__restrict__ aa_te2, const double *__restrict__ u, int in_top,
-            double *__restrict__ part, long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
+            const float4 *__restrict__ plo, const float *__restrict__ aa_te2, const double4 *__restrict__ p64,
+            const double *__restrict__ u, int in_top, double *__restrict__ part, long part_stride, int nchunk,
+            const char *__restrict__ done, int done_stride)
 {
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     __shared__ float4 sXY[64], sZU[64], sUU[64], sLA[64], sLB[64];
@@ -249,6 +171,8 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
     const int c = blockIdx.y;
     nchunk = sg.nch_aa;               // per-replica chunk count: a function of Nm alone
     if (c >= nchunk) return;
+    // one instance per pair-scalar family: the reference's scalars take the FP64 branch decision
+    if ((sg.aa_mode == PS_AA_REFERENCE) != REF) return;
     const int Nm = sg.Nm, tid = threadIdx.x;
     const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
     const int iA = tl.row0 + tid, iB = iA + AAF_THREADS;
@@ -292,11 +216,11 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
         // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
         const bool check = chain_hi || (jt < tl.row0 + 2 * AAF_THREADS && jt + nj > tl.row0);
         if (check)
-            aa_f2_cols<true>(sXY, sZU, sUU, sLA, sLB, jt, np, iA, iB, chain_hi, PA.w, PB.w, ax, ay, az, bx, by, bz,
-                             plo, bA, bB, fa, fb, fc, fd, sg, te2, t);
+            aa_f2_cols<true, REF>(sXY, sZU, sUU, sLA, sLB, jt, np, iA, iB, chain_hi, PA.w, PB.w, ax, ay, az, bx, by,
+                                  bz, plo, bA, bB, fa, fb, fc, fd, sg, te2, p64, t);
         else
-            aa_f2_cols<false>(sXY, sZU, sUU, sLA, sLB, jt, np, iA, iB, chain_hi, PA.w, PB.w, ax, ay, az, bx, by, bz,
-                              plo, bA, bB, fa, fb, fc, fd, sg, te2, t);
+            aa_f2_cols<false, REF>(sXY, sZU, sUU, sLA, sLB, jt, np, iA, iB, chain_hi, PA.w, PB.w, ax, ay, az, bx, by,
+                                   bz, plo, bA, bB, fa, fb, fc, fd, sg, te2, p64, t);
         // fold the two column lanes, then Kahan across column tiles
 #pragma unroll
         for (int q = 0; q < 6; q++) {
@@ -310,6 +234,141 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
     double *o = part + (long)c * part_stride + sg.top_off;
     if (actA) { o[3 * iA] = sK[0][tid]; o[3 * iA + 1] = sK[1][tid]; o[3 * iA + 2] = sK[2][tid]; }
     if (actB) { o[3 * iB] = sK[3][tid]; o[3 * iB + 1] = sK[4][tid]; o[3 * iB + 2] = sK[5][tid]; }
+}
+
+// ---------------------------------------------------------------------------
+// AA in FP64, two rows per thread.  A thread owns rows i and i + 64 of a 128-row
+// tile and sweeps 128-column tiles staged in shared memory as (x, y, z, chain)
+// and (u0, u1, u2, 0) double4 pairs, so each column's loads serve both rows.
+// Reciprocal square root: a single-precision seed refined by the second-order
+// term of the binomial series (1 - e)^(-1/2) = 1 + e/2 + 3 e^2 / 8 + O(e^3),
+// e = 1 - a y0^2 (Householder's iteration of order 2 for f(y) = y^-2 - a): from
+// a seed accurate to 2^-22 the truncation is below 2^-64, so the result is
+// within a couple of ulp of the correctly rounded value (checked against CUDA's
+// rsqrt by ps_rsqrt_check).  Self pairs and skipped same-chain pairs get
+// ri = 0, which zeroes their contribution; the near form (r <= 2 beta) is taken
+// under a warp vote.  Far form in factored scalars: y = ri (c + d ri^2),
+// (x - y) / r^2 = ri^3 (a + b ri^2), a = c0 - c2, b = c1 - c3, c = c2, d = c3.
+constexpr int AAD_THREADS = 64;
+
+__device__ __forceinline__ double rsqrt_seeded(double a)
+{
+    const double y = (double)rsqrtf((float)a);
+    const double e = fma(-(a * y), y, 1.0);
+    return fma(y * e, fma(0.375, e, 0.5), y);
+}
+
+template <bool CHECK>
+__device__ __forceinline__ void aa_d2_cols(const double4 *__restrict__ sP, const double4 *__restrict__ sU, int jt,
+                                           int nj, int iA, int iB, bool chain_hi, double4 PA, double4 PB, double ca,
+                                           double cb, double cc, double cd, double tb, double tb2, double n0,
+                                           double n1, double n2, double n3, double (&t)[6])
+{
+#pragma unroll 1
+    for (int k = 0; k < nj; k++) {
+        const double4 P = sP[k], U = sU[k];
+        const double ax = PA.x - P.x, ay = PA.y - P.y, az = PA.z - P.z;
+        const double bx = PB.x - P.x, by = PB.y - P.y, bz = PB.z - P.z;
+        const double r2A = fma(az, az, fma(ay, ay, ax * ax));
+        const double r2B = fma(bz, bz, fma(by, by, bx * bx));
+        bool sA = false, sB = false;
+        if constexpr (CHECK) {
+            const int j = jt + k;
+            sA = (j == iA) || (chain_hi && PA.w == P.w);
+            sB = (j == iB) || (chain_hi && PB.w == P.w);
+        }
+        const double riA = sA ? 0.0 : rsqrt_seeded(r2A), riB = sB ? 0.0 : rsqrt_seeded(r2B);
+        const double qA = riA * riA, qB = riB * riB;
+        double yA = riA * fma(cd, qA, cc), yB = riB * fma(cd, qB, cc);
+        double gA = (qA * riA) * fma(cb, qA, ca), gB = (qB * riB) * fma(cb, qB, ca);
+        // candidates for the near form; the reference's own distance decides within the band
+        const bool nA = !sA && r2A <= tb2 * (1.0 + 1e-10), nB = !sB && r2B <= tb2 * (1.0 + 1e-10);
+        if (__any_sync(0xffffffffu, nA || nB)) {
+            if (nA) {
+                const double r = ref_pair_dist(ax, ay, az);
+                if (!(r > tb)) { const double ri = 1.0 / r, x = fma(n1, r, n0); yA = fma(n3, r, n2); gA = (x - yA) * ri * ri; }
+            }
+            if (nB) {
+                const double r = ref_pair_dist(bx, by, bz);
+                if (!(r > tb)) { const double ri = 1.0 / r, x = fma(n1, r, n0); yB = fma(n3, r, n2); gB = (x - yB) * ri * ri; }
+            }
+        }
+        const double hA = gA * fma(az, U.z, fma(ay, U.y, ax * U.x));
+        const double hB = gB * fma(bz, U.z, fma(by, U.y, bx * U.x));
+        t[0] = fma(hA, ax, fma(yA, U.x, t[0]));
+        t[1] = fma(hA, ay, fma(yA, U.y, t[1]));
+        t[2] = fma(hA, az, fma(yA, U.z, t[2]));
+        t[3] = fma(hB, bx, fma(yB, U.x, t[3]));
+        t[4] = fma(hB, by, fma(yB, U.y, t[4]));
+        t[5] = fma(hB, bz, fma(yB, U.z, t[5]));
+    }
+}
+
+__global__ void __launch_bounds__(AAD_THREADS, 8)
+k_rpy_aa_d2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
+            const double *__restrict__ u, int in_top, double *__restrict__ part, long part_stride, int nchunk,
+            const char *__restrict__ done, int done_stride)
+{
+    if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
+    __shared__ double4 sP[128], sU[128];
+    const Tile tl = tiles[blockIdx.x];
+    const Seg &sg = segs[tl.rep];
+    const int c = blockIdx.y;
+    nchunk = sg.nch_aa;               // per-replica chunk count: a function of Nm alone
+    if (c >= nchunk) return;
+    const int Nm = sg.Nm, tid = threadIdx.x;
+    const int j0 = (int)((long)Nm * c / nchunk), j1 = (int)((long)Nm * (c + 1) / nchunk);
+    const int iA = tl.row0 + tid, iB = iA + AAD_THREADS;
+    const bool actA = tid < tl.nrow, actB = tid + AAD_THREADS < tl.nrow;
+    const int uoff = in_top ? sg.top_off : sg.vec_off;
+    const double4 PA = pos[sg.bead_off + (actA ? iA : tl.row0)], PB = pos[sg.bead_off + (actB ? iB : tl.row0)];
+    const bool chain_hi = sg.chain_HI != 0;
+    double c0, c1, c2, c3, n0, n1, n2, n3;
+    if (sg.aa_mode == PS_AA_RPY) {
+        const double b = sg.beta, b2 = b * b;
+        c0 = 1.5; c1 = -b2; c2 = 0.75; c3 = 0.5 * b2;
+        n0 = 1.0 / b; n1 = -0.1875 / b2; n2 = 1.0 / b; n3 = -0.28125 / b2;
+    } else {
+        c0 = 0.375; c1 = -2.0; c2 = 0.75; c3 = -0.5;
+        n0 = -1.0; n1 = 0.375; n2 = 1.0; n3 = -0.28125;
+    }
+    const double tb = 2.0 * sg.beta, ca = c0 - c2, cb = c1 - c3, tb2 = tb * tb;
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (int jt = j0; jt < j1; jt += 128) {
+        const int nj = min(128, j1 - jt);
+        __syncthreads();
+        for (int h = 0; h < 2; h++) {
+            const int jl = tid + h * AAD_THREADS;
+            if (jl < nj) {
+                const int j = jt + jl;
+                sP[jl] = pos[sg.bead_off + j];
+                sU[jl] = make_double4(u[uoff + 3 * j], u[uoff + 3 * j + 1], u[uoff + 3 * j + 2], 0.0);
+            }
+        }
+        __syncthreads();
+        double t[6] = {0, 0, 0, 0, 0, 0};
+        // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
+        const bool check = chain_hi || (jt < tl.row0 + 2 * AAD_THREADS && jt + nj > tl.row0);
+        if (check)
+            aa_d2_cols<true>(sP, sU, jt, nj, iA, iB, chain_hi, PA, PB, ca, cb, c2, c3, tb, tb2, n0, n1, n2, n3, t);
+        else
+            aa_d2_cols<false>(sP, sU, jt, nj, iA, iB, chain_hi, PA, PB, ca, cb, c2, c3, tb, tb2, n0, n1, n2, n3, t);
+#pragma unroll
+        for (int q = 0; q < 6; q++) a[q] += t[q];
+    }
+    double *o = part + (long)c * part_stride + sg.top_off;
+    if (actA) { o[3 * iA] = a[0]; o[3 * iA + 1] = a[1]; o[3 * iA + 2] = a[2]; }
+    if (actB) { o[3 * iB] = a[3]; o[3 * iB + 1] = a[4]; o[3 * iB + 2] = a[5]; }
+}
+
+// max |own - CUDA| / ulp(CUDA) of the reciprocal square root over a[0..n)
+__global__ void k_rsqrt_check(long n, const double *__restrict__ a, unsigned long long *__restrict__ worst)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double ref = rsqrt(a[i]), own = rsqrt_seeded(a[i]);
+    long long d = __double_as_longlong(own) - __double_as_longlong(ref);
+    atomicMax(worst, (unsigned long long)(d < 0 ? -d : d));
 }
 
 // ---------------------------------------------------------------------------
@@ -573,11 +632,19 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
     const typename V4<T>::t *pos = (const typename V4<T>::t *)(sizeof(T) == 8 ? (const void *)E.d_pos64 : (const void *)E.d_pos32);
     if (E.n_aa_tiles && !skip_aa) {
         if constexpr (sizeof(T) == 4)
-            ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
-                E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
+        {
+            if (E.any_aa_rpy)
+                ::ps_launch_count++, k_rpy_aa_f2<false><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
+                    E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
+                    E.part_stride, E.nch_aa, done, dstride);
+            if (E.any_aa_ref)
+                ::ps_launch_count++, k_rpy_aa_f2<true><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
+                    E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
+                    E.part_stride, E.nch_aa, done, dstride);
+        }
         else
-            ::ps_launch_count++, k_rpy_aa<T><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(
-                E.d_segs, E.d_aa_tiles, pos, E.d_pos32lo, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
+            ::ps_launch_count++, k_rpy_aa_d2<<<dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st>>>(
+                E.d_segs, E.d_aa_tiles, E.d_pos64, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
     }
     if (E.n_ab_tiles)
         ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
@@ -641,8 +708,11 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     cudaEventCreate(&b);
     auto launch = [&]() {
         if (which == 0 && E.n_aa_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_aa_f2<<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
-            else ::ps_launch_count++, k_rpy_aa<double><<<dim3(E.n_aa_tiles, E.nch_aa), RPY_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+            if (fp32) {
+                if (E.any_aa_rpy) ::ps_launch_count++, k_rpy_aa_f2<false><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+                if (E.any_aa_ref) ::ps_launch_count++, k_rpy_aa_f2<true><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+            }
+            else ::ps_launch_count++, k_rpy_aa_d2<<<dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
         } else if (which == 1 && E.n_ab_tiles) {
             if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
             else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
@@ -663,6 +733,19 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     cudaEventDestroy(b);
     *ms = reps > 0 ? (double)t / reps : 0.0;
     PS_CK(cudaGetLastError());
+    return PS_OK;
+}
+
+// largest distance in ulp between rsqrt_seeded and CUDA's rsqrt over a device array
+int rsqrt_check(const double *a, long n, unsigned long long *max_ulp, cudaStream_t st)
+{
+    unsigned long long *d = nullptr;
+    PS_CK(cudaMallocAsync(&d, sizeof(unsigned long long), st));
+    PS_CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), st));
+    if (n > 0) ::ps_launch_count++, k_rsqrt_check<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, d);
+    PS_CK(cudaMemcpyAsync(max_ulp, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    PS_CK(cudaFreeAsync(d, st));
+    PS_CK(cudaStreamSynchronize(st));
     return PS_OK;
 }
 

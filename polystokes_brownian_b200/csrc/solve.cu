@@ -314,6 +314,8 @@ __device__ void pair_mobility(const Seg &s, const double *__restrict__ x, const 
     double r2 = dx * dx + dy * dy + dz * dz, rinv = 1.0 / sqrt(r2), r = r2 * rinv;
     double e[3] = {dx * rinv, dy * rinv, dz * rinv};
     if (mono) {
+        r = ref_pair_dist(dx, dy, dz);   // the reference's distance decides the near/far branch
+        rinv = 1.0 / r;
         for (int k = 0; k < 6; k++) M[k * 6 + k] = s.beta_inv;
         bool coupled = s.mm_HI && !(s.chain_HI && chain[lo] == chain[hi]);
         if (coupled) {
@@ -375,9 +377,9 @@ k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ b
         double xs = 0.0, ys = 0.0;
         if (s.mm_HI && !(s.chain_HI && chain[lo] == chain[hi])) {
             double dx = x[3 * lo] - x[3 * hi], dy = x[3 * lo + 1] - x[3 * hi + 1], dz = x[3 * lo + 2] - x[3 * hi + 2];
-            double r2 = dx * dx + dy * dy + dz * dz, rinv = 1.0 / sqrt(r2);
-            if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(r2 * rinv, rinv, 2.0 * s.beta, xs, ys);
-            else aa_scalars<double>(r2 * rinv, rinv, 2.0 * s.beta, xs, ys);
+            const double r = ref_pair_dist(dx, dy, dz), rinv = 1.0 / r;
+            if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(r, rinv, 2.0 * s.beta, xs, ys);
+            else aa_scalars<double>(r, rinv, 2.0 * s.beta, xs, ys);
         }
         const double mob[4] = {s.beta_inv + xs, s.beta_inv + ys, s.beta_inv - xs, s.beta_inv - ys};
         for (int k = 0; k < 4; k++) {

