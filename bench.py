@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="N > 1: weak = one seeded ensemble per rank; strong = one ensemble split across ranks (LPT)")
+    ap.add_argument("--profile-steps", type=int, default=0, metavar="S",
+                    help="profiler driver: build the workload and run S steps (no autotuning, no bench line)")
     ap.add_argument("--profile-kernel", type=int, default=0, metavar="K",
                     help="profiler driver: build the workload, stage it once, launch only the monomer pair kernel "
                          "K times (default chunk width, no autotuning, no steps) and exit; prints no bench line")
@@ -99,6 +101,32 @@ def profile_kernel(args):
     print(json.dumps({"profile_kernel": "k_rpy_aa_f2" if prec == _capi.PS_PREC_MIXED else "k_rpy_aa",
                       "workload": name, "launches": args.profile_kernel + 1, "ms_per_launch": ms.value,
                       "device_gb_in_use": (total - free) / 1e9}))
+    b.close()
+
+
+def profile_steps(args):
+    """A short, fixed step sequence for profiler captures of the step's kernels (launch
+    lists, the HBM-bound solver kernels): the workload at the default chunk width, S steps."""
+    import torch
+    from polystokes_brownian_b200 import _capi
+    from polystokes_brownian_b200.engine import Batch
+
+    torch.cuda.set_device(0)
+    systems, name = workload(args)
+    prec = _capi.PS_PREC_MIXED if args.precision == "mixed" else _capi.PS_PREC_FP64
+    solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
+    b = Batch(systems, precision=prec)
+    st = torch.cuda.current_stream()
+    ms = []
+    for _ in range(args.profile_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        b.step(rtol=args.rtol, maxit=50000, solver=solver)
+        e1.record(st)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"profile_steps": args.profile_steps, "workload": name, "precision": args.precision,
+                      "solver": args.solver, "ms_per_step": ms}))
     b.close()
 
 
@@ -518,16 +546,22 @@ def velocity_error(systems, args, precision=None):
     prec = _capi.PS_PREC_MIXED if precision == "mixed" else _capi.PS_PREC_FP64
     solver = _capi.PS_SOLVE_STRUCTURED if args.solver == "structured" else _capi.PS_SOLVE_MINRES
     out = []
-    for pr, rt in ((prec, args.rtol), (_capi.PS_PREC_FP64, 1e-10)):
+    runs = [(prec, args.rtol, 0), (_capi.PS_PREC_FP64, 1e-10, 0)]
+    if prec == _capi.PS_PREC_MIXED:
+        runs.append((prec, args.rtol, 1))      # one FP64 iterative-refinement sweep per solve
+    for pr, rt, rf in runs:
         b = Batch(sub, precision=pr)
         fb = torch.from_numpy(np.random.default_rng(1).normal(size=b.ntop)).cuda()
         wr = torch.from_numpy(np.random.default_rng(2).normal(size=b.nvel)).cuda()
-        b.step(fb=fb, wrfd=wr, rtol=rt, maxit=50000, solver=solver)
+        b.step(fb=fb, wrfd=wr, rtol=rt, maxit=50000, solver=solver, refine=rf)
         out.append(b.step_outputs()["up"].cpu().numpy())
         b.close()
     err = float(np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1]))
-    return {"rel_err_up": err, "replicas": len(sub), "against": "FP64 at rtol 1e-10, same state and injected noise",
-            "bound": 1e-6, "ok": err <= 1e-6}
+    res = {"rel_err_up": err, "replicas": len(sub), "against": "FP64 at rtol 1e-10, same state and injected noise",
+           "bound": 1e-6, "ok": err <= 1e-6}
+    if len(out) > 2:
+        res["rel_err_up_refined"] = float(np.linalg.norm(out[2] - out[1]) / np.linalg.norm(out[1]))
+    return res
 
 
 def time_steps(systems, precision, solver, rtol, steps, warmup=1):
@@ -721,6 +755,18 @@ def run_b200(args):
             e1.synchronize()
             extra["fp64_batched"] = {"value": beads * 2 / (e0.elapsed_time(e1) * 1e-3), "unit": METRIC,
                                      "ms_per_step": e0.elapsed_time(e1) / 2, "form": "FP64, batched, same solver"}
+            # the FP64 monomer pair kernel of this form against the measured FP64 FMA peak
+            ms64, pk64 = C.c_double(0), C.c_double(0)
+            u64 = torch.randn(bf.ntop, dtype=torch.float64, device="cuda")
+            _capi.check(L.ps_time_kernel(bf.h, 0, 10, _ptr(u64), C.byref(ms64), bf.stream), "ps_time_kernel")
+            _capi.check(L.ps_fma_peak(1, C.byref(pk64), bf.stream), "ps_fma_peak")
+            f64 = pair_flops(systems)
+            if f64 > 0 and ms64.value > 0:
+                ach = f64 / (ms64.value * 1e-3) / 1e12
+                extra["roofline_fp64"] = {"bound": "fp64", "kernel": "k_rpy_aa_d2", "achieved": ach, "peak": pk64.value,
+                                          "unit": "TFLOP/s", "frac": ach / pk64.value, "ms_per_launch": ms64.value,
+                                          "flop_per_launch": f64, "flop_unit": f"{FLOP_AA} per directed monomer pair",
+                                          "peak_source": "measured FP64 FMA throughput of this GPU (ps_fma_peak)"}
             bf.close()
         if args.plain_sample > 0:
             pf = plain_fp64(systems, args)
@@ -780,6 +826,8 @@ if __name__ == "__main__":
     a = parse()
     if a.profile_kernel:
         profile_kernel(a)
+    elif a.profile_steps:
+        profile_steps(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

@@ -136,6 +136,10 @@ typedef struct ps_step_inputs {
     int32_t sqrt_kmax;  /* Lanczos subspace cap of the noise (0: 40) */
     double sqrt_tol;    /* Lanczos relative tolerance of the noise (0: 1e-6) */
     int32_t solver;     /* PS_SOLVE_MINRES (default) or PS_SOLVE_STRUCTURED */
+    int32_t refine;     /* mixed precision only: FP64 iterative-refinement sweeps per solve (0: none).
+                           Each sweep forms the saddle residual b - A x with the FP64 operator and
+                           adds the mixed-precision solution of A d = r (same rtol) to x.  No
+                           reference counterpart (the reference solves in FP64 throughout). */
 } ps_step_inputs;
 
 typedef struct ps_step_result {

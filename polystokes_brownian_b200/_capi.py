@@ -62,7 +62,7 @@ class PsSqrtResult(C.Structure):
 class PsStepInputs(C.Structure):
     _fields_ = [("fb", C.c_void_p), ("wrfd", C.c_void_p), ("zlub", C.c_void_p),
                 ("rtol", C.c_double), ("maxit", C.c_int32), ("sqrt_kmax", C.c_int32), ("sqrt_tol", C.c_double),
-                ("solver", C.c_int32)]
+                ("solver", C.c_int32), ("refine", C.c_int32)]
 
 
 class PsStepResult(C.Structure):

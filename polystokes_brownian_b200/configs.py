@@ -159,6 +159,14 @@ def suspension(n: int = 1024, phi: float = 0.2, seed: int = 0, gap: float = 0.01
 def brush(nchain: int = 128, nper: int = 32, seed: int = 0, dt: float = 1e-4, pair_mode: int = 1) -> System:
     """1 colloid (a_c = 5) with nchain chains of nper beads grown outward from its surface.
 
+    Each chain starts just outside the colloid on a uniformly random direction (the first
+    beads of this dense brush cannot all touch the surface: up to 0.4 further out), and the
+    chains grow together, one layer of beads at a time, by steps of 2.2 beta whose direction
+    mixes the outward radial direction with a random one: every bead stays farther from the
+    centre than the previous one of its chain and is placed where it overlaps no bead
+    placed before (the outward weight grows on each rejected try).  At 128 chains the grafting is dense
+    (about 0.15 of surface per chain), so the chains are stretched, as in a brush.
+
     The chains are free (tether=0): the reference tethers with the chain's own
     FENE r0/Lmax (init.cpp:308-317, rhs.cpp:110-121), which is singular for a
     graft distance (1 + beta) larger than Lmax = 0.6."""
@@ -168,12 +176,32 @@ def brush(nchain: int = 128, nper: int = 32, seed: int = 0, dt: float = 1e-4, pa
     grid = _Grid(2 * beta)
     grid.add(np.zeros(3), 1.0)
     step = 2.2 * beta
-    anchors = [_unit(rng) for _ in range(nchain)]
-
-    def start(rng, c):
-        return anchors[c] * (1.0 + beta + 0.05), anchors[c]
-
-    xm = _chains(rng, nchain, nper, beta, step, None, start, grid)
+    # layer by layer: every chain's first bead, then every chain's second bead, ...
+    chains = np.zeros((nchain, nper, 3))
+    for c in range(nchain):
+        # graft direction uniform on the sphere; the first bead sits just off the surface, pushed
+        # out by up to 0.4 where the dense first layer has no room at contact
+        for attempt in range(4000):
+            p = _unit(rng) * (1.0 + beta + 0.05 + 0.4 * min(1.0, attempt / 2000.0) * rng.random())
+            if grid.clear(p, beta, 2.0 + 2 * beta):
+                break
+        grid.add(p, beta)
+        chains[c, 0] = p
+    for k in range(1, nper):
+        for c in range(nchain):
+            prev = chains[c, k - 1]
+            rad = prev / np.linalg.norm(prev)
+            for attempt in range(2000):
+                w = min(1.0, 0.35 + attempt / 400.0)
+                d = w * rad + (1.0 - w) * _unit(rng)
+                d /= np.linalg.norm(d)
+                q = prev + step * d
+                if np.linalg.norm(q) > np.linalg.norm(prev) and grid.clear(q, beta, 2.0 + 2 * beta):
+                    break
+            grid.add(q, beta)
+            chains[c, k] = q
+    beads = list(chains.reshape(-1, 3))
+    xm = np.array(beads).reshape(-1, 3)
     params = make_params(Nm=nchain * nper, Nc=1, Npoly=nchain, Nmono_per_chain=nper, beta=beta, kT=1.0,
                          kbond=30 * ac * ac, r0=step, Lmax=3.0 / ac, fene=1, dt=dt, mm_HI=1, chain_HI=0,
                          aa_mode=pair_mode, ab_mode=pair_mode)

@@ -69,7 +69,8 @@ static void free_engine(Engine &E)
                     E.d_pmp[7], E.d_pmp[8], E.d_pmp[9], E.d_pms[0], E.d_pms[1], E.d_pms[2], E.d_pms[3],
                     E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8], E.d_obs_acc, E.d_obs_prev,
                     E.d_obs_ring, E.d_obs_msd, E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.d_obs_msdn,
-                    E.d_sl_reps, E.d_sl_skip, E.d_slV, E.d_slT, E.d_sl_sc, E.d_sl_u, E.d_sl_y, E.d_sl_y2};
+                    E.d_sl_reps, E.d_sl_skip, E.d_slV, E.d_slT, E.d_sl_sc, E.d_sl_u, E.d_sl_y, E.d_sl_y2,
+                    E.d_cell_big, E.d_cell_nbig, E.d_cell_tmp, E.d_ref_r, E.d_ref_d};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -317,6 +318,9 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_cell_start, sizeof(int) * (cells + 1));
     TRY_ALLOC(E.d_cell_count, sizeof(int) * (cells + 1));
     TRY_ALLOC(E.d_cell_sorted, sizeof(int) * bead);
+    TRY_ALLOC(E.d_cell_big, sizeof(int) * (bead / 64 + 1));
+    TRY_ALLOC(E.d_cell_nbig, sizeof(int));
+    TRY_ALLOC(E.d_cell_tmp, sizeof(int) * bead);
     TRY_ALLOC(E.d_cellgeo, sizeof(double) * 20 * R);
     TRY_ALLOC(E.d_nbr_ptr, sizeof(int) * (bead + 1));
     TRY_ALLOC(E.d_lub_ptr, sizeof(int) * (bead + 1));

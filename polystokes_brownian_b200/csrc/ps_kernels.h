@@ -92,6 +92,7 @@ struct Engine {
 
     // cell list / pair lists
     int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_sorted = nullptr, *d_cell_count = nullptr;
+    int *d_cell_big = nullptr, *d_cell_nbig = nullptr, *d_cell_tmp = nullptr;   // cells of more than 64 members
     long ncell_cap = 0;
     double *d_cellgeo = nullptr;     // per replica: org[3], size[3], nc[3] (as double), periodic
     long *d_cell_offs = nullptr;     // per replica: first cell
@@ -153,6 +154,7 @@ struct Engine {
     double *d_vdn = nullptr, *d_vdc = nullptr, *d_vb = nullptr, *d_up = nullptr, *d_ud = nullptr;
     double *d_drift = nullptr, *d_sb = nullptr, *d_fext = nullptr, *d_fb = nullptr, *d_wr = nullptr;
     double *d_tmp_top = nullptr, *d_tmp_top2 = nullptr;
+    double *d_ref_r = nullptr, *d_ref_d = nullptr;   // iterative refinement: residual, correction (allocated on first use)
     uint64_t seed = 12345, step_counter = 0;
     uint64_t *d_rseed = nullptr, *d_rstep = nullptr;   // per-replica Philox key and step counter
 

@@ -240,7 +240,8 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
 // AA in FP64, two rows per thread.  A thread owns rows i and i + 64 of a 128-row
 // tile and sweeps 128-column tiles staged in shared memory as (x, y, z, chain)
 // and (u0, u1, u2, 0) double4 pairs, so each column's loads serve both rows.
-// Reciprocal square root: a single-precision seed refined by the second-order
+// Reciprocal square root: a single-precision seed (the float image taken with integer
+// operations) refined by the second-order
 // term of the binomial series (1 - e)^(-1/2) = 1 + e/2 + 3 e^2 / 8 + O(e^3),
 // e = 1 - a y0^2 (Householder's iteration of order 2 for f(y) = y^-2 - a): from
 // a seed accurate to 2^-22 the truncation is below 2^-64, so the result is
@@ -251,17 +252,32 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
 // (x - y) / r^2 = ri^3 (a + b ri^2), a = c0 - c2, b = c1 - c3, c = c2, d = c3.
 constexpr int AAD_THREADS = 64;
 
-__device__ __forceinline__ double rsqrt_seeded(double a)
+// Single-precision image of a positive double in [2^-126, 2^128) by exponent re-bias and
+// mantissa truncation (relative error below 2^-23), with integer operations only, so the
+// FP64 pipe is left to the arithmetic; seed_as_double widens a positive normal float exactly.
+__device__ __forceinline__ float trunc_to_float(double a)
 {
-    const double y = (double)rsqrtf((float)a);
+    const int hi = __double2hiint(a), lo = __double2loint(a);
+    return __int_as_float(((hi - (896 << 20)) << 3) | (int)((unsigned)lo >> 29));
+}
+__device__ __forceinline__ double seed_as_double(float f)
+{
+    const int b = __float_as_int(f);
+    return __hiloint2double((b >> 3) + (896 << 20), b << 29);
+}
+
+__device__ __forceinline__ double rsqrt_seeded(double a, float af)
+{
+    const double y = seed_as_double(rsqrtf(af));
     const double e = fma(-(a * y), y, 1.0);
     return fma(y * e, fma(0.375, e, 0.5), y);
 }
+__device__ __forceinline__ double rsqrt_seeded(double a) { return rsqrt_seeded(a, trunc_to_float(a)); }
 
 template <bool CHECK>
 __device__ __forceinline__ void aa_d2_cols(const double4 *__restrict__ sP, const double4 *__restrict__ sU, int jt,
                                            int nj, int iA, int iB, bool chain_hi, double4 PA, double4 PB, double ca,
-                                           double cb, double cc, double cd, double tb, double tb2, double n0,
+                                           double cb, double cc, double cd, double tb, float tb2f, double n0,
                                            double n1, double n2, double n3, double (&t)[6])
 {
 #pragma unroll 1
@@ -277,12 +293,14 @@ __device__ __forceinline__ void aa_d2_cols(const double4 *__restrict__ sP, const
             sA = (j == iA) || (chain_hi && PA.w == P.w);
             sB = (j == iB) || (chain_hi && PB.w == P.w);
         }
-        const double riA = sA ? 0.0 : rsqrt_seeded(r2A), riB = sB ? 0.0 : rsqrt_seeded(r2B);
+        const float fA = trunc_to_float(r2A), fB = trunc_to_float(r2B);
+        const double riA = sA ? 0.0 : rsqrt_seeded(r2A, fA), riB = sB ? 0.0 : rsqrt_seeded(r2B, fB);
         const double qA = riA * riA, qB = riB * riB;
         double yA = riA * fma(cd, qA, cc), yB = riB * fma(cd, qB, cc);
         double gA = (qA * riA) * fma(cb, qA, ca), gB = (qB * riB) * fma(cb, qB, ca);
-        // candidates for the near form; the reference's own distance decides within the band
-        const bool nA = !sA && r2A <= tb2 * (1.0 + 1e-10), nB = !sB && r2B <= tb2 * (1.0 + 1e-10);
+        // candidates for the near form (a single-precision test with a 1e-6 margin, off the FP64
+        // pipe); the reference's own distance decides within the band
+        const bool nA = !sA && fA <= tb2f, nB = !sB && fB <= tb2f;
         if (__any_sync(0xffffffffu, nA || nB)) {
             if (nA) {
                 const double r = ref_pair_dist(ax, ay, az);
@@ -332,7 +350,8 @@ k_rpy_aa_d2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
         c0 = 0.375; c1 = -2.0; c2 = 0.75; c3 = -0.5;
         n0 = -1.0; n1 = 0.375; n2 = 1.0; n3 = -0.28125;
     }
-    const double tb = 2.0 * sg.beta, ca = c0 - c2, cb = c1 - c3, tb2 = tb * tb;
+    const double tb = 2.0 * sg.beta, ca = c0 - c2, cb = c1 - c3;
+    const float tb2f = (float)(tb * tb * (1.0 + 1e-6));
     double a[6] = {0, 0, 0, 0, 0, 0};
     for (int jt = j0; jt < j1; jt += 128) {
         const int nj = min(128, j1 - jt);
@@ -350,9 +369,9 @@ k_rpy_aa_d2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
         // rows of this tile are [row0, row0 + 128): only overlapping column tiles hold self pairs
         const bool check = chain_hi || (jt < tl.row0 + 2 * AAD_THREADS && jt + nj > tl.row0);
         if (check)
-            aa_d2_cols<true>(sP, sU, jt, nj, iA, iB, chain_hi, PA, PB, ca, cb, c2, c3, tb, tb2, n0, n1, n2, n3, t);
+            aa_d2_cols<true>(sP, sU, jt, nj, iA, iB, chain_hi, PA, PB, ca, cb, c2, c3, tb, tb2f, n0, n1, n2, n3, t);
         else
-            aa_d2_cols<false>(sP, sU, jt, nj, iA, iB, chain_hi, PA, PB, ca, cb, c2, c3, tb, tb2, n0, n1, n2, n3, t);
+            aa_d2_cols<false>(sP, sU, jt, nj, iA, iB, chain_hi, PA, PB, ca, cb, c2, c3, tb, tb2f, n0, n1, n2, n3, t);
 #pragma unroll
         for (int q = 0; q < 6; q++) a[q] += t[q];
     }

@@ -235,15 +235,45 @@ __global__ void k_cell_fill(long ntot, const int *__restrict__ cell, const int *
     int slot = atomicAdd(&fillc[c], 1);
     sorted[start[c] + slot] = (int)b;
 }
-__global__ void k_cell_sort(long ncells, const int *__restrict__ start, int *__restrict__ sorted)
+// Each cell's members in ascending bead order (the fill above places them by atomic slots).
+// Cells of up to 64 members are sorted in place by one thread; larger cells (piled or
+// collapsed beads) are listed for k_cell_sort_big, which ranks their members in parallel.
+constexpr int CELL_SORT_SERIAL = 64;
+
+__global__ void k_cell_sort(long ncells, const int *__restrict__ start, int *__restrict__ sorted,
+                            int *__restrict__ big, int *__restrict__ nbig)
 {
     long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     int a = start[c], e = start[c + 1];
+    if (e - a > CELL_SORT_SERIAL) {
+        big[atomicAdd(nbig, 1)] = (int)c;
+        return;
+    }
     for (int i = a + 1; i < e; i++) {
         int v = sorted[i], j = i - 1;
         while (j >= a && sorted[j] > v) { sorted[j + 1] = sorted[j]; j--; }
         sorted[j + 1] = v;
+    }
+}
+
+// one block per listed cell at a time: every member's rank is the number of smaller members
+// (bead indices are distinct), written to tmp and copied back
+__global__ void k_cell_sort_big(const int *__restrict__ start, int *__restrict__ sorted, const int *__restrict__ big,
+                                const int *__restrict__ nbig, int *__restrict__ tmp)
+{
+    const int n = *nbig;
+    for (int q = blockIdx.x; q < n; q += gridDim.x) {
+        const int c = big[q], a = start[c], k = start[c + 1] - a;
+        for (int i = threadIdx.x; i < k; i += blockDim.x) {
+            const int v = sorted[a + i];
+            int rank = 0;
+            for (int j = 0; j < k; j++) rank += sorted[a + j] < v;
+            tmp[a + rank] = v;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < k; i += blockDim.x) sorted[a + i] = tmp[a + i];
+        __syncthreads();
     }
 }
 
@@ -259,7 +289,11 @@ int stage_cells(Engine &E, cudaStream_t st, const long *d_cell_off, long ncells)
     if (rc) return rc;
     PS_CK(cudaMemsetAsync(E.d_cell_count, 0, sizeof(int) * (ncells + 1), st));
     ::ps_launch_count++, k_cell_fill<<<nb, thr, 0, st>>>(E.ntot, E.d_cell, E.d_cell_start, E.d_cell_count, E.d_cell_sorted);
-    ::ps_launch_count++, k_cell_sort<<<(unsigned)((ncells + thr - 1) / thr), thr, 0, st>>>(ncells, E.d_cell_start, E.d_cell_sorted);
+    PS_CK(cudaMemsetAsync(E.d_cell_nbig, 0, sizeof(int), st));
+    ::ps_launch_count++, k_cell_sort<<<(unsigned)((ncells + thr - 1) / thr), thr, 0, st>>>(ncells, E.d_cell_start, E.d_cell_sorted,
+                                                                                        E.d_cell_big, E.d_cell_nbig);
+    ::ps_launch_count++, k_cell_sort_big<<<148, 256, 0, st>>>(E.d_cell_start, E.d_cell_sorted, E.d_cell_big, E.d_cell_nbig,
+                                                             E.d_cell_tmp);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

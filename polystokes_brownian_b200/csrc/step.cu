@@ -2,6 +2,7 @@
 // replica (run.cpp:70-162, slip_vel.cpp:19-79/205-349, drift.cpp:9-62,
 // traj.cpp:9-94, quat.cpp:7-54).  Compiled with --fmad=false so position
 // updates round like the reference's C++.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -272,6 +273,20 @@ static int stage(Engine &E, double *rhs, cudaStream_t st)
     return stage_schur(E, st);
 }
 
+// r = b - y
+__global__ void k_resid(long n, const double *__restrict__ b, const double *__restrict__ y, double *__restrict__ r)
+{
+    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) r[k] = b[k] - y[k];
+}
+
+// x += d
+__global__ void k_add(long n, const double *__restrict__ d, double *__restrict__ x)
+{
+    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) x[k] += d[k];
+}
+
 static int solve(Engine &E, const double *b, double *x, int warm, const ps_step_inputs *in, ps_step_result *res,
                  int slot, cudaStream_t st)
 {
@@ -279,12 +294,39 @@ static int solve(Engine &E, const double *b, double *x, int warm, const ps_step_
                      in ? in->solver : PS_SOLVE_MINRES};
     if (o.rtol <= 0) o.rtol = 1e-6;
     ps_ksp_result kr;
-    int reason = (o.method == PS_SOLVE_STRUCTURED) ? structured_solve(E, b, x, &o, &kr, st)
-                                                   : minres_solve(E, b, x, &o, &kr, st);
+    auto run = [&](const double *rhs, double *sol, ps_ksp_opts &oo) {
+        return (oo.method == PS_SOLVE_STRUCTURED) ? structured_solve(E, rhs, sol, &oo, &kr, st)
+                                                  : minres_solve(E, rhs, sol, &oo, &kr, st);
+    };
+    int reason = run(b, x, o);
     if (reason == PS_ERR_CUDA) return reason;
+    int its = kr.iters_max, worst = kr.reason;
+    // FP64 iterative refinement of the mixed-precision solve: the residual with the FP64
+    // operator, a mixed-precision correction, x += d
+    const int sweeps = (in && E.precision == PS_PREC_MIXED) ? in->refine : 0;
+    if (sweeps > 0) {
+        if (!E.d_ref_r) {
+            PS_CK(cudaMalloc(&E.d_ref_r, sizeof(double) * E.nvec));
+            PS_CK(cudaMalloc(&E.d_ref_d, sizeof(double) * E.nvec));
+        }
+        const int thr = 256;
+        const unsigned g = (unsigned)((E.nvec + thr - 1) / thr);
+        for (int k = 0; k < sweeps; k++) {
+            apply_operator(E, 0, x, E.d_ref_d, nullptr, false, st);
+            ::ps_launch_count++, k_resid<<<g, thr, 0, st>>>(E.nvec, b, E.d_ref_d, E.d_ref_r);
+            ps_ksp_opts oc = o;
+            oc.warm = 0;
+            reason = run(E.d_ref_r, E.d_ref_d, oc);
+            if (reason == PS_ERR_CUDA) return reason;
+            ::ps_launch_count++, k_add<<<g, thr, 0, st>>>(E.nvec, E.d_ref_d, x);
+            its += kr.iters_max;
+            worst = std::min(worst, kr.reason);
+        }
+        PS_CK(cudaGetLastError());
+    }
     if (res) {
-        res->iters[slot] = kr.iters_max;
-        if (kr.reason < res->reason) res->reason = kr.reason;
+        res->iters[slot] = its;
+        if (worst < res->reason) res->reason = worst;
     }
     return PS_OK;
 }

@@ -201,9 +201,10 @@ class Batch:
 
     def step(self, fb: torch.Tensor | None = None, wrfd: torch.Tensor | None = None, rtol: float = 1e-8,
              maxit: int = 10000, sqrt_kmax: int = 0, sqrt_tol: float = 0.0, solver: int = 0,
-             zlub: torch.Tensor | None = None):
+             zlub: torch.Tensor | None = None, refine: int = 0):
         inp = _capi.PsStepInputs(None if fb is None else fb.data_ptr(), None if wrfd is None else wrfd.data_ptr(),
-                                 None if zlub is None else zlub.data_ptr(), rtol, maxit, sqrt_kmax, sqrt_tol, solver)
+                                 None if zlub is None else zlub.data_ptr(), rtol, maxit, sqrt_kmax, sqrt_tol, solver,
+                                 refine)
         res = _capi.PsStepResult()
         check(lib().ps_step(self.h, C.byref(inp), C.byref(res), self.stream), "ps_step")
         return res
