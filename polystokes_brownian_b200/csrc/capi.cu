@@ -132,7 +132,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         s.nper = d.Nmono_per_chain > 0 ? d.Nmono_per_chain : 1;
         s.ss_off = -1;
         s.nch_aa = std::max(1, (d.Nm + ps::g_aa_chunk_cols - 1) / ps::g_aa_chunk_cols);
-        s.nch_bb = std::max(1, (d.Nc + BB_CHUNK_COLS - 1) / BB_CHUNK_COLS);
+        s.nch_bb = std::max(1, std::min(BB_MAX_CHUNKS, (d.Nc + BB_CHUNK_COLS - 1) / BB_CHUNK_COLS));
         if (d.aa_mode == PS_AA_RPY) {
             double b = d.beta, b2 = b * b;
             const double c[8] = {1.5, -b2, 0.75, 0.5 * b2, 1.0 / b, -0.1875 / b2, 1.0 / b, -0.28125 / b2};

@@ -478,8 +478,10 @@ __device__ void warp_tql(double *d, double *e, double *Z, int n)
             for (i = m - 1; i >= l; i--) {
                 const double ei = e[i], di = d[i], di1 = d[i + 1];
                 double f = s * ei, b = c * ei;
-                r = hypot(f, g);
-                const double rr = r;
+                // rotation from one reciprocal square root (the chain of dependent
+                // divisions is this loop's latency; f, g are O(|T|), far from overflow)
+                const double r2 = f * f + g * g, ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
+                const double rr = r2 * ri;
                 __syncwarp();               // every lane has read this rotation's d, e
                 if (rr == 0.0) {
                     if (lane == 0) { e[i + 1] = rr; d[i + 1] = di1 - p; e[m] = 0.0; }
@@ -487,7 +489,7 @@ __device__ void warp_tql(double *d, double *e, double *Z, int n)
                     brk = true;
                     break;
                 }
-                s = f / rr; c = g / rr;
+                s = f * ri; c = g * ri;
                 g = di1 - p;
                 r = (di - g) * s + 2.0 * c * b;
                 p = s * r;

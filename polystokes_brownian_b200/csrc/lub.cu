@@ -20,7 +20,6 @@
 // with B11 = Y11B eps.d, B12 = Y12B eps.d, B21 = -Y12B eps.d.
 // Compiled with --fmad=false (pair membership must round like the oracle).
 #include <cmath>
-#include <curand_kernel.h>
 #include <vector>
 #include "ps_internal.h"
 #include "ps_kernels.h"
@@ -92,78 +91,6 @@ __global__ void k_lub_apply(long ntot, const int *__restrict__ bead_offs, int R,
         for (int k = 0; k < 3; k++) diag[s.vel_off + tb + k] = dF[k];
         if (!mono) for (int k = 0; k < 3; k++) diag[s.vel_off + wb + k] = dT[k];
     }
-}
-
-// Brownian lubrication force, gathered per bead (no atomics: the sum over a
-// bead's pairs runs in ascending partner order, so the result is bit-exact and
-// independent of the rest of the batch).  Each canonical pair p = (lo < hi) with
-// index q in the canonical CSR list owns 12 normals z_p (monomer pairs use the
-// first 6): injected (z + 12 q) or drawn from the replica's Philox stream with
-// subsequence = q - (first canonical pair of the replica).  Both beads of a pair
-// compute w_p = R_p^{1/2} z_p identically and take their own rows;
-// rhs_bot += -sqrt(2 kT / dt) w.
-__global__ void k_lub_noise(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
-                            const double *__restrict__ x, const double *__restrict__ tab, int nrow,
-                            const int *__restrict__ sptr, const int *__restrict__ snbr,
-                            const int *__restrict__ cptr, const int *__restrict__ cnbr, const double *__restrict__ z,
-                            const uint64_t *__restrict__ rseed, const uint64_t *__restrict__ rstep,
-                            double *__restrict__ rhs)
-{
-    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= ntot) return;
-    int r = rep_of_b(bead_offs, R, b);
-    const Seg &s = segs[r];
-    int i = (int)(b - s.bead_off);
-    const bool mono = i < s.Nm;
-    const int nd = mono ? 6 : 12;
-    const double scale = -sqrt(2 * s.kT / s.dt);
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int t = sptr[b]; t < sptr[b + 1]; t++) {
-        long j = snbr[t];
-        const bool low = b < j;
-        long lo = low ? b : j, hi = low ? j : b;
-        // canonical index of (lo, hi): binary search in lo's ascending list
-        int qa = cptr[lo], qb = cptr[lo + 1];
-        const int qend = qb;
-        while (qb - qa > 1) {
-            int mid = (qa + qb) >> 1;
-            if (cnbr[mid] <= hi) qa = mid; else qb = mid;
-        }
-        if (qa >= qend || cnbr[qa] != hi) continue;    // not in the canonical list (lists disagree)
-        const long q = qa;
-        double zp[12];
-        if (z) {
-            for (int k = 0; k < 12; k++) zp[k] = z[12 * q + k];
-        } else {
-            curandStatePhilox4_32_10_t stt;
-            curand_init(rseed[r], (unsigned long long)(q - cptr[s.bead_off]), (3ull * rstep[r] + 2) * 4ull, &stt);
-            for (int k = 0; k < 12; k++) zp[k] = curand_normal_double(&stt);
-        }
-        double w[12];
-        if (mono) {
-            double d[3], lam[4], sq[4], Sm[36];
-            mono_pair_modes(s, x, tab, nrow, lo, hi, d, lam);
-            for (int k = 0; k < 4; k++) sq[k] = lam[k] > 0 ? sqrt(lam[k]) : 0.0;
-            mono_pair_matrix(d, sq, Sm, 6);
-            for (int a = 0; a < 6; a++) {
-                double v = 0.0;
-                for (int c = 0; c < 6; c++) v += Sm[a * 6 + c] * zp[c];
-                w[a] = v;
-            }
-        } else {
-            double Rm[144];
-            lub_pair_block(s, x, tab, nrow, lo, hi, mono, Rm);
-            small_sqrt_apply(Rm, nd, zp, w);
-        }
-        const int o = low ? 0 : 3;
-        for (int k = 0; k < 3; k++) acc[k] += w[o + k];
-        if (!mono) for (int k = 0; k < 3; k++) acc[3 + k] += w[6 + o + k];
-    }
-    int tb, wb;
-    vel_dofs(s, i, tb, wb);
-    long base = (long)s.vec_off + s.nm3nc11;
-    for (int k = 0; k < 3; k++) rhs[base + tb + k] += scale * acc[k];
-    if (!mono) for (int k = 0; k < 3; k++) rhs[base + wb + k] += scale * acc[3 + k];
 }
 
 __global__ void k_canon_count(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr, int *__restrict__ cnt)
@@ -271,16 +198,6 @@ int lub_diag(Engine &E, cudaStream_t st)
     ::ps_launch_count++, k_lub_apply<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
         E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_tmp_vel, 0,
         E.d_tmp_vel2, E.d_lub_diag);
-    PS_CK(cudaGetLastError());
-    return PS_OK;
-}
-
-int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st)
-{
-    int thr = 64;
-    ::ps_launch_count++, k_lub_noise<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr,
-        E.d_lubc_nbr, z, E.d_rseed, E.d_rstep, rhs);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

@@ -67,93 +67,56 @@ __device__ __forceinline__ void vel_dofs(const Seg &s, int i, int &t, int &w)
     else { int c = i - s.Nm; t = s.nm3 + 3 * c; w = s.nm3nc3 + 3 * c; }
 }
 
-// cyclic Jacobi eigen-decomposition of a symmetric n x n (n <= 12) matrix:
-// on return A holds the eigenvalues on its diagonal and Q the eigenvectors
-// (columns), A_in = Q diag(A) Q^T
-__device__ inline void jacobi_eig(double *A, int n, double *Q)
-{
-    for (int k = 0; k < n * n; k++) Q[k] = (k / n == k % n) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 40; sweep++) {
-        double off = 0, tot = 0;
-        for (int p = 0; p < n; p++) for (int q = 0; q < n; q++) { double v = A[p * n + q] * A[p * n + q]; tot += v; if (p != q) off += v; }
-        if (off <= 1e-30 * tot || off == 0.0) break;
-        for (int p = 0; p < n - 1; p++)
-            for (int q = p + 1; q < n; q++) {
-                double apq = A[p * n + q];
-                if (fabs(apq) < 1e-300) continue;
-                double theta = (A[q * n + q] - A[p * n + p]) / (2 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-                double c = 1 / sqrt(t * t + 1), sn = t * c;
-                for (int k = 0; k < n; k++) {
-                    double akp = A[k * n + p], akq = A[k * n + q];
-                    A[k * n + p] = c * akp - sn * akq; A[k * n + q] = sn * akp + c * akq;
-                }
-                for (int k = 0; k < n; k++) {
-                    double apk = A[p * n + k], aqk = A[q * n + k];
-                    A[p * n + k] = c * apk - sn * aqk; A[q * n + k] = sn * apk + c * aqk;
-                    double qkp = Q[k * n + p], qkq = Q[k * n + q];
-                    Q[k * n + p] = c * qkp - sn * qkq; Q[k * n + q] = sn * qkp + c * qkq;
-                }
-            }
-    }
-}
-
-// out = A^{1/2} z for a symmetric n x n (n <= 12) A (destroyed), negative
-// eigenvalues floored at 0
-__device__ inline void small_sqrt_apply(double *A, int n, const double *z, double *out)
-{
-    double Q[144];
-    jacobi_eig(A, n, Q);
-    double t[12];
-    for (int jj = 0; jj < n; jj++) {
-        double acc = 0;
-        for (int ii = 0; ii < n; ii++) acc += Q[ii * n + jj] * z[ii];
-        double lam = A[jj * n + jj];
-        t[jj] = (lam > 0 ? sqrt(lam) : 0.0) * acc;
-    }
-    for (int ii = 0; ii < n; ii++) {
-        double acc = 0;
-        for (int jj = 0; jj < n; jj++) acc += Q[ii * n + jj] * t[jj];
-        out[ii] = acc;
-    }
-}
-
 // 12x12 (or 6x6) pair block R_p in the canonical orientation d = (x_hi - x_lo)/r
-__device__ inline void lub_pair_block(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab, int nrow,
-                               long lo, long hi, bool mono, double *Rm)
+// separation direction d and the ten table scalars of the pair; a = bead radius
+__device__ inline void lub_pair_geom(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab,
+                                     int nrow, long lo, long hi, double a, double d[3], double f[10])
 {
-    const double a = mono ? s.beta : 1.0, sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
     double dx = x[3 * hi] - x[3 * lo], dy = x[3 * hi + 1] - x[3 * lo + 1], dz = x[3 * hi + 2] - x[3 * lo + 2];
     mimg_l(s, dx, dy, dz);
     double rr = sqrt(dx * dx + dy * dy + dz * dz);
-    double d[3] = {dx / rr, dy / rr, dz / rr};
-    double f[10];
+    d[0] = dx / rr; d[1] = dy / rr; d[2] = dz / rr;
     lub_scalars(tab, nrow, rr / a, f);
+}
+
+// the entries of the pair block that depend on the component pair (p, qq); the
+// block is zero elsewhere (nd = 6 for monomer pairs: A blocks only)
+__device__ __forceinline__ void lub_pair_entries(const double d[3], const double f[10], double a, bool mono, int p,
+                                                 int qq, double *Rm)
+{
+    const double sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
+    const int nd = mono ? 6 : 12;
+    {
+        double dd = d[p] * d[qq], id = (p == qq) - dd;
+        double a11 = sa * (f[0] * dd + f[2] * id), a12 = sa * (f[1] * dd + f[3] * id);
+        Rm[(0 + p) * nd + 0 + qq] = a11; Rm[(3 + p) * nd + 3 + qq] = a11;
+        Rm[(0 + p) * nd + 3 + qq] = a12; Rm[(3 + p) * nd + 0 + qq] = a12;
+    }
+    if (mono) return;
+    int k3 = 3 - p - qq;
+    double ed = 0.0;
+    if (p != qq && k3 >= 0 && k3 < 3) ed = (((p - qq + 3) % 3) == 2 ? 1.0 : -1.0) * d[k3];
+    double b11 = sb * f[4] * ed, b12 = sb * f[5] * ed, b21 = -b12, b22 = -b11;
+    Rm[(6 + p) * nd + 0 + qq] = b11; Rm[(6 + p) * nd + 3 + qq] = b12;
+    Rm[(9 + p) * nd + 0 + qq] = b21; Rm[(9 + p) * nd + 3 + qq] = b22;
+    Rm[(0 + qq) * nd + 6 + p] = b11; Rm[(3 + qq) * nd + 6 + p] = b12;
+    Rm[(0 + qq) * nd + 9 + p] = b21; Rm[(3 + qq) * nd + 9 + p] = b22;
+    double dd = d[p] * d[qq], id = (p == qq) - dd;
+    double c11 = sc * (f[6] * dd + f[8] * id), c12 = sc * (f[7] * dd + f[9] * id);
+    Rm[(6 + p) * nd + 6 + qq] = c11; Rm[(9 + p) * nd + 9 + qq] = c11;
+    Rm[(6 + p) * nd + 9 + qq] = c12; Rm[(9 + p) * nd + 6 + qq] = c12;
+}
+
+__device__ inline void lub_pair_block(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab, int nrow,
+                               long lo, long hi, bool mono, double *Rm)
+{
+    const double a = mono ? s.beta : 1.0;
+    double d[3], f[10];
+    lub_pair_geom(s, x, tab, nrow, lo, hi, a, d, f);
     const int nd = mono ? 6 : 12;
     for (int k = 0; k < nd * nd; k++) Rm[k] = 0.0;
     for (int p = 0; p < 3; p++)
-        for (int qq = 0; qq < 3; qq++) {
-            double dd = d[p] * d[qq], id = (p == qq) - dd;
-            double a11 = sa * (f[0] * dd + f[2] * id), a12 = sa * (f[1] * dd + f[3] * id);
-            Rm[(0 + p) * nd + 0 + qq] = a11; Rm[(3 + p) * nd + 3 + qq] = a11;
-            Rm[(0 + p) * nd + 3 + qq] = a12; Rm[(3 + p) * nd + 0 + qq] = a12;
-        }
-    if (mono) return;
-    for (int p = 0; p < 3; p++)
-        for (int qq = 0; qq < 3; qq++) {
-            int k3 = 3 - p - qq;
-            double ed = 0.0;
-            if (p != qq && k3 >= 0 && k3 < 3) ed = (((p - qq + 3) % 3) == 2 ? 1.0 : -1.0) * d[k3];
-            double b11 = sb * f[4] * ed, b12 = sb * f[5] * ed, b21 = -b12, b22 = -b11;
-            Rm[(6 + p) * nd + 0 + qq] = b11; Rm[(6 + p) * nd + 3 + qq] = b12;
-            Rm[(9 + p) * nd + 0 + qq] = b21; Rm[(9 + p) * nd + 3 + qq] = b22;
-            Rm[(0 + qq) * nd + 6 + p] = b11; Rm[(3 + qq) * nd + 6 + p] = b12;
-            Rm[(0 + qq) * nd + 9 + p] = b21; Rm[(3 + qq) * nd + 9 + p] = b22;
-            double dd = d[p] * d[qq], id = (p == qq) - dd;
-            double c11 = sc * (f[6] * dd + f[8] * id), c12 = sc * (f[7] * dd + f[9] * id);
-            Rm[(6 + p) * nd + 6 + qq] = c11; Rm[(9 + p) * nd + 9 + qq] = c11;
-            Rm[(6 + p) * nd + 9 + qq] = c12; Rm[(9 + p) * nd + 6 + qq] = c12;
-        }
+        for (int qq = 0; qq < 3; qq++) lub_pair_entries(d, f, a, mono, p, qq, Rm);
 }
 
 // Monomer pair block in closed form.  K = [[A11, A12], [A12, A11]] with

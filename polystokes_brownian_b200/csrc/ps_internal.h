@@ -52,7 +52,8 @@ struct Seg {
 
 // Column chunk widths of the far-field pair kernels.
 constexpr int AA_CHUNK_COLS = 256;        // default; ps_autotune may pick another, process-wide
-constexpr int BB_CHUNK_COLS = 64;
+constexpr int BB_CHUNK_COLS = 32;        // colloid columns per chunk, for up to BB_MAX_CHUNKS chunks
+constexpr int BB_MAX_CHUNKS = 64;
 
 // Row tile of the far-field pair kernels.
 struct Tile { int rep; int row0; int nrow; int mtile; };
@@ -209,57 +210,65 @@ __device__ __forceinline__ void mm_flat(const T e[3], T xm, T ym, T zm, T Mm[25]
 //   lo row: U += A F - B T + G S ; W += B F + C T + H S ; E += -G^T F + H^T T + Mm S
 //   hi row: U += A F - B T - G S ; W += B F + C T + H S ; E +=  G^T F + H^T T + Mm^T S
 // (derived from the dense block placement, mob.cpp:1042-1143)
+//
+// The blocks are applied in contracted form, never built.  With the stresslet
+// 5-vector S expanded to the symmetric traceless matrix S^ (S^00 = S0,
+// S^11 = S4, S^22 = -S0 - S4, S^01 = S1, S^02 = S2, S^12 = S3), v = S^ e,
+// s = e.v, c = T x e and flat(Z) = [Z00 - Z22, 2 Z01, 2 Z02, 2 Z12, Z11 - Z22]
+// (the flattening of mob.cpp:221-227, under which isotropic parts vanish):
+//   G S   = 2 yg v - (xg + 2 yg) s e          H S   = 2 yh e x v
+//   G^T F = flat(yg (e F^T + F e^T) - (xg + 2 yg)(e.F) e e^T)
+//   H^T T = flat(yh (e c^T + c e^T))
+//   Mm S  = flat((1.5 xm - 2 ym + 0.5 zm) s e e^T + (ym - zm)(e v^T + v e^T) + zm S^)
+// Mm is symmetric, so both rows use Mm S.  About 230 FLOP per directed pair
+// (FMA counted as 2), against 242 for the 11 x 11 block-vector product alone
+// when the block is built first.
 template <class T>
 __device__ __forceinline__ void bb_apply(const T e[3], T r, T rinv, bool is_lo, const T in[11], T out[11])
 {
     (void)r;
-    T ri2 = rinv * rinv, ri3 = ri2 * rinv, ri4 = ri3 * rinv, ri5 = ri4 * rinv;
-    T xa = T(1.5) * rinv - ri3, ya = T(0.75) * rinv + T(0.5) * ri3;
-    T yb = T(-0.75) * ri2;
-    T xg = T(2.25) * ri2 - T(3.6) * ri4, yg = T(1.2) * ri4;
-    T xc = T(0.75) * ri3, yc = T(-0.375) * ri3;
-    T yh = T(-1.125) * ri3;
-    T xm = T(-4.5) * ri3 + T(10.8) * ri5, ym = T(2.25) * ri3 - T(7.2) * ri5, zm = T(1.8) * ri5;
-    const T *F = in, *Tq = in + 3, *S = in + 6;
-    T eF = e[0] * F[0] + e[1] * F[1] + e[2] * F[2];
-    T eT = e[0] * Tq[0] + e[1] * Tq[1] + e[2] * Tq[2];
-    // A F
-    T AF[3], CT[3], BF[3], BT[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        AF[a] = ya * F[a] + (xa - ya) * eF * e[a];
-        // reference C: diag x ee + y(1-ee), off-diagonal (x + y) ee (mob.cpp:249-254)
-        CT[a] = (xc + yc) * eT * e[a] + yc * Tq[a] - T(2) * yc * e[a] * e[a] * Tq[a];
-    }
-    // B v = yb (v x e)
-    BF[0] = yb * (F[1] * e[2] - F[2] * e[1]);
-    BF[1] = yb * (F[2] * e[0] - F[0] * e[2]);
-    BF[2] = yb * (F[0] * e[1] - F[1] * e[0]);
-    BT[0] = yb * (Tq[1] * e[2] - Tq[2] * e[1]);
-    BT[1] = yb * (Tq[2] * e[0] - Tq[0] * e[2]);
-    BT[2] = yb * (Tq[0] * e[1] - Tq[1] * e[0]);
-    T G[15], H[15], Mm[25];
-    gt_flat(e, xg, yg, G);
-    ht_flat(e, yh, H);
-    mm_flat(e, xm, ym, zm, Mm);
-    T sg = is_lo ? T(1) : T(-1);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        T gs = 0, hs = 0;
-#pragma unroll
-        for (int q = 0; q < 5; q++) { gs += G[a * 5 + q] * S[q]; hs += H[a * 5 + q] * S[q]; }
-        out[a] += AF[a] - BT[a] + sg * gs;
-        out[3 + a] += BF[a] + CT[a] + hs;
-    }
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-        T gf = 0, ht = 0, ms = 0;
-#pragma unroll
-        for (int a = 0; a < 3; a++) { gf += G[a * 5 + q] * F[a]; ht += H[a * 5 + q] * Tq[a]; }
-#pragma unroll
-        for (int p = 0; p < 5; p++) ms += (is_lo ? Mm[q * 5 + p] : Mm[p * 5 + q]) * S[p];
-        out[6 + q] += -sg * gf + ht + ms;
-    }
+    const T ri2 = rinv * rinv, ri3 = ri2 * rinv, ri4 = ri2 * ri2, ri5 = ri4 * rinv;
+    const T xa = T(1.5) * rinv - ri3, ya = T(0.75) * rinv + T(0.5) * ri3;
+    const T yb = T(-0.75) * ri2;
+    const T xg = T(2.25) * ri2 - T(3.6) * ri4, yg = T(1.2) * ri4;
+    const T xc = T(0.75) * ri3, yc = T(-0.375) * ri3;
+    const T yh = T(-1.125) * ri3;
+    const T xm = T(-4.5) * ri3 + T(10.8) * ri5, ym = T(2.25) * ri3 - T(7.2) * ri5, zm = T(1.8) * ri5;
+    const T sg = is_lo ? T(1) : T(-1);
+    const T F0 = in[0], F1 = in[1], F2 = in[2], T0 = in[3], T1 = in[4], T2 = in[5];
+    const T S0 = in[6], S1 = in[7], S2 = in[8], S3 = in[9], S4 = in[10], S22 = -S0 - S4;
+    const T e0 = e[0], e1 = e[1], e2 = e[2];
+    const T v0 = S0 * e0 + S1 * e1 + S2 * e2;
+    const T v1 = S1 * e0 + S4 * e1 + S3 * e2;
+    const T v2 = S2 * e0 + S3 * e1 + S22 * e2;
+    const T s = e0 * v0 + e1 * v1 + e2 * v2;
+    const T eF = e0 * F0 + e1 * F1 + e2 * F2;
+    const T eT = e0 * T0 + e1 * T1 + e2 * T2;
+    const T c0 = T1 * e2 - T2 * e1, c1 = T2 * e0 - T0 * e2, c2 = T0 * e1 - T1 * e0;   // T x e
+    const T kg = xg + T(2) * yg;
+    // U row: A F - B T +- G S, with B v = yb (v x e)
+    const T cu = (xa - ya) * eF - sg * kg * s, g2 = sg * T(2) * yg;
+    out[0] += ya * F0 - yb * c0 + g2 * v0 + cu * e0;
+    out[1] += ya * F1 - yb * c1 + g2 * v1 + cu * e1;
+    out[2] += ya * F2 - yb * c2 + g2 * v2 + cu * e2;
+    // W row: B F + C T + H S; C as the reference writes it: diagonal x ee + y (1 - ee),
+    // off-diagonal (x + y) ee (mob.cpp:249-254)
+    const T cw = (xc + yc) * eT, h2 = T(2) * yh;
+    out[3] += yb * (F1 * e2 - F2 * e1) + cw * e0 + yc * T0 - T(2) * yc * e0 * e0 * T0 + h2 * (e1 * v2 - e2 * v1);
+    out[4] += yb * (F2 * e0 - F0 * e2) + cw * e1 + yc * T1 - T(2) * yc * e1 * e1 * T1 + h2 * (e2 * v0 - e0 * v2);
+    out[5] += yb * (F0 * e1 - F1 * e0) + cw * e2 + yc * T2 - T(2) * yc * e2 * e2 * T2 + h2 * (e0 * v1 - e1 * v0);
+    // E row: flat(Z), Z = gam e e^T + e w^T + w e^T + zm S^
+    const T gam = (T(1.5) * xm - T(2) * ym + T(0.5) * zm) * s + sg * kg * eF;
+    const T ymz = ym - zm, sy = sg * yg;
+    const T w0 = yh * c0 + ymz * v0 - sy * F0;
+    const T w1 = yh * c1 + ymz * v1 - sy * F1;
+    const T w2 = yh * c2 + ymz * v2 - sy * F2;
+    const T z22 = gam * e2 * e2 + T(2) * e2 * w2 + zm * S22;
+    out[6] += gam * e0 * e0 + T(2) * e0 * w0 + zm * S0 - z22;
+    out[7] += T(2) * (gam * e0 * e1 + e0 * w1 + e1 * w0 + zm * S1);
+    out[8] += T(2) * (gam * e0 * e2 + e0 * w2 + e2 * w0 + zm * S2);
+    out[9] += T(2) * (gam * e1 * e2 + e1 * w2 + e2 * w1 + zm * S3);
+    out[10] += gam * e1 * e1 + T(2) * e1 * w1 + zm * S4 - z22;
 }
 
 // Monomer-colloid translation scalars (x along e, y across) and, for the

@@ -523,8 +523,8 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     P4 pi = pos[sg.bead_off + Nm + (active ? i : tl.row0)];
     float4 li = make_float4(0.f, 0.f, 0.f, 0.f);
     if constexpr (F32) li = plo[sg.bead_off + Nm + (active ? i : tl.row0)];
-    Acc<T> acc[11];
-    for (int q = 0; q < 11; q++) acc[q].zero();
+    T out[11];   // accumulated over the chunk's column tiles in column order
+    for (int q = 0; q < 11; q++) out[q] = T(0);
     for (int jt = j0; jt < j1; jt += CT) {
         int nj = min(CT, j1 - jt);
         __syncthreads();
@@ -538,8 +538,6 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             if constexpr (F32) sl[threadIdx.x] = plo[sg.bead_off + Nm + jt + threadIdx.x];
         }
         __syncthreads();
-        T out[11];
-        for (int q = 0; q < 11; q++) out[q] = T(0);
         for (int k = 0; k < nj; k++) {
             int j = jt + k;
             if (j == i) continue;
@@ -556,15 +554,14 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             T e[3] = {dx * rinv, dy * rinv, dz * rinv};
             bb_apply<T>(e, r2 * rinv, rinv, lo, su + 11 * k, out);
         }
-        for (int q = 0; q < 11; q++) acc[q].add(out[q]);
     }
     if (active) {
         double *o = part + (long)c * part_stride + sg.top_off;
         for (int a = 0; a < 3; a++) {
-            o[sg.nm3 + 3 * i + a] = (double)acc[a].get();
-            o[sg.nm3 + sg.nc3 + 3 * i + a] = (double)acc[3 + a].get();
+            o[sg.nm3 + 3 * i + a] = (double)out[a];
+            o[sg.nm3 + sg.nc3 + 3 * i + a] = (double)out[3 + a];
         }
-        for (int q = 0; q < 5; q++) o[sg.nm3nc6 + 5 * i + q] = (double)acc[6 + q].get();
+        for (int q = 0; q < 5; q++) o[sg.nm3nc6 + 5 * i + q] = (double)out[6 + q];
     }
 }
 
@@ -582,9 +579,12 @@ __device__ __forceinline__ int find_rep(const int *__restrict__ offs, int R, lon
     return lo;
 }
 
-// One block per entry of the replica-aligned block table of the output layout
-// (saddle vectors for mode 0, mobility vectors for mode 1), so the replica is
-// known without a search and a converged replica's blocks leave at once.
+// One block column per entry of the replica-aligned block table of the output
+// layout (saddle vectors for mode 0, mobility vectors for mode 1), so the
+// replica is known without a search and a converged replica's blocks leave at
+// once; blockIdx.y splits an entry's span so that each thread sums one output
+// (a single large replica otherwise leaves most SMs idle while every thread
+// walks its chunk partials four times over).
 __global__ void k_combine(const Seg *__restrict__ segs, RedTable T, int mode, const double *__restrict__ x,
                           const double *__restrict__ scale, const double *__restrict__ partAA, int nchAA,
                           const double *__restrict__ partAB, const double *__restrict__ partBB, int nchBB,
@@ -598,15 +598,18 @@ __global__ void k_combine(const Seg *__restrict__ segs, RedTable T, int mode, co
     const Seg &sg = segs[r];
     const int xo = mode == 0 ? sg.vec_off : sg.top_off;
     const double s = scale ? scale[r] : 1.0;
-    for (int e = threadIdx.x; e < B.len; e += blockDim.x) {
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < B.len; e += blockDim.x * gridDim.y) {
         const long k = (long)B.start + e;
         const int i = (int)(k - xo);
         double v = 0.0;
         if (i < sg.nm3nc11) {
             if (i < sg.nm3) {
                 v = sg.beta_inv * x[xo + i];
-                if (sg.mm_HI)
-                    for (int c = 0; c < (nchAA ? sg.nch_aa : 0); c++) v += partAA[(long)c * part_stride + sg.top_off + i];
+                if (sg.mm_HI) {
+                    const int nc = nchAA ? sg.nch_aa : 0;
+#pragma unroll 8
+                    for (int c = 0; c < nc; c++) v += partAA[(long)c * part_stride + sg.top_off + i];
+                }
                 if (sg.Nc > 0) v += partAB[sg.top_off + i];
             } else {
                 int j = i - sg.nm3;          // colloid-local DOF in [0, nc11)
@@ -622,8 +625,10 @@ __global__ void k_combine(const Seg *__restrict__ segs, RedTable T, int mode, co
                     if (p == 4) self += 0.9 * x[sb + 0];
                 }
                 v = self;
-                if (sg.Nc >= 2)
+                if (sg.Nc >= 2) {
+#pragma unroll 8
                     for (int c = 0; c < sg.nch_bb; c++) v += partBB[(long)c * part_stride + sg.top_off + i];
+                }
                 if (sg.Nm > 0)
                     for (int t = 0; t < sg.n_mtiles; t++) v += partBA[((long)sg.ba_off + (long)t * sg.Nc + cidx) * 11 + q];
                 if (sg.shell_schur) {
@@ -690,7 +695,7 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
         lub_y = E.d_luby;
     }
     const RedTable &T = mode == 0 ? E.red : E.red_top;
-    ::ps_launch_count++, k_combine<<<(unsigned)T.nblk, RB_THREADS, 0, st>>>(
+    ::ps_launch_count++, k_combine<<<dim3((unsigned)T.nblk, RB_EPT), RB_THREADS, 0, st>>>(
         E.d_segs, T, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
         E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
 }

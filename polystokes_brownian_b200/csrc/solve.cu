@@ -21,6 +21,7 @@
 // because M is not positive definite (the reference's own monomer pair scalars
 // make it indefinite) take the result as the warm start of a MINRES polish.
 #include <cmath>
+#include <curand_kernel.h>
 #include <vector>
 #include "ps_internal.h"
 #include "ps_kernels.h"
@@ -355,138 +356,271 @@ __device__ void pair_mobility(const Seg &s, const double *__restrict__ x, const 
         }
 }
 
+// Parallel-ordered Jacobi eigen-decomposition of a symmetric 12 x 12 matrix
+// in shared memory by one warp: each sweep is 11 rounds of 6 disjoint
+// rotations (the circle schedule: (r, 11) and (r + i, r - i) mod 11, i = 1..5),
+// whose angles depend only on their own 2 x 2 blocks, so a round equals its six
+// rotations applied one after another; each rotation is the one of jacobi_eig
+// (same angle, same stopping test at the start of a sweep).  On return A holds
+// the eigenvalues on its diagonal and Q the eigenvectors (columns).
+struct PsWarpSmem {
+    double K[144], Q[144], S[144], M[144];
+    double cs[12];
+    int pq[12];
+};
+
+__device__ void warp_jacobi12(double *A, double *Q, double *cs, int *pq, int lane)
+{
+    for (int t = lane; t < 144; t += 32) Q[t] = (t / 12 == t % 12) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int sweep = 0; sweep < 40; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (int t = lane; t < 144; t += 32) {
+            const double v = A[t] * A[t];
+            tot += v;
+            if (t / 12 != t % 12) off += v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if (off <= 1e-30 * tot || off == 0.0) break;
+        for (int rnd = 0; rnd < 11; rnd++) {
+            if (lane < 6) {
+                int p = lane == 0 ? rnd : (rnd + lane) % 11, q = lane == 0 ? 11 : (rnd - lane + 11) % 11;
+                if (p > q) { const int t = p; p = q; q = t; }
+                const double apq = A[p * 12 + q];
+                double c = 1.0, sn = 0.0;
+                if (fabs(apq) >= 1e-300) {
+                    const double theta = (A[q * 12 + q] - A[p * 12 + p]) / (2 * apq);
+                    const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+                    c = 1 / sqrt(t * t + 1);
+                    sn = t * c;
+                }
+                cs[lane] = c; cs[6 + lane] = sn; pq[lane] = p; pq[6 + lane] = q;
+            }
+            __syncwarp();
+            for (int t = lane; t < 72; t += 32) {          // A <- A J (columns p, q of every row)
+                const int i = t / 12, k = t % 12, p = pq[i], q = pq[6 + i];
+                const double c = cs[i], sn = cs[6 + i], akp = A[k * 12 + p], akq = A[k * 12 + q];
+                A[k * 12 + p] = c * akp - sn * akq;
+                A[k * 12 + q] = sn * akp + c * akq;
+            }
+            __syncwarp();
+            for (int t = lane; t < 72; t += 32) {          // A <- J^T A (rows p, q), Q <- Q J
+                const int i = t / 12, k = t % 12, p = pq[i], q = pq[6 + i];
+                const double c = cs[i], sn = cs[6 + i];
+                const double apk = A[p * 12 + k], aqk = A[q * 12 + k];
+                A[p * 12 + k] = c * apk - sn * aqk;
+                A[q * 12 + k] = sn * apk + c * aqk;
+                const double qkp = Q[k * 12 + p], qkq = Q[k * 12 + q];
+                Q[k * 12 + p] = c * qkp - sn * qkq;
+                Q[k * 12 + q] = sn * qkp + c * qkq;
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+}
+
+// One colloid pair (lo, hi) by one warp: K = R_lub pair block, S = K^{1/2}
+// (eigenvalues floored at 0), M = two-body FT far-field mobility (symmetrised),
+// P = (I + S M S)^{-1} by Cholesky, identity if not positive definite.  The
+// arithmetic per entry is that of the serial form: every sum runs over k in
+// ascending order.
+__device__ void ps_setup_colloid_pair(const Seg &s, long lo, long hi, const double *__restrict__ x,
+                                      const double *__restrict__ tab, int nrow, double *__restrict__ So,
+                                      double *__restrict__ Po, PsWarpSmem &w, int lane)
+{
+    double *K = w.K, *Q = w.Q, *S = w.S, *M = w.M;
+    for (int t = lane; t < 144; t += 32) { K[t] = 0.0; M[t] = 0.0; }
+    __syncwarp();
+    {
+        double d[3], f[10];
+        lub_pair_geom(s, x, tab, nrow, lo, hi, 1.0, d, f);
+        if (lane < 9) lub_pair_entries(d, f, 1.0, false, lane / 3, lane % 3, K);
+    }
+    if (lane < 12) {
+        // the partner's (F, T) column -> this bead's (U, W) rows, e = (x_lo - x_hi)/r as in the BB kernel
+        const double dx = x[3 * lo] - x[3 * hi], dy = x[3 * lo + 1] - x[3 * hi + 1], dz = x[3 * lo + 2] - x[3 * hi + 2];
+        const double r2 = dx * dx + dy * dy + dz * dz, rinv = 1.0 / sqrt(r2), r = r2 * rinv;
+        const double e[3] = {dx * rinv, dy * rinv, dz * rinv};
+        M[lane * 12 + lane] = lane < 6 ? 1.0 : 0.75;
+        const bool is_lo = lane < 6;
+        const int c = lane % 6;
+        const int rowU = is_lo ? 0 : 3, rowW = is_lo ? 6 : 9, colF = is_lo ? 3 : 0, colT = is_lo ? 9 : 6;
+        double in[11], out[11];
+        for (int k = 0; k < 11; k++) { in[k] = 0.0; out[k] = 0.0; }
+        in[c] = 1.0;
+        bb_apply<double>(e, r, rinv, is_lo, in, out);
+        const int col = c < 3 ? colF + c : colT + (c - 3);
+        for (int a = 0; a < 3; a++) { M[(rowU + a) * 12 + col] = out[a]; M[(rowW + a) * 12 + col] = out[3 + a]; }
+    }
+    __syncwarp();
+    for (int t = lane; t < 144; t += 32) {
+        const int a = t / 12, c = t % 12;
+        if (c > a) {
+            const double v = 0.5 * (M[a * 12 + c] + M[c * 12 + a]);
+            M[a * 12 + c] = v; M[c * 12 + a] = v;
+        }
+    }
+    warp_jacobi12(K, Q, w.cs, w.pq, lane);
+    for (int t = lane; t < 144; t += 32) {
+        const int a = t / 12, c = t % 12;
+        double v = 0.0;
+        for (int k = 0; k < 12; k++) {
+            const double lam = K[k * 12 + k];
+            v += Q[a * 12 + k] * (lam > 0 ? sqrt(lam) : 0.0) * Q[c * 12 + k];
+        }
+        S[t] = v;
+    }
+    __syncwarp();
+    for (int t = lane; t < 144; t += 32) {          // K <- M S
+        const int a = t / 12, c = t % 12;
+        double v = 0.0;
+        for (int k = 0; k < 12; k++) v += M[a * 12 + k] * S[k * 12 + c];
+        K[t] = v;
+    }
+    __syncwarp();
+    for (int t = lane; t < 144; t += 32) {          // Q <- I + S M S
+        const int a = t / 12, c = t % 12;
+        double v = (a == c) ? 1.0 : 0.0;
+        for (int k = 0; k < 12; k++) v += S[a * 12 + k] * K[k * 12 + c];
+        Q[t] = v;
+    }
+    __syncwarp();
+    bool ok = true;
+    for (int j = 0; j < 12; j++) {                  // Cholesky Q = C C^T in place (lower)
+        double dj = Q[j * 12 + j];
+        for (int k = 0; k < j; k++) dj -= Q[j * 12 + k] * Q[j * 12 + k];
+        if (!(dj > 0)) { ok = false; break; }
+        dj = sqrt(dj);
+        const int i = j + 1 + lane;
+        double v = 0.0;
+        if (i < 12) {
+            v = Q[i * 12 + j];
+            for (int k = 0; k < j; k++) v -= Q[i * 12 + k] * Q[j * 12 + k];
+        }
+        __syncwarp();
+        if (lane == 0) Q[j * 12 + j] = dj;
+        if (i < 12) Q[i * 12 + j] = v / dj;
+        __syncwarp();
+    }
+    for (int t = lane; t < 144; t += 32) So[t] = S[t];
+    if (!ok) {
+        for (int t = lane; t < 144; t += 32) Po[t] = (t / 12 == t % 12) ? 1.0 : 0.0;
+        __syncwarp();
+        return;
+    }
+    if (lane < 12) {                                // P = Q^{-1}, column `lane`
+        const int c = lane;
+        double v[12];
+        for (int i = 0; i < 12; i++) {
+            double t = (i == c) ? 1.0 : 0.0;
+            for (int k = 0; k < i; k++) t -= Q[i * 12 + k] * v[k];
+            v[i] = t / Q[i * 12 + i];
+        }
+        for (int i = 11; i >= 0; i--) {
+            double t = v[i];
+            for (int k = i + 1; k < 12; k++) t -= Q[k * 12 + i] * v[k];
+            v[i] = t / Q[i * 12 + i];
+        }
+        for (int i = 0; i < 12; i++) Po[i * 12 + c] = v[i];
+    }
+    __syncwarp();
+}
+
 // per pair: S = K^{1/2} and P = (I + S M_pp S)^{-1} (identity if not positive
-// definite); monomer pairs in closed form as compact 6 x 6 blocks (row stride 6),
-// colloid pairs by Jacobi + Cholesky as 12 x 12 blocks; each pair owns a
-// 144-double slot in S and in P
+// definite); each pair owns a 144-double slot in S and in P.  Monomer pairs: one
+// thread each, closed form, compact 6 x 6 blocks (row stride 6).  Colloid pairs:
+// one warp per colloid in the blocks past the pair blocks, taking the canonical
+// pairs for which it is the lower bead (ps_setup_colloid_pair), 12 x 12 blocks.
 __global__ void __launch_bounds__(PS_THREADS)
 k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
            const Seg *__restrict__ segs, const double *__restrict__ x, const double *__restrict__ chain,
-           const double *__restrict__ tab, int nrow, double *__restrict__ Sout, double *__restrict__ Pout)
+           const double *__restrict__ tab, int nrow, long ncoll, const int *__restrict__ coll_rep,
+           const int *__restrict__ cptr, double *__restrict__ Sout, double *__restrict__ Pout)
 {
-    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ PsWarpSmem wsm[PS_THREADS / 32];
+    const long nbp = (npair + blockDim.x - 1) / blockDim.x;
+    if (blockIdx.x >= nbp) {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const long c = (long)(blockIdx.x - nbp) * (blockDim.x >> 5) + wid;
+        if (c >= ncoll) return;
+        const Seg &s = segs[coll_rep[c]];
+        const long b = s.bead_off + s.Nm + (c - s.coll_off);
+        for (int q = cptr[b]; q < cptr[b + 1]; q++)
+            ps_setup_colloid_pair(s, b, pairs[q].y, x, tab, nrow, Sout + 144L * q, Pout + 144L * q, wsm[wid], lane);
+        return;
+    }
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npair) return;
     const long lo = pairs[q].x, hi = pairs[q].y;
     const Seg &s = segs[rep_of_b(bead_offs, R, lo)];
-    const bool mono = (lo - s.bead_off) < s.Nm;
+    if ((lo - s.bead_off) >= s.Nm) return;            // colloid pair: its lower colloid's warp
     double *So = Sout + 144 * q, *Po = Pout + 144 * q;
-    if (mono) {
-        // closed form: S and the mobility share the modes of the pair block
-        double d[3], lam[4], sq[4], pm[4];
-        mono_pair_modes(s, x, tab, nrow, lo, hi, d, lam);
-        double xs = 0.0, ys = 0.0;
-        if (s.mm_HI && !(s.chain_HI && chain[lo] == chain[hi])) {
-            double dx = x[3 * lo] - x[3 * hi], dy = x[3 * lo + 1] - x[3 * hi + 1], dz = x[3 * lo + 2] - x[3 * hi + 2];
-            const double r = ref_pair_dist(dx, dy, dz), rinv = 1.0 / r;
-            if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(r, rinv, 2.0 * s.beta, xs, ys);
-            else aa_scalars<double>(r, rinv, 2.0 * s.beta, xs, ys);
-        }
-        const double mob[4] = {s.beta_inv + xs, s.beta_inv + ys, s.beta_inv - xs, s.beta_inv - ys};
-        for (int k = 0; k < 4; k++) {
-            double l = lam[k] > 0 ? lam[k] : 0.0;
-            sq[k] = sqrt(l);
-            double t = 1.0 + l * mob[k];
-            pm[k] = t > 0 ? 1.0 / t : 1.0;
-        }
-        // compact 6 x 6 blocks (row stride 6) at the start of the pair's slot
-        mono_pair_matrix(d, sq, So, 6);
-        mono_pair_matrix(d, pm, Po, 6);
-        return;
+    // closed form: S and the mobility share the modes of the pair block
+    double d[3], lam[4], sq[4], pm[4];
+    mono_pair_modes(s, x, tab, nrow, lo, hi, d, lam);
+    double xs = 0.0, ys = 0.0;
+    if (s.mm_HI && !(s.chain_HI && chain[lo] == chain[hi])) {
+        double dx = x[3 * lo] - x[3 * hi], dy = x[3 * lo + 1] - x[3 * hi + 1], dz = x[3 * lo + 2] - x[3 * hi + 2];
+        const double r = ref_pair_dist(dx, dy, dz), rinv = 1.0 / r;
+        if (s.aa_mode == PS_AA_RPY) aa_scalars_rpy<double>(r, rinv, 2.0 * s.beta, xs, ys);
+        else aa_scalars<double>(r, rinv, 2.0 * s.beta, xs, ys);
     }
-    const int nd = 12;
-    double K[144], Q[144], S[144], M[144];
-    lub_pair_block(s, x, tab, nrow, lo, hi, mono, K);
-    jacobi_eig(K, nd, Q);
-    for (int a = 0; a < nd; a++)
-        for (int c = 0; c < nd; c++) {
-            double v = 0.0;
-            for (int k = 0; k < nd; k++) {
-                double lam = K[k * nd + k];
-                v += Q[a * nd + k] * (lam > 0 ? sqrt(lam) : 0.0) * Q[c * nd + k];
-            }
-            S[a * nd + c] = v;
-        }
-    pair_mobility(s, x, chain, lo, hi, mono, M);
-    // T = I + S M S  (K <- M S, Q <- T)
-    for (int a = 0; a < nd; a++)
-        for (int c = 0; c < nd; c++) {
-            double v = 0.0;
-            for (int k = 0; k < nd; k++) v += M[a * nd + k] * S[k * nd + c];
-            K[a * nd + c] = v;
-        }
-    for (int a = 0; a < nd; a++)
-        for (int c = 0; c < nd; c++) {
-            double v = (a == c) ? 1.0 : 0.0;
-            for (int k = 0; k < nd; k++) v += S[a * nd + k] * K[k * nd + c];
-            Q[a * nd + c] = v;
-        }
-    // Cholesky T = C C^T in place (lower), then P = T^{-1} column by column
-    bool ok = true;
-    for (int j = 0; j < nd && ok; j++) {
-        double d = Q[j * nd + j];
-        for (int k = 0; k < j; k++) d -= Q[j * nd + k] * Q[j * nd + k];
-        if (!(d > 0)) { ok = false; break; }
-        d = sqrt(d);
-        Q[j * nd + j] = d;
-        for (int i = j + 1; i < nd; i++) {
-            double v = Q[i * nd + j];
-            for (int k = 0; k < j; k++) v -= Q[i * nd + k] * Q[j * nd + k];
-            Q[i * nd + j] = v / d;
-        }
+    const double mob[4] = {s.beta_inv + xs, s.beta_inv + ys, s.beta_inv - xs, s.beta_inv - ys};
+    for (int k = 0; k < 4; k++) {
+        double l = lam[k] > 0 ? lam[k] : 0.0;
+        sq[k] = sqrt(l);
+        double t = 1.0 + l * mob[k];
+        pm[k] = t > 0 ? 1.0 / t : 1.0;
     }
-    for (int k = 0; k < 144; k++) { So[k] = 0.0; Po[k] = 0.0; }
-    for (int a = 0; a < nd; a++)
-        for (int c = 0; c < nd; c++) So[a * 12 + c] = S[a * nd + c];
-    if (!ok) { for (int a = 0; a < nd; a++) Po[a * 12 + a] = 1.0; return; }
-    for (int c = 0; c < nd; c++) {
-        double v[12];
-        for (int i = 0; i < nd; i++) {
-            double t = (i == c) ? 1.0 : 0.0;
-            for (int k = 0; k < i; k++) t -= Q[i * nd + k] * v[k];
-            v[i] = t / Q[i * nd + i];
-        }
-        for (int i = nd - 1; i >= 0; i--) {
-            double t = v[i];
-            for (int k = i + 1; k < nd; k++) t -= Q[k * nd + i] * v[k];
-            v[i] = t / Q[i * nd + i];
-        }
-        for (int i = 0; i < nd; i++) Po[i * 12 + c] = v[i];
-    }
+    // compact 6 x 6 blocks (row stride 6) at the start of the pair's slot
+    mono_pair_matrix(d, sq, So, 6);
+    mono_pair_matrix(d, pm, Po, 6);
+}
+
+static void launch_ps_setup(Engine &E, cudaStream_t st)
+{
+    const long npair = E.lub_npairs;
+    const long nbp = (npair + PS_THREADS - 1) / PS_THREADS, nbc = (E.ncoll + PS_THREADS / 32 - 1) / (PS_THREADS / 32);
+    ::ps_launch_count++, k_ps_setup<<<(unsigned)(nbp + nbc), PS_THREADS, 0, st>>>(
+        npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.ncoll,
+        E.d_coll_rep, E.d_lubc_ptr, E.d_pS, E.d_pP);
 }
 
 // v = L y (+ add): per bead, the rows of S_q y_q that belong to it, summed over
-// its near pairs in ascending partner order; optionally written into the first
-// nm3nc6 entries of a mobility-layout vector and reduced into ||D^{-1} L y||^2
-// per bead (constraint-row entries of D)
-__global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
-                       const int *__restrict__ sptr, const int *__restrict__ snbr, const int *__restrict__ cidx,
-                       const double *__restrict__ S, const double *__restrict__ y,
-                       const double *__restrict__ add, double *__restrict__ vel, double *__restrict__ top,
-                       const double *__restrict__ D, double *__restrict__ bead_part, const char *__restrict__ done,
-                       int dstride)
+// its near pairs; optionally written into the first nm3nc6 entries of a
+// mobility-layout vector and reduced into ||D^{-1} L y||^2 per bead
+// (constraint-row entries of D).  Monomer beads take one thread each and sum
+// their pairs in ascending partner order.  Colloid beads, which gather the
+// long lists (every near monomer and colloid), take one warp each from the
+// blocks past the bead blocks: lane l sums the pairs l, l + 32, ... of the
+// colloid's list and a fixed butterfly joins the lanes, so the order is fixed.
+__device__ __forceinline__ void ps_L_pair(const double *__restrict__ Sq, const double *__restrict__ yq, bool low,
+                                          int ng, int nd, double acc[6])
 {
-    long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= ntot) return;
-    const int r = rep_of_b(bead_offs, R, b);
-    if (rep_done(done, dstride, r)) return;
-    const Seg &s = segs[r];
-    const int i = (int)(b - s.bead_off);
+    double yv[12];
+#pragma unroll
+    for (int c = 0; c < 12; c++) yv[c] = c < nd ? yq[c] : 0.0;
+    for (int g = 0; g < ng; g++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const double *row = Sq + (6 * g + (low ? 0 : 3) + k) * nd;
+            double v = 0.0;
+#pragma unroll
+            for (int c = 0; c < 12; c++)
+                if (c < nd) v += row[c] * yv[c];
+            acc[3 * g + k] += v;
+        }
+}
+
+__device__ __forceinline__ void ps_L_out(const Seg &s, int i, long b, const double acc[6], const double *__restrict__ add,
+                                         double *__restrict__ vel, double *__restrict__ top,
+                                         const double *__restrict__ D, double *__restrict__ bead_part)
+{
     const bool mono = i < s.Nm;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int t = sptr[b]; t < sptr[b + 1]; t++) {
-        const int qa = cidx[t];
-        if (qa < 0) continue;                           // not in the canonical list (lists disagree)
-        const bool low = b < (long)snbr[t];
-        const double *Sq = S + 144L * qa, *yq = y + 12L * qa;
-        const int ng = mono ? 1 : 2, nd = mono ? 6 : 12;    // monomer pairs: 6 x 6 block, zero elsewhere
-        for (int g = 0; g < ng; g++)
-            for (int k = 0; k < 3; k++) {
-                const int row = 6 * g + (low ? 0 : 3) + k;
-                double v = 0.0;
-                for (int c = 0; c < nd; c++) v += Sq[row * nd + c] * yq[c];
-                acc[3 * g + k] += v;
-            }
-    }
     int tb, wb;
     vel_dofs(s, i, tb, wb);
     double nrm = 0.0;
@@ -501,75 +635,161 @@ __global__ void k_ps_L(long ntot, const int *__restrict__ bead_offs, int R, cons
     if (bead_part) bead_part[b] = nrm;
 }
 
+__global__ void k_ps_L(long ntot, long ncoll, const int *__restrict__ coll_rep, const int *__restrict__ bead_offs,
+                       int R, const Seg *__restrict__ segs, const int *__restrict__ sptr, const int *__restrict__ snbr,
+                       const int *__restrict__ cidx, const double *__restrict__ S, const double *__restrict__ y,
+                       const double *__restrict__ add, double *__restrict__ vel, double *__restrict__ top,
+                       const double *__restrict__ D, double *__restrict__ bead_part, const char *__restrict__ done,
+                       int dstride)
+{
+    const long nbb = (ntot + blockDim.x - 1) / blockDim.x;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (blockIdx.x >= nbb) {
+        const long c = (long)(blockIdx.x - nbb) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (c >= ncoll) return;
+        const int lane = threadIdx.x & 31, r = coll_rep[c];
+        if (rep_done(done, dstride, r)) return;
+        const Seg &s = segs[r];
+        const int i = s.Nm + (int)(c - s.coll_off);
+        const long b = s.bead_off + i;
+        for (int t = sptr[b] + lane; t < sptr[b + 1]; t += 32) {
+            const int qa = cidx[t];
+            if (qa < 0) continue;                       // not in the canonical list (lists disagree)
+            ps_L_pair(S + 144L * qa, y + 12L * qa, b < (long)snbr[t], 2, 12, acc);
+        }
+#pragma unroll
+        for (int q = 0; q < 6; q++)
+            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (lane == 0) ps_L_out(s, i, b, acc, add, vel, top, D, bead_part);
+        return;
+    }
+    const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ntot) return;
+    const int r = rep_of_b(bead_offs, R, b);
+    if (rep_done(done, dstride, r)) return;
+    const Seg &s = segs[r];
+    const int i = (int)(b - s.bead_off);
+    if (i >= s.Nm) return;                              // colloid: one warp in the blocks past nbb
+    for (int t = sptr[b]; t < sptr[b + 1]; t++) {
+        const int qa = cidx[t];
+        if (qa < 0) continue;
+        ps_L_pair(S + 144L * qa, y + 12L * qa, b < (long)snbr[t], 1, 6, acc);   // monomer pairs: 6 x 6 blocks
+    }
+    ps_L_out(s, i, b, acc, add, vel, top, D, bead_part);
+}
+
+static void launch_ps_L(Engine &E, const double *y, const double *add, double *vel, double *top, const double *D,
+                        double *bead_part, const char *done, int dstride, cudaStream_t st)
+{
+    const int thr = 128;
+    const long nbb = (E.ntot + thr - 1) / thr, nbc = (E.ncoll + thr / 32 - 1) / (thr / 32);
+    ::ps_launch_count++, k_ps_L<<<(unsigned)(nbb + nbc), thr, 0, st>>>(
+        E.ntot, E.ncoll, E.d_coll_rep, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr, E.d_lub_cidx, E.d_pS,
+        y, add, vel, top, D, bead_part, done, dstride);
+}
+
 // w_q = sign * S_q z_q (+ p_q), z gathered from the velocity rows of the Mr apply
 // (y + y2 for replicas with a dense stresslet block) plus an optional velocity
-// vector; part[q] = p_q . w_q
+// vector; part[q] = p_q . w_q.  Sixteen lanes per pair: lane a gathers z_a and
+// forms row a (rows and columns past nd, 6 for monomer pairs, add nothing), and
+// a fixed butterfly over the sixteen lanes forms the dot.
+constexpr int LT_LANES = 16;
+
+// z_a = (P_q r)_a for lane a of a pair's team (r_c held by lane c); rows and
+// columns past nd (6 for monomer pairs) add nothing, columns in ascending order
+__device__ __forceinline__ double pm_matvec(const double *__restrict__ Pq, int a, int nd, double ra, unsigned team)
+{
+    double z = 0.0;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+        const double rc = __shfl_sync(team, ra, c, LT_LANES);
+        if (a < nd && c < nd) z += Pq[a * nd + c] * rc;
+    }
+    return z;
+}
+
 __global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
                         const Seg *__restrict__ segs, const double *__restrict__ S, const double *__restrict__ y,
                         const double *__restrict__ y2, const double *__restrict__ addv, double sign,
                         const double *__restrict__ p, double *__restrict__ w, double *__restrict__ part,
                         const char *__restrict__ done, int dstride)
 {
-    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= npair) return;
+    const long q = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LT_LANES;
+    const int a = threadIdx.x % LT_LANES;
+    const unsigned team = 0xffffu << (threadIdx.x & 16);
+    if (q >= npair) return;                       // whole teams leave together
     const long lo = pairs[q].x, hi = pairs[q].y;
     const int r = rep_of_b(bead_offs, R, lo);
     if (rep_done(done, dstride, r)) return;
     const Seg &s = segs[r];
     const bool mono = (lo - s.bead_off) < s.Nm;
-    int dof[12], nd;
-    pair_dofs(s, lo, hi, mono, dof, nd);
-    double z[12];
-    for (int k = 0; k < 12; k++) z[k] = 0.0;
-    for (int k = 0; k < nd; k++)
-        z[k] = y[s.top_off + dof[k]] + (s.ss_off >= 0 ? y2[s.top_off + dof[k]] : 0.0) +
-               (addv ? addv[s.vel_off + dof[k]] : 0.0);
-    const double *Sq = S + 144L * q;
+    const int nd = mono ? 6 : 12;
+    double za = 0.0;
+    if (a < nd) {
+        const long bd = (a % 6) < 3 ? lo : hi;
+        int tb, wb;
+        vel_dofs(s, (int)(bd - s.bead_off), tb, wb);
+        const int d = (a < 6 ? tb : wb) + a % 3;
+        za = y[s.top_off + d] + (s.ss_off >= 0 ? y2[s.top_off + d] : 0.0) + (addv ? addv[s.vel_off + d] : 0.0);
+    }
+    const double *Sq = S + 144L * q + a * nd;
+    double v = 0.0;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+        const double zc = __shfl_sync(team, za, c, LT_LANES);
+        if (a < nd && c < nd) v += Sq[c] * zc;
+    }
+    v *= sign;
     double dot = 0.0;
-    // monomer pairs hold a 6 x 6 block (zero elsewhere): rows and columns past nd add nothing
-    for (int a = 0; a < 12; a++) {
-        double v = 0.0;
-        if (a < nd)
-            for (int c = 0; c < nd; c++) v += Sq[a * nd + c] * z[c];
-        v *= sign;
-        if (p) { v += p[12 * q + a]; dot += p[12 * q + a] * v; }
+    if (a < 12) {
+        if (p) { v += p[12 * q + a]; dot = p[12 * q + a] * v; }
         w[12 * q + a] = v;
     }
-    if (part) part[q] = dot;
+    if (part) {
+#pragma unroll
+        for (int o = LT_LANES / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(team, dot, o, LT_LANES);
+        if (a == 0) part[q] = dot;
+    }
 }
 
-// first iterate: y = 0, r = rhs (in rv), z = P r, p = z, part = r . z
+// first iterate: y = 0, r = rhs (in rv), z = P r, p = z, part = r . z;
+// a team of LT_LANES lanes per pair, lane a owning entry a
 __global__ void k_ps_init(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
                           const Seg *__restrict__ segs, const double *__restrict__ P, double *__restrict__ yv,
                           const double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ pv,
                           double *__restrict__ part)
 {
-    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long q = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LT_LANES;
+    const int a = threadIdx.x % LT_LANES;
+    const unsigned team = 0xffffu << (threadIdx.x & 16);
     if (q >= npair) return;
     const long lo = pairs[q].x;
     const Seg &s = segs[rep_of_b(bead_offs, R, lo)];
     const int nd = (lo - s.bead_off) < s.Nm ? 6 : 12;     // monomer pairs: 6 x 6 block, zero elsewhere
-    const double *Pq = P + 144L * q;
+    const long e = 12 * q + a;
+    const double ra = a < 12 ? rv[e] : 0.0;
+    const double v = pm_matvec(P + 144L * q, a, nd, ra, team);
     double dot = 0.0;
-    for (int a = 0; a < 12; a++) {
-        double v = 0.0;
-        if (a < nd)
-            for (int c = 0; c < nd; c++) v += Pq[a * nd + c] * rv[12 * q + c];
-        zv[12 * q + a] = v;
-        pv[12 * q + a] = v;
-        yv[12 * q + a] = 0.0;
-        dot += rv[12 * q + a] * v;
+    if (a < 12) {
+        zv[e] = v;
+        pv[e] = v;
+        yv[e] = 0.0;
+        dot = ra * v;
     }
-    part[q] = dot;
+#pragma unroll
+    for (int o = LT_LANES / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(team, dot, o, LT_LANES);
+    if (a == 0) part[q] = dot;
 }
 
-// y += alpha p ; r -= alpha Ap ; z = P r ; part = r . z
+// y += alpha p ; r -= alpha Ap ; z = P r ; part = r . z; a team per pair as k_ps_init
 __global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
                             const Seg *__restrict__ segs, const PcgScal *__restrict__ pc, const double *__restrict__ P,
                             const double *__restrict__ pv, const double *__restrict__ Ap, double *__restrict__ yv,
                             double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ part)
 {
-    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long q = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LT_LANES;
+    const int a = threadIdx.x % LT_LANES;
+    const unsigned team = 0xffffu << (threadIdx.x & 16);
     if (q >= npair) return;
     const long lo = pairs[q].x;
     const int r = rep_of_b(bead_offs, R, lo);
@@ -577,32 +797,33 @@ __global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const in
     if (sc.done) return;
     // monomer pairs: 6 x 6 blocks, and entries 6..11 of every pair vector stay zero
     const int nd = (lo - segs[r].bead_off) < segs[r].Nm ? 6 : 12;
-    double rq[12];
-    for (int a = 0; a < nd; a++) {
-        yv[12 * q + a] += sc.alpha * pv[12 * q + a];
-        rq[a] = rv[12 * q + a] - sc.alpha * Ap[12 * q + a];
-        rv[12 * q + a] = rq[a];
+    const long e = 12 * q + a;
+    double ra = 0.0;
+    if (a < nd) {
+        yv[e] += sc.alpha * pv[e];
+        ra = rv[e] - sc.alpha * Ap[e];
+        rv[e] = ra;
     }
-    const double *Pq = P + 144L * q;
+    const double v = pm_matvec(P + 144L * q, a, nd, ra, team);
     double dot = 0.0;
-    for (int a = 0; a < nd; a++) {
-        double v = 0.0;
-        for (int c = 0; c < nd; c++) v += Pq[a * nd + c] * rq[c];
-        zv[12 * q + a] = v;
-        dot += rq[a] * v;
+    if (a < nd) {
+        zv[e] = v;
+        dot = ra * v;
     }
-    part[q] = dot;
+#pragma unroll
+    for (int o = LT_LANES / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(team, dot, o, LT_LANES);
+    if (a == 0) part[q] = dot;
 }
 
-// p = z + beta p
+// p = z + beta p, one thread per pair-vector entry
 __global__ void k_ps_dir(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
                          const PcgScal *__restrict__ pc, const double *__restrict__ zv, double *__restrict__ pv)
 {
-    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= npair) return;
-    const PcgScal sc = pc[rep_of_b(bead_offs, R, pairs[q].x)];
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 12 * npair) return;
+    const PcgScal &sc = pc[rep_of_b(bead_offs, R, pairs[e / 12].x)];
     if (sc.done) return;
-    for (int a = 0; a < 12; a++) pv[12 * q + a] = zv[12 * q + a] + sc.beta * pv[12 * q + a];
+    pv[e] = zv[e] + sc.beta * pv[e];
 }
 
 // per-replica sums over the bead table: pair partials by lower bead plus the
@@ -617,9 +838,10 @@ __global__ void k_ps_reduce(RedTable T, const int *__restrict__ cptr, const doub
     const RBlk B = T.d_blk[blockIdx.x];
     if (pc[B.rep].done) return;
     double v[2] = {0.0, 0.0};
+    // pairs are stored by lower bead, so the block's beads own one contiguous pair range
+    for (long q = cptr[B.start] + threadIdx.x; q < cptr[B.start + B.len]; q += RB_THREADS) v[0] += part[q];
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
         long b = B.start + e;
-        for (int q = cptr[b]; q < cptr[b + 1]; q++) v[0] += part[q];
         if (add0) v[0] += add0[b];
         if (bead_part) v[1] += bead_part[b];
         if (add1) v[1] += add1[b];
@@ -789,65 +1011,113 @@ __device__ __forceinline__ void s_precond(const double r[5], double z[5])
     for (int k = 1; k < 4; k++) z[k] = r[k] / 1.8;
 }
 
-// one thread per pair (t < npair) or per bead (t - npair; stresslet entries of
-// joint-replica colloids, nothing for other beads).
+// MINRES element work of pair t by a team of LT_LANES lanes, lane a owning entry a
+// of the pair vectors (a < 12); the partial dots join over the team by a fixed
+// butterfly.  mode as k_pm_elem.
+__device__ __forceinline__ void pm_pair_team(long t, int a, unsigned team, const int2 *__restrict__ pairs,
+                                             const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
+                                             const MinresScal *__restrict__ mr, int mode, int k, const PMArgs &A)
+{
+    const long bead = pairs[t].x;
+    const int r = rep_of_b(bead_offs, R, bead);
+    const Seg &sp = segs[r];
+    const int nd = (bead - sp.bead_off) < sp.Nm ? 6 : 12;   // monomer pairs: 6 x 6 blocks
+    const MinresScal m = mr[r];
+    const long e = 12 * t + a;
+    const bool act = a < 12;
+    double dot0 = 0.0, dot1 = 0.0;
+    if (mode == 0) {
+        const double rv = act ? A.R[1].pair[e] : 0.0;
+        const double zv = pm_matvec(A.P + 144L * t, a, nd, rv, team);
+        if (act) {
+            A.z.pair[e] = zv; A.x.pair[e] = 0.0; A.v.pair[e] = 0.0;
+            A.W[0].pair[e] = 0.0; A.W[1].pair[e] = 0.0; A.W[2].pair[e] = 0.0;
+            dot0 = rv * zv;
+            dot1 = zv * zv;
+        }
+    } else if (mode == 1 || mode == 3) {
+        if (act) {
+            double *vv = A.v.pair;
+            if (m.pending) {
+                const double w = (vv[e] - m.up_oldeps * A.W[k % 3].pair[e] - m.up_delta * A.W[(k + 1) % 3].pair[e]) *
+                                 m.up_ginv;
+                A.W[(k + 2) % 3].pair[e] = w;
+                A.x.pair[e] += m.up_phi * w;
+            }
+            if (mode == 1 && !m.done) {
+                const double vq = A.z.pair[e] * m.sinv;
+                double x = m.sinv * A.Az[e];
+                if (k >= 2) x -= (m.beta / m.oldb) * A.R[(k + 2) % 3].pair[e];
+                vv[e] = vq;
+                A.R[(k + 1) % 3].pair[e] = x;
+                dot0 = vq * x;
+            }
+        }
+    } else if (mode == 2 && !m.done) {
+        double rv = 0.0;
+        if (act) {
+            double *av = A.R[(k + 1) % 3].pair;
+            rv = av[e] - (m.alfa / m.beta) * A.R[k % 3].pair[e];
+            av[e] = rv;
+        }
+        const double zv = pm_matvec(A.P + 144L * t, a, nd, rv, team);
+        if (act) {
+            A.z.pair[e] = zv;
+            dot0 = rv * zv;
+        }
+    }
+    if (mode <= 2) {
+#pragma unroll
+        for (int o = LT_LANES / 2; o > 0; o >>= 1) {
+            dot0 += __shfl_xor_sync(team, dot0, o, LT_LANES);
+            dot1 += __shfl_xor_sync(team, dot1, o, LT_LANES);
+        }
+        if (a == 0) { A.part[t] = dot0; A.part2[t] = dot1; }
+    }
+}
+
+// Teams of LT_LANES lanes per pair (global thread < npair * LT_LANES), then one
+// thread per bead (stresslet entries of joint-replica colloids, nothing for
+// other beads).
 // mode 0 init, 1 alpha (pending w/x update, v = z/beta, Av), 2 beta (r_{k+1}, z = P r), 3 flush
 __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs,
                           int R, const Seg *__restrict__ segs, const MinresScal *__restrict__ mr, int mode, int k,
                           PMArgs A)
 {
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool is_pair = t < npair;
-    if (t >= npair + ntot) return;
-    long base, bead;
-    int n;
-    double *u_s = nullptr;
-    const double *y_s = nullptr;
-    int nd = 12;          // pair blocks: 6 x 6 (row stride 6) for monomer pairs
-    if (is_pair) {
-        base = 12 * t;
-        n = 12;
-        bead = pairs[t].x;
-        const Seg &sp = segs[rep_of_b(bead_offs, R, bead)];
-        if (bead - sp.bead_off < sp.Nm) nd = 6;
-    } else {
-        bead = t - npair;
-        const Seg &s0 = segs[rep_of_b(bead_offs, R, bead)];
-        const int i = (int)(bead - s0.bead_off);
-        if (!(s0.Nc > 0 && s0.ss_off < 0 && i >= s0.Nm)) {
-            if (mode <= 2) { A.sA[bead] = 0.0; A.sB[bead] = 0.0; }
-            return;
-        }
-        base = (long)s0.top_off + s0.nm3nc6 + 5 * (i - s0.Nm);
-        n = 5;
-        u_s = A.u + base;
-        y_s = A.y + base;
+    const long gt = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long npt = npair * LT_LANES;
+    if (gt < npt) {
+        pm_pair_team(gt / LT_LANES, threadIdx.x % LT_LANES, 0xffffu << (threadIdx.x & 16), pairs, bead_offs, R, segs,
+                     mr, mode, k, A);
+        return;
     }
+    const long bead = gt - npt;
+    if (bead >= ntot) return;
     const int r = rep_of_b(bead_offs, R, bead);
+    const Seg &s0 = segs[r];
+    const int i = (int)(bead - s0.bead_off);
+    if (!(s0.Nc > 0 && s0.ss_off < 0 && i >= s0.Nm)) {
+        if (mode <= 2) { A.sA[bead] = 0.0; A.sB[bead] = 0.0; }
+        return;
+    }
+    const long base = (long)s0.top_off + s0.nm3nc6 + 5 * (i - s0.Nm);
+    const int n = 5;
+    double *u_s = A.u + base;
+    const double *y_s = A.y + base;
     const MinresScal m = mr[r];
-    auto V = [&](const PMVec &p) { return (is_pair ? p.pair : p.s) + base; };
+    auto V = [&](const PMVec &p) { return p.s + base; };
     double dot0 = 0.0, dot1 = 0.0;
     if (mode == 0) {
-        double rv[12], zv[12];
+        double rv[5], zv[5];
         double *rr = V(A.R[1]);
         for (int a = 0; a < n; a++) rv[a] = rr[a];
-        if (is_pair) {
-            const double *Pq = A.P + 144L * t;
-            for (int a = 0; a < 12; a++) {
-                double acc = 0.0;
-                if (a < nd)
-                    for (int c = 0; c < nd; c++) acc += Pq[a * nd + c] * rv[c];
-                zv[a] = acc;
-            }
-        } else {
-            s_precond(rv, zv);
-        }
+        s_precond(rv, zv);
         double *zz = V(A.z), *xx = V(A.x), *vv = V(A.v), *w0 = V(A.W[0]), *w1 = V(A.W[1]), *w2 = V(A.W[2]);
         for (int a = 0; a < n; a++) {
             zz[a] = zv[a]; xx[a] = 0.0; vv[a] = 0.0; w0[a] = 0.0; w1[a] = 0.0; w2[a] = 0.0;
             dot0 += rv[a] * zv[a];
             dot1 += zv[a] * zv[a];
-            if (u_s) u_s[a] = zv[a];
+            u_s[a] = zv[a];
         }
     } else if (mode == 1 || mode == 3) {
         double *vv = V(A.v);
@@ -863,13 +1133,12 @@ __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs,
         }
         if (mode == 1 && !m.done) {
             const double *zz = V(A.z);
-            const double *az = is_pair ? A.Az + base : y_s;
             double *av = V(A.R[(k + 1) % 3]);
             const double *rm1 = V(A.R[(k + 2) % 3]);
             const double c1 = (k >= 2) ? m.beta / m.oldb : 0.0;
             for (int a = 0; a < n; a++) {
                 double vq = zz[a] * m.sinv;
-                double x = m.sinv * az[a];
+                double x = m.sinv * y_s[a];
                 if (k >= 2) x -= c1 * rm1[a];
                 vv[a] = vq;
                 av[a] = x;
@@ -880,30 +1149,17 @@ __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs,
         double *av = V(A.R[(k + 1) % 3]);
         const double *rk = V(A.R[k % 3]);
         const double c2 = m.alfa / m.beta;
-        double rv[12], zv[12];
+        double rv[5], zv[5];
         for (int a = 0; a < n; a++) { rv[a] = av[a] - c2 * rk[a]; av[a] = rv[a]; }
-        if (is_pair) {
-            const double *Pq = A.P + 144L * t;
-            for (int a = 0; a < 12; a++) {
-                double acc = 0.0;
-                if (a < nd)
-                    for (int c = 0; c < nd; c++) acc += Pq[a * nd + c] * rv[c];
-                zv[a] = acc;
-            }
-        } else {
-            s_precond(rv, zv);
-        }
+        s_precond(rv, zv);
         double *zz = V(A.z);
         for (int a = 0; a < n; a++) {
             zz[a] = zv[a];
             dot0 += rv[a] * zv[a];
-            if (u_s) u_s[a] = zv[a];
+            u_s[a] = zv[a];
         }
     }
-    if (mode <= 2) {
-        if (is_pair) { A.part[t] = dot0; A.part2[t] = dot1; }
-        else { A.sA[bead] = dot0; A.sB[bead] = dot1; }
-    }
+    if (mode <= 2) { A.sA[bead] = dot0; A.sB[bead] = dot1; }
 }
 
 // per-replica MINRES scalar updates over the bead table (pair partials by lower bead)
@@ -918,9 +1174,13 @@ __global__ void k_pm_reduce(RedTable T, const int *__restrict__ cptr, const doub
     if (mode != 1 && m0.done) return;
     if (mode == 1 && m0.done && !m0.pending) return;
     double v[2] = {0.0, 0.0};
+    // pairs are stored by lower bead, so the block's beads own one contiguous pair range
+    for (long q = cptr[B.start] + threadIdx.x; q < cptr[B.start + B.len]; q += RB_THREADS) {
+        v[0] += part[q];
+        v[1] += part2[q];
+    }
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
         long b = B.start + e;
-        for (int q = cptr[b]; q < cptr[b + 1]; q++) { v[0] += part[q]; v[1] += part2[q]; }
         v[0] += sA[b];
         v[1] += sB[b];
     }
@@ -1002,8 +1262,10 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     const long npair = E.lub_npairs;
     const int thr = 128;
     const unsigned nbp = (unsigned)((std::max<long>(npair, 1) + PS_THREADS - 1) / PS_THREADS);
+    const unsigned nbp_lt = (unsigned)((std::max<long>(npair, 1) * LT_LANES + PS_THREADS - 1) / PS_THREADS);
+    const unsigned nbp_e = (unsigned)((std::max<long>(npair, 1) * 12 + PS_THREADS - 1) / PS_THREADS);
     const unsigned nbb = (unsigned)((E.ntot + thr - 1) / thr);
-    const unsigned nbe = (unsigned)((npair + E.ntot + thr - 1) / thr);
+    const unsigned nbe = (unsigned)((npair * LT_LANES + E.ntot + thr - 1) / thr);
     const char *dn = (const char *)&E.d_pmr[0].done;
     const int ds = (int)sizeof(MinresScal);
     PMArgs A;
@@ -1021,7 +1283,7 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     // rhs into R[1]: pairs L^T (g + Mr b_bot), stresslets b_S + (M b_bot)_S
     mr_apply(E, fp32, dn, ds, st);
     if (npair)
-        ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+        ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                               E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, A.R[1].pair,
                                                               nullptr, dn, ds);
     ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
@@ -1040,12 +1302,10 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
         for (int j = 0; j < 8 && k < maxit; j++) {
             k++;
             // Az = A z: u = [L z_y ; z_S] (z_S already in u), apply, z_y + L^T (...)_t
-            ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                          E.d_lub_nbr, E.d_lub_cidx, E.d_pS, A.z.pair,
-                                                          nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds);
+            launch_ps_L(E, A.z.pair, nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds, st);
             mr_apply(E, fp32, dn, ds, st);
             if (npair)
-                ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                       E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
                                                                       A.z.pair, E.d_pmp[9], nullptr, dn, ds);
             ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
@@ -1083,6 +1343,8 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     const long npair = E.lub_npairs;
     const int thr = 128;
     const unsigned nbp = (unsigned)((std::max<long>(npair, 1) + PS_THREADS - 1) / PS_THREADS);
+    const unsigned nbp_lt = (unsigned)((std::max<long>(npair, 1) * LT_LANES + PS_THREADS - 1) / PS_THREADS);
+    const unsigned nbp_e = (unsigned)((std::max<long>(npair, 1) * 12 + PS_THREADS - 1) / PS_THREADS);
     const unsigned nbb = (unsigned)((E.ntot + thr - 1) / thr);
     int rc = diag_saddle(E, E.d_D, st);
     if (rc) return rc;
@@ -1110,9 +1372,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     // the pair blocks depend on the staged positions and the table only: solves
     // that share a staging (the deterministic and the noise solve) set them up once
     if (npair && !E.ps_setup_valid) {
-        ::ps_launch_count++, k_ps_setup<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                                 E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.d_pS,
-                                                                 E.d_pP);
+        launch_ps_setup(E, st);
         E.ps_setup_valid = true;
     }
     if (E.n_ss_reps) {
@@ -1141,10 +1401,10 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
             // rhs = L^T (g + Mr b_bot) (joint replicas: Mr -> M, and b_S + (M b_bot)_S) ; r = rhs ; z = P r ; p = z
             mr_apply(E, fp32, dn, ds, st);
             if (npair) {
-                ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                                       E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
                                                                       (const char *)dn, ds);
-                ::ps_launch_count++, k_ps_init<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                ::ps_launch_count++, k_ps_init<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                         E.d_segs, E.d_pP, yv, rv, zv, pv, E.d_ppart);
             }
         }
@@ -1152,9 +1412,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
             ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
                                                       yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
         // initial residual ||D^{-1} L r||^2 + ||D^{-1} r_S||^2
-        ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
-                                                      E.d_lub_cidx, E.d_pS, rv, nullptr, nullptr, nullptr,
-                                                      E.d_D, bead_part, (const char *)dn, ds);
+        launch_ps_L(E, rv, nullptr, nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds, st);
         ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA, sB,
                                                                       E.d_pcg, 1, maxit, E.d_nactive);
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1164,12 +1422,10 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
         while (nact > 0 && k < maxit) {
             for (int j = 0; j < check_every && k < maxit; j++, k++) {
                 // Ap = p + L^T Mr L p  (joint replicas: [p_y + L^T (M u)_t ; (M u)_S], u = [L p_y ; p_S])
-                ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                              E.d_lub_nbr, E.d_lub_cidx, E.d_pS, pv, nullptr,
-                                                              nullptr, E.d_pu, nullptr, nullptr, (const char *)dn, ds);
+                launch_ps_L(E, pv, nullptr, nullptr, E.d_pu, nullptr, nullptr, (const char *)dn, ds, st);
                 mr_apply(E, fp32, dn, ds, st);
                 if (npair)
-                    ::ps_launch_count++, k_ps_LT<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                    ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                           E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
                                                                           pv, Ap, E.d_ppart, (const char *)dn, ds);
                 if (joint)
@@ -1178,19 +1434,17 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                 ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, nullptr, sA,
                                                                               nullptr, E.d_pcg, 0, maxit, E.d_nactive);
                 if (npair)
-                    ::ps_launch_count++, k_ps_update<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                    ::ps_launch_count++, k_ps_update<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                               E.d_segs, E.d_pcg, E.d_pP, pv, Ap, yv, rv,
                                                                               zv, E.d_ppart);
                 if (joint)
                     ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
-                ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr,
-                                                              E.d_lub_nbr, E.d_lub_cidx, E.d_pS, rv, nullptr,
-                                                              nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds);
+                launch_ps_L(E, rv, nullptr, nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds, st);
                 ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA,
                                                                               sB, E.d_pcg, 2, maxit, E.d_nactive);
                 if (npair)
-                    ::ps_launch_count++, k_ps_dir<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                    ::ps_launch_count++, k_ps_dir<<<nbp_e, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                            E.d_pcg, zv, pv);
                 if (joint)
                     ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
@@ -1202,9 +1456,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
         }
     }
     // F_t = -b_bot + L y (into u_t and the force rows), then U = Mr F_t - g, F_S
-    ::ps_launch_count++, k_ps_L<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr,
-                                                  E.d_lub_cidx, E.d_pS, yv, cvel, tmp, E.d_pu, nullptr,
-                                                  nullptr, nullptr, 0);
+    launch_ps_L(E, yv, cvel, tmp, E.d_pu, nullptr, nullptr, nullptr, 0, st);
     ::ps_launch_count++, k_ps_ft<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, tmp, x);
     if (joint)
         ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
@@ -1298,6 +1550,65 @@ int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o
     }
     if (res) *res = r0;
     return r0.reason;
+}
+
+// ---------------------------------------------------------------------------
+// Brownian lubrication force, rhs_bot += -sqrt(2 kT / dt) sum_p B_p R_p^{1/2} z_p.
+// Each canonical pair q owns 12 normals z_q (monomer pairs use the first 6):
+// injected (z + 12 q) or drawn from the replica's Philox stream with
+// subsequence q - (first canonical pair of the replica).  R_p^{1/2} is the
+// symmetric square root that the pair-space setup stores as the pair's S block,
+// so the force is the L-gather of the pair-space solve applied to z (one
+// evaluation per pair; the staging's setup is shared with the solve after it).
+__global__ void k_lub_z(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
+                        const Seg *__restrict__ segs, const int *__restrict__ cptr, const uint64_t *__restrict__ rseed,
+                        const uint64_t *__restrict__ rstep, double *__restrict__ z)
+{
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npair) return;
+    const int r = rep_of_b(bead_offs, R, pairs[q].x);
+    curandStatePhilox4_32_10_t stt;
+    curand_init(rseed[r], (unsigned long long)(q - cptr[segs[r].bead_off]), (3ull * rstep[r] + 2) * 4ull, &stt);
+    for (int k = 0; k < 12; k++) z[12 * q + k] = curand_normal_double(&stt);
+}
+
+__global__ void k_lub_noise_add(long nvel, const int *__restrict__ vel_offs, int R, const Seg *__restrict__ segs,
+                                const double *__restrict__ v, double *__restrict__ rhs)
+{
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nvel) return;
+    const Seg &s = segs[rep_at(vel_offs, R, k)];
+    rhs[(long)s.vec_off + s.nm3nc11 + (k - s.vel_off)] += -sqrt(2.0 * s.kT / s.dt) * v[k];
+}
+
+int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st)
+{
+    const long npair = E.lub_npairs;
+    if (npair <= 0) return PS_OK;
+    int rc;
+    if ((rc = ensure_pair_space(E))) return rc;
+    const unsigned nbp = (unsigned)((npair + PS_THREADS - 1) / PS_THREADS);
+    if (!E.ps_setup_valid) {
+        launch_ps_setup(E, st);
+        E.ps_setup_valid = true;
+    }
+    if (!z) {
+        const long nz = 12 * npair;
+        if (nz > E.zlub_cap) {
+            cudaFree(E.d_zlub);
+            E.zlub_cap = nz * 3 / 2 + 1024;
+            PS_CK(cudaMalloc(&E.d_zlub, sizeof(double) * E.zlub_cap));
+        }
+        ::ps_launch_count++, k_lub_z<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                                                              E.d_lubc_ptr, E.d_rseed, E.d_rstep, E.d_zlub);
+        z = E.d_zlub;
+    }
+    launch_ps_L(E, z, nullptr, E.d_tmp_vel, nullptr, nullptr, nullptr, nullptr, 0, st);
+    const int thr = 256;
+    ::ps_launch_count++, k_lub_noise_add<<<(unsigned)((E.nvel + thr - 1) / thr), thr, 0, st>>>(
+        E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_tmp_vel, rhs);
+    PS_CK(cudaGetLastError());
+    return PS_OK;
 }
 
 }  // namespace ps

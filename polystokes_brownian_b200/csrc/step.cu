@@ -368,7 +368,7 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         ::ps_launch_count++, k_add_noise<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
         if (E.any_lub && E.lub_npairs > 0) {
             // Brownian lubrication force: 12 normals per canonical pair, injected
-            // or drawn inside the gather from the replica's Philox stream
+            // or drawn from the replica's Philox stream
             const double *zl = in ? in->zlub : nullptr;
             if (zl && is_host_ptr(zl)) {
                 long nz = 12 * E.lub_npairs;
