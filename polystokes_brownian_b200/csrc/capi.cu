@@ -70,7 +70,7 @@ static void free_engine(Engine &E)
                     E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8], E.d_obs_acc, E.d_obs_prev,
                     E.d_obs_ring, E.d_obs_msd, E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.d_obs_msdn,
                     E.d_sl_reps, E.d_sl_skip, E.d_slV, E.d_slT, E.d_sl_sc, E.d_sl_u, E.d_sl_y, E.d_sl_y2,
-                    E.d_cell_big, E.d_cell_nbig, E.d_cell_tmp, E.d_ref_r, E.d_ref_d};
+                    E.d_cell_big, E.d_cell_nbig, E.d_cell_tmp, E.d_ref_r, E.d_ref_d, E.d_pm_cnt};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);

@@ -450,59 +450,70 @@ __global__ void k_lz_init(RedTable T, const Seg *__restrict__ segs, double *__re
     }
 }
 
-// Implicit QL (symmetric tridiagonal, Wilkinson shift) on one warp: lane 0
-// runs the scalar recurrences, all lanes rotate the eigenvector columns.
-__device__ void warp_tql(double *d, double *e, double *Z, int n)
+// Implicit QL (symmetric tridiagonal, Wilkinson shift) on one warp.  Lane 0
+// runs each QL iteration's scalar recurrence on the shared d, e and records
+// the iteration's rotations (c, s) in rot; then every lane applies them, in the
+// recurrence's order, to its own rows of Z.  A row sees the same rotations in
+// the same order as when each rotation is applied to all rows at once, so Z is
+// the same, without a warp barrier per rotation.  rot holds 2 n doubles.
+__device__ void warp_tql(double *d, double *e, double *Z, double *rot, int n)
 {
-    // Every lane runs the same scalar recurrence on the same shared d, e (so all
-    // lanes hold identical rotations without shuffles); lane 0 writes d, e back
-    // and each lane applies the rotations to its own rows of Z.
     const int lane = threadIdx.x & 31;
     for (int k = lane; k < n * n; k += 32) Z[k] = (k / n == k % n) ? 1.0 : 0.0;
     __syncwarp();
     for (int l = 0; l < n; l++) {
         int iter = 0;
         while (true) {
-            int m;
-            for (m = l; m < n - 1; m++) {
-                double dd = fabs(d[m]) + fabs(d[m + 1]);
-                if (fabs(e[m]) <= 1e-16 * dd) break;
-            }
-            if (m == l || iter++ >= 60) break;
-            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-            double r = hypot(g, 1.0);
-            g = d[m] - d[l] + e[l] / (g + copysign(r, g));
-            double s = 1, c = 1, p = 0;
-            int i;
-            bool brk = false;
-            for (i = m - 1; i >= l; i--) {
-                const double ei = e[i], di = d[i], di1 = d[i + 1];
-                double f = s * ei, b = c * ei;
-                // rotation from one reciprocal square root (the chain of dependent
-                // divisions is this loop's latency; f, g are O(|T|), far from overflow)
-                const double r2 = f * f + g * g, ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
-                const double rr = r2 * ri;
-                __syncwarp();               // every lane has read this rotation's d, e
-                if (rr == 0.0) {
-                    if (lane == 0) { e[i + 1] = rr; d[i + 1] = di1 - p; e[m] = 0.0; }
-                    __syncwarp();
-                    brk = true;
-                    break;
+            int m = l, go = 0, iend = l;
+            if (lane == 0) {
+                for (m = l; m < n - 1; m++) {
+                    double dd = fabs(d[m]) + fabs(d[m + 1]);
+                    if (fabs(e[m]) <= 1e-16 * dd) break;
                 }
-                s = f * ri; c = g * ri;
-                g = di1 - p;
-                r = (di - g) * s + 2.0 * c * b;
-                p = s * r;
-                if (lane == 0) { e[i + 1] = rr; d[i + 1] = g + p; }
-                g = c * r - b;
-                for (int k = lane; k < n; k += 32) {
-                    double fz = Z[k * n + i + 1];
-                    Z[k * n + i + 1] = s * Z[k * n + i] + c * fz;
-                    Z[k * n + i] = c * Z[k * n + i] - s * fz;
+                go = (m != l) && (iter < 60);
+                if (go) {
+                    double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+                    double r = hypot(g, 1.0);
+                    g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+                    double s = 1, c = 1, p = 0;
+                    bool brk = false;
+                    for (int i = m - 1; i >= l; i--) {
+                        const double ei = e[i], di = d[i], di1 = d[i + 1];
+                        double f = s * ei, b = c * ei;
+                        // rotation from one reciprocal square root (the chain of dependent
+                        // divisions is this loop's latency; f, g are O(|T|), far from overflow)
+                        const double r2 = f * f + g * g, ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
+                        const double rr = r2 * ri;
+                        if (rr == 0.0) {
+                            e[i + 1] = rr; d[i + 1] = di1 - p; e[m] = 0.0;
+                            brk = true;
+                            iend = i + 1;
+                            break;
+                        }
+                        s = f * ri; c = g * ri;
+                        g = di1 - p;
+                        r = (di - g) * s + 2.0 * c * b;
+                        p = s * r;
+                        e[i + 1] = rr; d[i + 1] = g + p;
+                        g = c * r - b;
+                        rot[2 * i] = c; rot[2 * i + 1] = s;
+                    }
+                    if (!brk) { d[l] -= p; e[l] = g; e[m] = 0.0; }
                 }
             }
-            if (brk) continue;
-            if (lane == 0) { d[l] -= p; e[l] = g; e[m] = 0.0; }
+            iter++;
+            m = __shfl_sync(0xffffffffu, m, 0);
+            go = __shfl_sync(0xffffffffu, go, 0);
+            iend = __shfl_sync(0xffffffffu, iend, 0);
+            if (!go) break;
+            __syncwarp();                       // rot, d, e written by lane 0 are visible
+            for (int k = lane; k < n; k += 32)
+                for (int i = m - 1; i >= iend; i--) {
+                    const double c = rot[2 * i], sn = rot[2 * i + 1];
+                    const double fz = Z[k * n + i + 1];
+                    Z[k * n + i + 1] = sn * Z[k * n + i] + c * fz;
+                    Z[k * n + i] = c * Z[k * n + i] - sn * fz;
+                }
             __syncwarp();
         }
     }
@@ -519,13 +530,13 @@ __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const double *__restr
     const int lane = threadIdx.x;
     int mr = lz[r].done ? lz[r].m : m;
     if (mr <= 0) return;
-    double *d = sm, *e = sm + LZ_KMAX, *Z = sm + 2 * LZ_KMAX;
+    double *d = sm, *e = sm + LZ_KMAX, *Z = sm + 2 * LZ_KMAX, *rot = Z + LZ_KMAX * LZ_KMAX;
     for (int i = lane; i < mr; i += 32) {
         d[i] = alpha[(long)LZ_KMAX * r + i];
         e[i] = (i < mr - 1) ? betad[(long)LZ_KMAX * r + i] : 0.0;
     }
     __syncwarp();
-    warp_tql(d, e, Z, mr);
+    warp_tql(d, e, Z, rot, mr);
     __syncwarp();
     double *g = gbuf + (long)(LZ_KMAX + 1) * r;   // g[0..m-1], g[LZ_KMAX] = |g|^2 of previous
     double diff2 = 0, nrm2 = 0;
@@ -601,7 +612,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     ::ps_launch_count++, k_lz_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, V, z, lz, nrm2);
     PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
     const int check = 8;   // convergence test every 8 vectors; the cap is handled after the loop
-    size_t smem = sizeof(double) * (2 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
+    size_t smem = sizeof(double) * (4 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
     std::vector<LzScal> hl(E.R);
     int j = 0;
     for (j = 0; j < kmax; j++) {
@@ -767,7 +778,7 @@ __global__ void k_sl_finish(const Seg *__restrict__ segs, const int *__restrict_
                             const double *__restrict__ ab, SlScal *__restrict__ sc, const double *__restrict__ fb,
                             const double *__restrict__ ymcm, double *__restrict__ W)
 {
-    __shared__ double d[SL_KMAX], e[SL_KMAX], Z[SL_KMAX * SL_KMAX], g[SL_KMAX];
+    __shared__ double d[SL_KMAX], e[SL_KMAX], Z[SL_KMAX * SL_KMAX], g[SL_KMAX], rot[2 * SL_KMAX];
     const int slot = blockIdx.x, r = reps[slot];
     const Seg &s = segs[r];
     const int n = s.nc11, m = sc[slot].m;
@@ -777,7 +788,7 @@ __global__ void k_sl_finish(const Seg *__restrict__ segs, const int *__restrict_
     if (m > 0 && threadIdx.x < 32) {
         for (int i = threadIdx.x; i < m; i += 32) { d[i] = alpha[i]; e[i] = (i < m - 1) ? betad[i] : 0.0; }
         __syncwarp();
-        warp_tql(d, e, Z, m);
+        warp_tql(d, e, Z, rot, m);
         __syncwarp();
         int nneg = 0;
         for (int i = threadIdx.x; i < m; i += 32) {

@@ -79,16 +79,18 @@ __device__ inline void lub_pair_geom(const Seg &s, const double *__restrict__ x,
     lub_scalars(tab, nrow, rr / a, f);
 }
 
-// the entries of the pair block that depend on the component pair (p, qq); the
-// block is zero elsewhere (nd = 6 for monomer pairs: A blocks only)
-__device__ __forceinline__ void lub_pair_entries(const double d[3], const double f[10], double a, bool mono, int p,
-                                                 int qq, double *Rm)
+// the entries of a pair block that depend on the component pair (p, qq), from
+// its ten coefficients g (A11 along/across d, A12 along/across, the rotation-
+// translation couplings B11 = g4 E and B12 = g5 E with E v = v x d, C11 and
+// C12 along/across); the block is zero elsewhere (nd = 6 for monomer pairs:
+// A blocks only)
+__device__ __forceinline__ void pair_block_entries(const double d[3], const double g[10], bool mono, int p, int qq,
+                                                   double *Rm)
 {
-    const double sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
     const int nd = mono ? 6 : 12;
     {
         double dd = d[p] * d[qq], id = (p == qq) - dd;
-        double a11 = sa * (f[0] * dd + f[2] * id), a12 = sa * (f[1] * dd + f[3] * id);
+        double a11 = g[0] * dd + g[2] * id, a12 = g[1] * dd + g[3] * id;
         Rm[(0 + p) * nd + 0 + qq] = a11; Rm[(3 + p) * nd + 3 + qq] = a11;
         Rm[(0 + p) * nd + 3 + qq] = a12; Rm[(3 + p) * nd + 0 + qq] = a12;
     }
@@ -96,15 +98,72 @@ __device__ __forceinline__ void lub_pair_entries(const double d[3], const double
     int k3 = 3 - p - qq;
     double ed = 0.0;
     if (p != qq && k3 >= 0 && k3 < 3) ed = (((p - qq + 3) % 3) == 2 ? 1.0 : -1.0) * d[k3];
-    double b11 = sb * f[4] * ed, b12 = sb * f[5] * ed, b21 = -b12, b22 = -b11;
+    double b11 = g[4] * ed, b12 = g[5] * ed, b21 = -b12, b22 = -b11;
     Rm[(6 + p) * nd + 0 + qq] = b11; Rm[(6 + p) * nd + 3 + qq] = b12;
     Rm[(9 + p) * nd + 0 + qq] = b21; Rm[(9 + p) * nd + 3 + qq] = b22;
     Rm[(0 + qq) * nd + 6 + p] = b11; Rm[(3 + qq) * nd + 6 + p] = b12;
     Rm[(0 + qq) * nd + 9 + p] = b21; Rm[(3 + qq) * nd + 9 + p] = b22;
     double dd = d[p] * d[qq], id = (p == qq) - dd;
-    double c11 = sc * (f[6] * dd + f[8] * id), c12 = sc * (f[7] * dd + f[9] * id);
+    double c11 = g[6] * dd + g[8] * id, c12 = g[7] * dd + g[9] * id;
     Rm[(6 + p) * nd + 6 + qq] = c11; Rm[(9 + p) * nd + 9 + qq] = c11;
     Rm[(6 + p) * nd + 9 + qq] = c12; Rm[(9 + p) * nd + 6 + qq] = c12;
+}
+
+// the lubrication pair block's coefficients: the table scalars with the
+// prefactors a (A), (2/3) a^2 (B) and (4/3) a^3 (C)
+__device__ __forceinline__ void lub_pair_coeffs(const double f[10], double a, double g[10])
+{
+    const double sa = a, sb = (2.0 / 3.0) * a * a, sc = (4.0 / 3.0) * a * a * a;
+    for (int k = 0; k < 4; k++) g[k] = sa * f[k];
+    g[4] = sb * f[4]; g[5] = sb * f[5];
+    for (int k = 6; k < 10; k++) g[k] = sc * f[k];
+}
+
+__device__ __forceinline__ void lub_pair_entries(const double d[3], const double f[10], double a, bool mono, int p,
+                                                 int qq, double *Rm)
+{
+    double g[10];
+    lub_pair_coeffs(f, a, g);
+    pair_block_entries(d, g, mono, p, qq, Rm);
+}
+
+// square root (eigenvalues floored at 0) of the symmetric 2 x 2 [[a, b], [b, c]]
+// by one Jacobi rotation: returns its entries tt, tr, rr
+__device__ __forceinline__ void sqrt_sym2(double a, double b, double c, double &tt, double &tr, double &rr)
+{
+    if (fabs(b) < 1e-300) { tt = a > 0 ? sqrt(a) : 0.0; tr = 0.0; rr = c > 0 ? sqrt(c) : 0.0; return; }
+    const double theta = (c - a) / (2 * b);
+    const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+    const double co = 1 / sqrt(t * t + 1), sn = t * co;
+    const double l1 = a - t * b, l2 = c + t * b;
+    const double s1 = l1 > 0 ? sqrt(l1) : 0.0, s2 = l2 > 0 ? sqrt(l2) : 0.0;
+    tt = co * co * s1 + sn * sn * s2;
+    tr = -co * sn * s1 + sn * co * s2;
+    rr = sn * sn * s1 + co * co * s2;
+}
+
+// Coefficients (placement of pair_block_entries) of K^{1/2}, K a colloid pair
+// block with coefficients k (eigenvalues floored at 0), in closed form.  K
+// commutes with the exchange of the two colloids (d -> -d) and with rotations
+// about d: in the basis [U_lo + U_hi, W_lo - W_hi] / sqrt2 (block I) and
+// [U_lo - U_hi, W_lo + W_hi] / sqrt2 (block II) it splits into two 6 x 6 blocks,
+// each with one eigenvalue for translation along d, one for rotation along d,
+// and a doubly degenerate 2 x 2 block [[a_perp, b], [b, c_perp]] that couples
+// translation along e1 to rotation along e1 x d.  The square root keeps that
+// structure, so it has coefficients of the same kind.
+__device__ inline void colloid_pair_sqrt_coeffs(const double k[10], double g[10])
+{
+    auto sq = [](double v) { return v > 0 ? sqrt(v) : 0.0; };
+    const double aIp = k[0] + k[1], aIIp = k[0] - k[1];        // translation along d
+    const double cIp = k[6] - k[7], cIIp = k[6] + k[7];        // rotation along d
+    double ttI, trI, rrI, ttII, trII, rrII;
+    sqrt_sym2(k[2] + k[3], k[4] + k[5], k[8] - k[9], ttI, trI, rrI);
+    sqrt_sym2(k[2] - k[3], k[4] - k[5], k[8] + k[9], ttII, trII, rrII);
+    g[0] = 0.5 * (sq(aIp) + sq(aIIp)); g[1] = 0.5 * (sq(aIp) - sq(aIIp));
+    g[2] = 0.5 * (ttI + ttII); g[3] = 0.5 * (ttI - ttII);
+    g[4] = 0.5 * (trI + trII); g[5] = 0.5 * (trI - trII);
+    g[6] = 0.5 * (sq(cIIp) + sq(cIp)); g[7] = 0.5 * (sq(cIIp) - sq(cIp));
+    g[8] = 0.5 * (rrII + rrI); g[9] = 0.5 * (rrII - rrI);
 }
 
 __device__ inline void lub_pair_block(const Seg &s, const double *__restrict__ x, const double *__restrict__ tab, int nrow,

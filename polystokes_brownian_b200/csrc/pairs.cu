@@ -112,11 +112,10 @@ __device__ __forceinline__ void partners(const Seg &s, int r, long b, const doub
                     }
                 }
     }
-    if (which != 1 && !(which >= 2 && i < s.Nm)) {
-        // colloid partners (all colloids follow all monomers); lubrication pairs
-        // are equal-radius, so monomers have no colloid partners there
-        int c0 = (which == 3) ? 0 : (i < s.Nm ? 0 : i - s.Nm + 1);
-        for (int c = c0; c < s.Nc; c++) {
+    if (which == 0 && i < s.Nm) {
+        // a monomer's colloid partners (all colloids follow all monomers);
+        // lubrication pairs are equal-radius, so monomers have none there
+        for (int c = 0; c < s.Nc; c++) {
             long j = (long)s.bead_off + s.Nm + c;
             bool take = (which == 3) ? (j != b) : (j > b);
             if (take && in_list(s, x, b, j, which, geo + 20 * r + 10)) f(j);
@@ -124,14 +123,51 @@ __device__ __forceinline__ void partners(const Seg &s, int r, long b, const doub
     }
 }
 
+// A colloid's partners are colloids only (monomer-colloid pairs belong to the
+// monomer): one warp per colloid scans the replica's colloids 32 at a time and a
+// ballot hands each partner its rank, so the list comes out in ascending order.
+template <class F>
+__device__ __forceinline__ int colloid_partners_warp(const Seg &s, int r, long b, const double *__restrict__ x,
+                                                     const double *__restrict__ geo, int which, int lane, F f)
+{
+    int n = 0;
+    if (which == 1) return 0;
+    const int i = (int)(b - s.bead_off);
+    const int c0 = (which == 3) ? 0 : i - s.Nm + 1;
+    for (int cb = c0; cb < s.Nc; cb += 32) {
+        const int c = cb + lane;
+        const long j = (long)s.bead_off + s.Nm + c;
+        const bool hit = c < s.Nc && ((which == 3) ? (j != b) : (j > b)) && in_list(s, x, b, j, which, geo + 20 * r + 10);
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) f(j, n + __popc(m & ((1u << lane) - 1u)));
+        n += __popc(m);
+    }
+    return n;
+}
+
+// Monomers: one thread each (cell-list stencil, then the colloids); colloids:
+// one warp each in the blocks past the bead blocks.
 __global__ void k_pairs_count(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                               const double *__restrict__ x, const double *__restrict__ geo,
                               const long *__restrict__ cell_off, const int *__restrict__ cstart,
-                              const int *__restrict__ csorted, int which, int *__restrict__ cnt)
+                              const int *__restrict__ csorted, long ncoll, const int *__restrict__ coll_rep,
+                              int which, int *__restrict__ cnt)
 {
+    const long nbb = (ntot + blockDim.x - 1) / blockDim.x;
+    if (blockIdx.x >= nbb) {
+        const long c = (long)(blockIdx.x - nbb) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (c >= ncoll) return;
+        const int lane = threadIdx.x & 31, r = coll_rep[c];
+        const Seg &s = segs[r];
+        const long b = s.bead_off + s.Nm + (c - s.coll_off);
+        const int n = colloid_partners_warp(s, r, b, x, geo, which, lane, [&](long, int) {});
+        if (lane == 0) cnt[b] = n;
+        return;
+    }
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int r = rep_find(bead_offs, R, b);
+    if (b - segs[r].bead_off >= segs[r].Nm) return;
     int n = 0;
     partners(segs[r], r, b, x, geo, cell_off, cstart, csorted, which, [&](long) { n++; });
     cnt[b] = n;
@@ -140,12 +176,24 @@ __global__ void k_pairs_count(long ntot, const int *__restrict__ bead_offs, int 
 __global__ void k_pairs_fill(long ntot, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                              const double *__restrict__ x, const double *__restrict__ geo,
                              const long *__restrict__ cell_off, const int *__restrict__ cstart,
-                             const int *__restrict__ csorted, int which, const int *__restrict__ ptr,
-                             int *__restrict__ nbr)
+                             const int *__restrict__ csorted, long ncoll, const int *__restrict__ coll_rep, int which,
+                             const int *__restrict__ ptr, int *__restrict__ nbr)
 {
+    const long nbb = (ntot + blockDim.x - 1) / blockDim.x;
+    if (blockIdx.x >= nbb) {
+        const long c = (long)(blockIdx.x - nbb) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (c >= ncoll) return;
+        const int lane = threadIdx.x & 31, r = coll_rep[c];
+        const Seg &s = segs[r];
+        const long b = s.bead_off + s.Nm + (c - s.coll_off);
+        const int a = ptr[b];
+        colloid_partners_warp(s, r, b, x, geo, which, lane, [&](long j, int k) { nbr[a + k] = (int)j; });
+        return;
+    }
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int r = rep_find(bead_offs, R, b);
+    if (b - segs[r].bead_off >= segs[r].Nm) return;
     int a = ptr[b], n = 0;
     partners(segs[r], r, b, x, geo, cell_off, cstart, csorted, which, [&](long j) { nbr[a + n++] = (int)j; });
     // ascending partner order
@@ -264,9 +312,9 @@ __global__ void k_pairs_expand(long ntot, const int *__restrict__ ptr, const int
 int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
 {
     int thr = 128;
-    unsigned nbk = (unsigned)((E.ntot + thr - 1) / thr);
+    unsigned nbk = (unsigned)((E.ntot + thr - 1) / thr + (E.ncoll + thr / 32 - 1) / (thr / 32));
     ::ps_launch_count++, k_pairs_count<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
-                                       E.d_cell_start, E.d_cell_sorted, which, E.d_nbr_count);
+                                       E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_count);
     int rc = exclusive_scan(E, E.d_nbr_count, E.d_nbr_ptr, E.ntot, st);
     if (rc) return rc;
     int tot = 0;
@@ -278,7 +326,7 @@ int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
         PS_CK(cudaMalloc(&E.d_nbr, sizeof(int) * E.nbr_cap));
     }
     ::ps_launch_count++, k_pairs_fill<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
-                                      E.d_cell_start, E.d_cell_sorted, which, E.d_nbr_ptr, E.d_nbr);
+                                      E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_ptr, E.d_nbr);
     PS_CK(cudaGetLastError());
     *npairs = tot;
     return PS_OK;

@@ -155,6 +155,7 @@ struct Engine {
     double *d_drift = nullptr, *d_sb = nullptr, *d_fext = nullptr, *d_fb = nullptr, *d_wr = nullptr;
     double *d_tmp_top = nullptr, *d_tmp_top2 = nullptr;
     double *d_ref_r = nullptr, *d_ref_d = nullptr;   // iterative refinement: residual, correction (allocated on first use)
+    int *d_pm_cnt = nullptr;                         // pair-space MINRES: items finished per replica (first use)
     uint64_t seed = 12345, step_counter = 0;
     uint64_t *d_rseed = nullptr, *d_rstep = nullptr;   // per-replica Philox key and step counter
 

@@ -356,89 +356,28 @@ __device__ void pair_mobility(const Seg &s, const double *__restrict__ x, const 
         }
 }
 
-// Parallel-ordered Jacobi eigen-decomposition of a symmetric 12 x 12 matrix
-// in shared memory by one warp: each sweep is 11 rounds of 6 disjoint
-// rotations (the circle schedule: (r, 11) and (r + i, r - i) mod 11, i = 1..5),
-// whose angles depend only on their own 2 x 2 blocks, so a round equals its six
-// rotations applied one after another; each rotation is the one of jacobi_eig
-// (same angle, same stopping test at the start of a sweep).  On return A holds
-// the eigenvalues on its diagonal and Q the eigenvectors (columns).
+// shared-memory scratch of one warp for one colloid pair
 struct PsWarpSmem {
     double K[144], Q[144], S[144], M[144];
-    double cs[12];
-    int pq[12];
 };
 
-__device__ void warp_jacobi12(double *A, double *Q, double *cs, int *pq, int lane)
-{
-    for (int t = lane; t < 144; t += 32) Q[t] = (t / 12 == t % 12) ? 1.0 : 0.0;
-    __syncwarp();
-    for (int sweep = 0; sweep < 40; sweep++) {
-        double off = 0.0, tot = 0.0;
-        for (int t = lane; t < 144; t += 32) {
-            const double v = A[t] * A[t];
-            tot += v;
-            if (t / 12 != t % 12) off += v;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            off += __shfl_xor_sync(0xffffffffu, off, o);
-            tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        }
-        if (off <= 1e-30 * tot || off == 0.0) break;
-        for (int rnd = 0; rnd < 11; rnd++) {
-            if (lane < 6) {
-                int p = lane == 0 ? rnd : (rnd + lane) % 11, q = lane == 0 ? 11 : (rnd - lane + 11) % 11;
-                if (p > q) { const int t = p; p = q; q = t; }
-                const double apq = A[p * 12 + q];
-                double c = 1.0, sn = 0.0;
-                if (fabs(apq) >= 1e-300) {
-                    const double theta = (A[q * 12 + q] - A[p * 12 + p]) / (2 * apq);
-                    const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-                    c = 1 / sqrt(t * t + 1);
-                    sn = t * c;
-                }
-                cs[lane] = c; cs[6 + lane] = sn; pq[lane] = p; pq[6 + lane] = q;
-            }
-            __syncwarp();
-            for (int t = lane; t < 72; t += 32) {          // A <- A J (columns p, q of every row)
-                const int i = t / 12, k = t % 12, p = pq[i], q = pq[6 + i];
-                const double c = cs[i], sn = cs[6 + i], akp = A[k * 12 + p], akq = A[k * 12 + q];
-                A[k * 12 + p] = c * akp - sn * akq;
-                A[k * 12 + q] = sn * akp + c * akq;
-            }
-            __syncwarp();
-            for (int t = lane; t < 72; t += 32) {          // A <- J^T A (rows p, q), Q <- Q J
-                const int i = t / 12, k = t % 12, p = pq[i], q = pq[6 + i];
-                const double c = cs[i], sn = cs[6 + i];
-                const double apk = A[p * 12 + k], aqk = A[q * 12 + k];
-                A[p * 12 + k] = c * apk - sn * aqk;
-                A[q * 12 + k] = sn * apk + c * aqk;
-                const double qkp = Q[k * 12 + p], qkq = Q[k * 12 + q];
-                Q[k * 12 + p] = c * qkp - sn * qkq;
-                Q[k * 12 + q] = sn * qkp + c * qkq;
-            }
-            __syncwarp();
-        }
-    }
-    __syncwarp();
-}
-
-// One colloid pair (lo, hi) by one warp: K = R_lub pair block, S = K^{1/2}
-// (eigenvalues floored at 0), M = two-body FT far-field mobility (symmetrised),
-// P = (I + S M S)^{-1} by Cholesky, identity if not positive definite.  The
-// arithmetic per entry is that of the serial form: every sum runs over k in
-// ascending order.
+// One colloid pair (lo, hi) by one warp: S = K^{1/2} of the R_lub pair block in
+// closed form (colloid_pair_sqrt_coeffs), M = two-body FT far-field mobility
+// (symmetrised), P = (I + S M S)^{-1} by Cholesky, identity if not positive
+// definite.  Every matrix-product entry sums over k in ascending order.
 __device__ void ps_setup_colloid_pair(const Seg &s, long lo, long hi, const double *__restrict__ x,
                                       const double *__restrict__ tab, int nrow, double *__restrict__ So,
                                       double *__restrict__ Po, PsWarpSmem &w, int lane)
 {
     double *K = w.K, *Q = w.Q, *S = w.S, *M = w.M;
-    for (int t = lane; t < 144; t += 32) { K[t] = 0.0; M[t] = 0.0; }
+    for (int t = lane; t < 144; t += 32) { S[t] = 0.0; M[t] = 0.0; }
     __syncwarp();
     {
-        double d[3], f[10];
+        double d[3], f[10], kc[10], g[10];
         lub_pair_geom(s, x, tab, nrow, lo, hi, 1.0, d, f);
-        if (lane < 9) lub_pair_entries(d, f, 1.0, false, lane / 3, lane % 3, K);
+        lub_pair_coeffs(f, 1.0, kc);
+        colloid_pair_sqrt_coeffs(kc, g);
+        if (lane < 9) pair_block_entries(d, g, false, lane / 3, lane % 3, S);
     }
     if (lane < 12) {
         // the partner's (F, T) column -> this bead's (U, W) rows, e = (x_lo - x_hi)/r as in the BB kernel
@@ -463,16 +402,6 @@ __device__ void ps_setup_colloid_pair(const Seg &s, long lo, long hi, const doub
             const double v = 0.5 * (M[a * 12 + c] + M[c * 12 + a]);
             M[a * 12 + c] = v; M[c * 12 + a] = v;
         }
-    }
-    warp_jacobi12(K, Q, w.cs, w.pq, lane);
-    for (int t = lane; t < 144; t += 32) {
-        const int a = t / 12, c = t % 12;
-        double v = 0.0;
-        for (int k = 0; k < 12; k++) {
-            const double lam = K[k * 12 + k];
-            v += Q[a * 12 + k] * (lam > 0 ? sqrt(lam) : 0.0) * Q[c * 12 + k];
-        }
-        S[t] = v;
     }
     __syncwarp();
     for (int t = lane; t < 144; t += 32) {          // K <- M S
@@ -1014,7 +943,7 @@ __device__ __forceinline__ void s_precond(const double r[5], double z[5])
 // MINRES element work of pair t by a team of LT_LANES lanes, lane a owning entry a
 // of the pair vectors (a < 12); the partial dots join over the team by a fixed
 // butterfly.  mode as k_pm_elem.
-__device__ __forceinline__ void pm_pair_team(long t, int a, unsigned team, const int2 *__restrict__ pairs,
+__device__ __forceinline__ int pm_pair_team(long t, int a, unsigned team, const int2 *__restrict__ pairs,
                                              const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                                              const MinresScal *__restrict__ mr, int mode, int k, const PMArgs &A)
 {
@@ -1074,137 +1003,35 @@ __device__ __forceinline__ void pm_pair_team(long t, int a, unsigned team, const
         }
         if (a == 0) { A.part[t] = dot0; A.part2[t] = dot1; }
     }
+    return r;
 }
 
-// Teams of LT_LANES lanes per pair (global thread < npair * LT_LANES), then one
-// thread per bead (stresslet entries of joint-replica colloids, nothing for
-// other beads).
-// mode 0 init, 1 alpha (pending w/x update, v = z/beta, Av), 2 beta (r_{k+1}, z = P r), 3 flush
-__global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs,
-                          int R, const Seg *__restrict__ segs, const MinresScal *__restrict__ mr, int mode, int k,
-                          PMArgs A)
+// Per-replica MINRES scalar recurrences from the replica's totals t0, t1 (the
+// sums of the pair and bead partials of k_pm_elem); mode 0 init, 1 alpha, 2 beta.
+__device__ void pm_scalars(MinresScal *mr, int r, int mode, double t0, double t1, int maxit, double rtol,
+                           int *nactive)
 {
-    const long gt = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long npt = npair * LT_LANES;
-    if (gt < npt) {
-        pm_pair_team(gt / LT_LANES, threadIdx.x % LT_LANES, 0xffffu << (threadIdx.x & 16), pairs, bead_offs, R, segs,
-                     mr, mode, k, A);
-        return;
-    }
-    const long bead = gt - npt;
-    if (bead >= ntot) return;
-    const int r = rep_of_b(bead_offs, R, bead);
-    const Seg &s0 = segs[r];
-    const int i = (int)(bead - s0.bead_off);
-    if (!(s0.Nc > 0 && s0.ss_off < 0 && i >= s0.Nm)) {
-        if (mode <= 2) { A.sA[bead] = 0.0; A.sB[bead] = 0.0; }
-        return;
-    }
-    const long base = (long)s0.top_off + s0.nm3nc6 + 5 * (i - s0.Nm);
-    const int n = 5;
-    double *u_s = A.u + base;
-    const double *y_s = A.y + base;
-    const MinresScal m = mr[r];
-    auto V = [&](const PMVec &p) { return p.s + base; };
-    double dot0 = 0.0, dot1 = 0.0;
-    if (mode == 0) {
-        double rv[5], zv[5];
-        double *rr = V(A.R[1]);
-        for (int a = 0; a < n; a++) rv[a] = rr[a];
-        s_precond(rv, zv);
-        double *zz = V(A.z), *xx = V(A.x), *vv = V(A.v), *w0 = V(A.W[0]), *w1 = V(A.W[1]), *w2 = V(A.W[2]);
-        for (int a = 0; a < n; a++) {
-            zz[a] = zv[a]; xx[a] = 0.0; vv[a] = 0.0; w0[a] = 0.0; w1[a] = 0.0; w2[a] = 0.0;
-            dot0 += rv[a] * zv[a];
-            dot1 += zv[a] * zv[a];
-            u_s[a] = zv[a];
-        }
-    } else if (mode == 1 || mode == 3) {
-        double *vv = V(A.v);
-        if (m.pending) {
-            double *wn = V(A.W[(k + 2) % 3]);
-            const double *w1 = V(A.W[k % 3]), *w2 = V(A.W[(k + 1) % 3]);
-            double *xx = V(A.x);
-            for (int a = 0; a < n; a++) {
-                double w = (vv[a] - m.up_oldeps * w1[a] - m.up_delta * w2[a]) * m.up_ginv;
-                wn[a] = w;
-                xx[a] += m.up_phi * w;
-            }
-        }
-        if (mode == 1 && !m.done) {
-            const double *zz = V(A.z);
-            double *av = V(A.R[(k + 1) % 3]);
-            const double *rm1 = V(A.R[(k + 2) % 3]);
-            const double c1 = (k >= 2) ? m.beta / m.oldb : 0.0;
-            for (int a = 0; a < n; a++) {
-                double vq = zz[a] * m.sinv;
-                double x = m.sinv * y_s[a];
-                if (k >= 2) x -= c1 * rm1[a];
-                vv[a] = vq;
-                av[a] = x;
-                dot0 += vq * x;
-            }
-        }
-    } else if (mode == 2 && !m.done) {
-        double *av = V(A.R[(k + 1) % 3]);
-        const double *rk = V(A.R[k % 3]);
-        const double c2 = m.alfa / m.beta;
-        double rv[5], zv[5];
-        for (int a = 0; a < n; a++) { rv[a] = av[a] - c2 * rk[a]; av[a] = rv[a]; }
-        s_precond(rv, zv);
-        double *zz = V(A.z);
-        for (int a = 0; a < n; a++) {
-            zz[a] = zv[a];
-            dot0 += rv[a] * zv[a];
-            u_s[a] = zv[a];
-        }
-    }
-    if (mode <= 2) { A.sA[bead] = dot0; A.sB[bead] = dot1; }
-}
-
-// per-replica MINRES scalar updates over the bead table (pair partials by lower bead)
-__global__ void k_pm_reduce(RedTable T, const int *__restrict__ cptr, const double *__restrict__ part,
-                            const double *__restrict__ part2, const double *__restrict__ sA,
-                            const double *__restrict__ sB, MinresScal *mr, int mode, int maxit, double rtol,
-                            int *nactive)
-{
-    __shared__ double sh[RB_THREADS / 32][2];
-    const RBlk B = T.d_blk[blockIdx.x];
-    const MinresScal m0 = mr[B.rep];
+    const MinresScal m0 = mr[r];
     if (mode != 1 && m0.done) return;
     if (mode == 1 && m0.done && !m0.pending) return;
-    double v[2] = {0.0, 0.0};
-    // pairs are stored by lower bead, so the block's beads own one contiguous pair range
-    for (long q = cptr[B.start] + threadIdx.x; q < cptr[B.start + B.len]; q += RB_THREADS) {
-        v[0] += part[q];
-        v[1] += part2[q];
-    }
-    for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
-        long b = B.start + e;
-        v[0] += sA[b];
-        v[1] += sB[b];
-    }
-    block_sum<2>(v, sh);
-    double tot[2];
-    if (!finish_block<2>(T, B, blockIdx.x, v, tot)) return;
     MinresScal m = m0;
     if (mode == 0) {
         m = MinresScal{};
-        double np0 = sqrt(tot[1]);
+        double np0 = sqrt(t1);
         m.np = np0;
         m.ttol = fmax(rtol * np0, 1e-50);
-        if (tot[0] < 0) { m.done = 1; m.reason = -8; }
-        else if (np0 <= m.ttol || tot[0] == 0.0) { m.done = 1; m.reason = 2; }
+        if (t0 < 0) { m.done = 1; m.reason = -8; }
+        else if (np0 <= m.ttol || t0 == 0.0) { m.done = 1; m.reason = 2; }
         else {
-            m.beta = sqrt(tot[0]); m.phibar = m.beta; m.cs = -1; m.sn = 0; m.sinv = 1.0 / m.beta;
+            m.beta = sqrt(t0); m.phibar = m.beta; m.cs = -1; m.sn = 0; m.sinv = 1.0 / m.beta;
         }
         if (m.done) atomicSub(nactive, 1);
     } else if (mode == 1) {
         if (m.pending) m.pending = 0;
-        if (!m.done) m.alfa = tot[0];
+        if (!m.done) m.alfa = t0;
     } else {
         m.it += 1;
-        double bb = tot[0];
+        double bb = t0;
         m.oldb = m.beta;
         if (bb < 0) {
             m.done = 1; m.reason = -8;
@@ -1231,7 +1058,161 @@ __global__ void k_pm_reduce(RedTable T, const int *__restrict__ cptr, const doub
         }
         if (m.done) atomicSub(nactive, 1);
     }
-    mr[B.rep] = m;
+    mr[r] = m;
+}
+
+// In-kernel completion of the per-replica sums: every pair team and every bead
+// thread counts one item of its replica (warp-aggregated atomics after a
+// fence); the block whose count completes replica r sums r's pair partials (a
+// contiguous range, pairs being stored by lower bead) and bead partials in a
+// fixed order -- strided over the block, then a shuffle tree and the warps in
+// order, whichever block finishes -- and runs the scalar recurrence.
+struct PMRed {
+    int *cnt;                  // per replica, zero between launches
+    const int *cptr;           // canonical pair pointer by lower bead
+    int maxit;
+    double rtol;
+    int *nactive;
+};
+
+__device__ void pm_count_and_finish(int myrep, const Seg *__restrict__ segs, const PMArgs &A, const PMRed &red,
+                                    MinresScal *mr, int mode)
+{
+    __shared__ int s_n, s_list[1024];
+    __shared__ double s_sum[32][2];
+    if (threadIdx.x == 0) s_n = 0;
+    __threadfence();
+    __syncthreads();
+    const unsigned valid = __ballot_sync(0xffffffffu, myrep >= 0);
+    if (myrep >= 0) {
+        const unsigned grp = __match_any_sync(valid, myrep);
+        if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) {
+            const Seg &s = segs[myrep];
+            const int total = red.cptr[s.bead_off + s.Np] - red.cptr[s.bead_off] + s.Np;
+            const int n = __popc(grp);
+            if (atomicAdd(&red.cnt[myrep], n) + n == total) s_list[atomicAdd(&s_n, 1)] = myrep;
+        }
+    }
+    __syncthreads();
+    const int nfin = s_n;
+    for (int i = 0; i < nfin; i++) {
+        const int r = s_list[i];
+        __threadfence();
+        const Seg &s = segs[r];
+        double v0 = 0.0, v1 = 0.0;
+        for (long q = red.cptr[s.bead_off] + threadIdx.x; q < red.cptr[s.bead_off + s.Np]; q += blockDim.x) {
+            v0 += __ldcg(A.part + q);
+            v1 += __ldcg(A.part2 + q);
+        }
+        for (long b = s.bead_off + threadIdx.x; b < (long)s.bead_off + s.Np; b += blockDim.x) {
+            v0 += __ldcg(A.sA + b);
+            v1 += __ldcg(A.sB + b);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            v0 += __shfl_down_sync(0xffffffffu, v0, o);
+            v1 += __shfl_down_sync(0xffffffffu, v1, o);
+        }
+        if ((threadIdx.x & 31) == 0) { s_sum[threadIdx.x >> 5][0] = v0; s_sum[threadIdx.x >> 5][1] = v1; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t0 = 0.0, t1 = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) { t0 += s_sum[w][0]; t1 += s_sum[w][1]; }
+            pm_scalars(mr, r, mode, t0, t1, red.maxit, red.rtol, red.nactive);
+            red.cnt[r] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Teams of LT_LANES lanes per pair (global thread < npair * LT_LANES), then one
+// thread per bead (stresslet entries of joint-replica colloids, nothing for
+// other beads); modes 0..2 finish their replica sums in the same launch
+// (pm_count_and_finish).  No thread leaves early: every thread reaches the
+// block barriers of the finish.
+// mode 0 init, 1 alpha (pending w/x update, v = z/beta, Av), 2 beta (r_{k+1}, z = P r), 3 flush
+__global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs,
+                          int R, const Seg *__restrict__ segs, MinresScal *mr, int mode, int k, PMArgs A, PMRed red)
+{
+    const long gt = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long npt = npair * LT_LANES;
+    int myrep = -1;                                   // replica of the item this thread counts
+    if (gt < npt) {
+        const int a = threadIdx.x % LT_LANES;
+        const int r = pm_pair_team(gt / LT_LANES, a, 0xffffu << (threadIdx.x & 16), pairs, bead_offs, R, segs, mr,
+                                   mode, k, A);
+        if (a == 0) myrep = r;
+    } else if (gt - npt < ntot) {
+        const long bead = gt - npt;
+        const int r = rep_of_b(bead_offs, R, bead);
+        myrep = r;
+        const Seg &s0 = segs[r];
+        const int i = (int)(bead - s0.bead_off);
+        if (!(s0.Nc > 0 && s0.ss_off < 0 && i >= s0.Nm)) {
+            if (mode <= 2) { A.sA[bead] = 0.0; A.sB[bead] = 0.0; }
+        } else {
+            const long base = (long)s0.top_off + s0.nm3nc6 + 5 * (i - s0.Nm);
+            const int n = 5;
+            double *u_s = A.u + base;
+            const double *y_s = A.y + base;
+            const MinresScal m = mr[r];
+            auto V = [&](const PMVec &p) { return p.s + base; };
+            double dot0 = 0.0, dot1 = 0.0;
+            if (mode == 0) {
+                double rv[5], zv[5];
+                double *rr = V(A.R[1]);
+                for (int a = 0; a < n; a++) rv[a] = rr[a];
+                s_precond(rv, zv);
+                double *zz = V(A.z), *xx = V(A.x), *vv = V(A.v), *w0 = V(A.W[0]), *w1 = V(A.W[1]), *w2 = V(A.W[2]);
+                for (int a = 0; a < n; a++) {
+                    zz[a] = zv[a]; xx[a] = 0.0; vv[a] = 0.0; w0[a] = 0.0; w1[a] = 0.0; w2[a] = 0.0;
+                    dot0 += rv[a] * zv[a];
+                    dot1 += zv[a] * zv[a];
+                    u_s[a] = zv[a];
+                }
+            } else if (mode == 1 || mode == 3) {
+                double *vv = V(A.v);
+                if (m.pending) {
+                    double *wn = V(A.W[(k + 2) % 3]);
+                    const double *w1 = V(A.W[k % 3]), *w2 = V(A.W[(k + 1) % 3]);
+                    double *xx = V(A.x);
+                    for (int a = 0; a < n; a++) {
+                        double w = (vv[a] - m.up_oldeps * w1[a] - m.up_delta * w2[a]) * m.up_ginv;
+                        wn[a] = w;
+                        xx[a] += m.up_phi * w;
+                    }
+                }
+                if (mode == 1 && !m.done) {
+                    const double *zz = V(A.z);
+                    double *av = V(A.R[(k + 1) % 3]);
+                    const double *rm1 = V(A.R[(k + 2) % 3]);
+                    const double c1 = (k >= 2) ? m.beta / m.oldb : 0.0;
+                    for (int a = 0; a < n; a++) {
+                        double vq = zz[a] * m.sinv;
+                        double x = m.sinv * y_s[a];
+                        if (k >= 2) x -= c1 * rm1[a];
+                        vv[a] = vq;
+                        av[a] = x;
+                        dot0 += vq * x;
+                    }
+                }
+            } else if (mode == 2 && !m.done) {
+                double *av = V(A.R[(k + 1) % 3]);
+                const double *rk = V(A.R[k % 3]);
+                const double c2 = m.alfa / m.beta;
+                double rv[5], zv[5];
+                for (int a = 0; a < n; a++) { rv[a] = av[a] - c2 * rk[a]; av[a] = rv[a]; }
+                s_precond(rv, zv);
+                double *zz = V(A.z);
+                for (int a = 0; a < n; a++) {
+                    zz[a] = zv[a];
+                    dot0 += rv[a] * zv[a];
+                    u_s[a] = zv[a];
+                }
+            }
+            if (mode <= 2) { A.sA[bead] = dot0; A.sB[bead] = dot1; }
+        }
+    }
+    if (mode <= 2) pm_count_and_finish(myrep, segs, A, red, mr, mode);
 }
 
 static int ensure_pair_space(Engine &E)
@@ -1258,7 +1239,6 @@ static int ensure_pair_space(Engine &E)
 static int pair_minres(Engine &E, const double *b, const double *g, int maxit, double rtol, bool fp32,
                        cudaStream_t st, double **ysol, double **ssol, int *iters)
 {
-    RedTable &TB = E.red_bead;
     const long npair = E.lub_npairs;
     const int thr = 128;
     const unsigned nbp = (unsigned)((std::max<long>(npair, 1) + PS_THREADS - 1) / PS_THREADS);
@@ -1280,6 +1260,11 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     A.part = E.d_ppart; A.part2 = E.d_ppart2;
     A.sA = E.d_sbead[0]; A.sB = E.d_sbead[1];
     PS_CK(cudaMemsetAsync(E.d_pmr, 0, sizeof(MinresScal) * E.R, st));
+    if (!E.d_pm_cnt) {
+        PS_CK(cudaMalloc(&E.d_pm_cnt, sizeof(int) * E.R));
+        PS_CK(cudaMemsetAsync(E.d_pm_cnt, 0, sizeof(int) * E.R, st));
+    }
+    const PMRed red = {E.d_pm_cnt, E.d_lubc_ptr, maxit, rtol, E.d_nactive};
     // rhs into R[1]: pairs L^T (g + Mr b_bot), stresslets b_S + (M b_bot)_S
     mr_apply(E, fp32, dn, ds, st);
     if (npair)
@@ -1292,9 +1277,7 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     *E.h_nactive = E.R;
     PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
     ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                     E.d_pmr, 0, 0, A);
-    ::ps_launch_count++, k_pm_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, A.part, A.part2, A.sA, A.sB,
-                                                                  E.d_pmr, 0, maxit, rtol, E.d_nactive);
+                                                     E.d_pmr, 0, 0, A, red);
     PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
     int nact = *E.h_nactive, k = 0;
@@ -1309,13 +1292,9 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
                                                                       E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
                                                                       A.z.pair, E.d_pmp[9], nullptr, dn, ds);
             ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                             E.d_segs, E.d_pmr, 1, k, A);
-            ::ps_launch_count++, k_pm_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, A.part, A.part2, A.sA,
-                                                                          A.sB, E.d_pmr, 1, maxit, rtol, E.d_nactive);
+                                                             E.d_segs, E.d_pmr, 1, k, A, red);
             ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                             E.d_segs, E.d_pmr, 2, k, A);
-            ::ps_launch_count++, k_pm_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, A.part, A.part2, A.sA,
-                                                                          A.sB, E.d_pmr, 2, maxit, rtol, E.d_nactive);
+                                                             E.d_segs, E.d_pmr, 2, k, A, red);
         }
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
@@ -1323,7 +1302,7 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     }
     // the last pending w/x update
     ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                     E.d_pmr, 3, k + 1, A);
+                                                     E.d_pmr, 3, k + 1, A, red);
     PS_CK(cudaGetLastError());
     *ysol = A.x.pair;
     *ssol = A.x.s;
