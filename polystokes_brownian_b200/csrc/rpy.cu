@@ -496,9 +496,14 @@ k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
 }
 
 // ---------------------------------------------------------------------------
-// BB: colloid rows x colloid columns (FTS, 11 -> 11).
+// BB: colloid rows x colloid columns (FTS, 11 -> 11).  BB_SPLIT threads per row
+// (a block is BB_SPLIT x RPY_THREADS threads): thread group h takes the tile
+// columns h, h + BB_SPLIT, ...; the groups' sums are joined in group order in
+// shared memory, so a replica of a thousand colloids fills the SMs without
+// more chunk partials.
+constexpr int BB_SPLIT = 2;
 template <class T>
-__global__ void __launch_bounds__(RPY_THREADS)
+__global__ void __launch_bounds__(RPY_THREADS * BB_SPLIT)
 k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
          long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
@@ -510,15 +515,17 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
     __shared__ P4 sp[CT];
     __shared__ float4 sl[F32 ? CT : 1];
     __shared__ T su[CT * 11];
+    __shared__ T sred[BB_SPLIT - 1][11][RPY_THREADS];
     const Tile tl = tiles[blockIdx.x];
     const Seg &sg = segs[tl.rep];
     const int c = blockIdx.y;
     nchunk = sg.nch_bb;
     if (c >= nchunk) return;
+    const int row = threadIdx.x % RPY_THREADS, grp = threadIdx.x / RPY_THREADS;
     const int Nc = sg.Nc, Nm = sg.Nm;
     const int j0 = (int)((long)Nc * c / nchunk), j1 = (int)((long)Nc * (c + 1) / nchunk);
-    const int i = tl.row0 + threadIdx.x;
-    const bool active = threadIdx.x < tl.nrow;
+    const int i = tl.row0 + row;
+    const bool active = row < tl.nrow;
     const int uoff = in_top ? sg.top_off : sg.vec_off;
     P4 pi = pos[sg.bead_off + Nm + (active ? i : tl.row0)];
     float4 li = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -538,7 +545,7 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             if constexpr (F32) sl[threadIdx.x] = plo[sg.bead_off + Nm + jt + threadIdx.x];
         }
         __syncthreads();
-        for (int k = 0; k < nj; k++) {
+        for (int k = grp; k < nj; k += BB_SPLIT) {
             int j = jt + k;
             if (j == i) continue;
             P4 pj = sp[k];
@@ -555,7 +562,12 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
             bb_apply<T>(e, r2 * rinv, rinv, lo, su + 11 * k, out);
         }
     }
-    if (active) {
+    if (grp > 0)
+        for (int q = 0; q < 11; q++) sred[grp - 1][q][row] = out[q];
+    __syncthreads();
+    if (grp == 0 && active) {
+        for (int g = 0; g < BB_SPLIT - 1; g++)
+            for (int q = 0; q < 11; q++) out[q] += sred[g][q][row];
         double *o = part + (long)c * part_stride + sg.top_off;
         for (int a = 0; a < 3; a++) {
             o[sg.nm3 + 3 * i + a] = (double)out[a];
@@ -678,7 +690,7 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
     // velocity error on a suspension at gap 0.01 (FP64: tracks rtol); they are
     // cheap wherever monomers carry the O(N^2) work
     if (E.n_bb_tiles)
-        ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(
+        ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, st>>>(
             E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, in_top, E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
 }
 
@@ -741,7 +753,7 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
             if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
             else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
         } else if (which == 2 && E.n_bb_tiles) {
-            ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS, 0, st>>>(E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
+            ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, st>>>(E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
         } else if (which == 3) {
             apply_operator(E, 1, u, E.d_tmp_top2, nullptr, fp32, st);
         }

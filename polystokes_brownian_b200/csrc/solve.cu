@@ -924,8 +924,9 @@ static void mr_apply(Engine &E, bool fp32, const void *dn, int ds, cudaStream_t 
 struct PMVec { double *pair; double *s; };
 struct PMArgs {
     PMVec R[3], W[3], v, z, x;
-    const double *Az;          // operator output, pair storage (S part: y_S of the apply)
-    const double *y;           // the apply's output (mobility layout)
+    const double *y;           // the apply's output (mobility layout; its S part is y_S)
+    const double *y2;          // the dense stresslet block's share of the output (replicas with one)
+    const double *S;           // pair square-root blocks (L = [B_q S_q])
     double *u;                 // the apply's input (mobility layout): its S part gets z_S
     const double *P;           // pair preconditioner blocks
     double *part, *part2;      // per-pair partials
@@ -965,17 +966,35 @@ __device__ __forceinline__ int pm_pair_team(long t, int a, unsigned team, const 
             dot1 = zv * zv;
         }
     } else if (mode == 1 || mode == 3) {
-        if (act) {
-            double *vv = A.v.pair;
-            if (m.pending) {
-                const double w = (vv[e] - m.up_oldeps * A.W[k % 3].pair[e] - m.up_delta * A.W[(k + 1) % 3].pair[e]) *
-                                 m.up_ginv;
-                A.W[(k + 2) % 3].pair[e] = w;
-                A.x.pair[e] += m.up_phi * w;
+        double *vv = A.v.pair;
+        if (act && m.pending) {
+            const double w = (vv[e] - m.up_oldeps * A.W[k % 3].pair[e] - m.up_delta * A.W[(k + 1) % 3].pair[e]) *
+                             m.up_ginv;
+            A.W[(k + 2) % 3].pair[e] = w;
+            A.x.pair[e] += m.up_phi * w;
+        }
+        if (mode == 1 && !m.done) {
+            // the pair rows of A z: z_q + S_q (y + y2) gathered at the pair's DOFs (the L^T of
+            // the apply; lane a gathers entry a and forms row a, columns in ascending order)
+            double ya = 0.0;
+            if (a < nd) {
+                const long bd = (a % 6) < 3 ? bead : (long)pairs[t].y;
+                int tb, wb;
+                vel_dofs(sp, (int)(bd - sp.bead_off), tb, wb);
+                const int d = (a < 6 ? tb : wb) + a % 3;
+                ya = A.y[sp.top_off + d] + (sp.ss_off >= 0 ? A.y2[sp.top_off + d] : 0.0);
             }
-            if (mode == 1 && !m.done) {
+            const double *Sq = A.S + 144L * t + a * nd;
+            double sy = 0.0;
+#pragma unroll
+            for (int c = 0; c < 12; c++) {
+                const double yc = __shfl_sync(team, ya, c, LT_LANES);
+                if (a < nd && c < nd) sy += Sq[c] * yc;
+            }
+            if (act) {
+                const double az = sy + A.z.pair[e];
                 const double vq = A.z.pair[e] * m.sinv;
-                double x = m.sinv * A.Az[e];
+                double x = m.sinv * az;
                 if (k >= 2) x -= (m.beta / m.oldb) * A.R[(k + 2) % 3].pair[e];
                 vv[e] = vq;
                 A.R[(k + 1) % 3].pair[e] = x;
@@ -1253,8 +1272,9 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     A.v = {E.d_pmp[6], E.d_pms[6]};
     A.z = {E.d_pmp[7], E.d_pms[7]};
     A.x = {E.d_pmp[8], E.d_pms[8]};
-    A.Az = E.d_pmp[9];
     A.y = E.d_py;
+    A.y2 = E.d_py2;
+    A.S = E.d_pS;
     A.u = E.d_pu;
     A.P = E.d_pP;
     A.part = E.d_ppart; A.part2 = E.d_ppart2;
@@ -1284,13 +1304,9 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     while (nact > 0 && k < maxit) {
         for (int j = 0; j < 8 && k < maxit; j++) {
             k++;
-            // Az = A z: u = [L z_y ; z_S] (z_S already in u), apply, z_y + L^T (...)_t
+            // Az = A z: u = [L z_y ; z_S] (z_S already in u), apply; mode 1 forms z_y + L^T (...)_t itself
             launch_ps_L(E, A.z.pair, nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds, st);
             mr_apply(E, fp32, dn, ds, st);
-            if (npair)
-                ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                      E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
-                                                                      A.z.pair, E.d_pmp[9], nullptr, dn, ds);
             ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                              E.d_segs, E.d_pmr, 1, k, A, red);
             ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
