@@ -1080,11 +1080,25 @@ __device__ void pm_scalars(MinresScal *mr, int r, int mode, double t0, double t1
     mr[r] = m;
 }
 
+// Fixed-order sum of x[lo, hi) over the block: thread t takes lo + t, lo + t + B,
+// ... into eight independent accumulators (eight loads in flight), joined in order.
+__device__ __forceinline__ double block_strided_sum(const double *__restrict__ x, long lo, long hi)
+{
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const long B = blockDim.x;
+    for (long q = lo + threadIdx.x; q < hi; q += 8 * B) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (q + u * B < hi) acc[u] += __ldcg(x + q + u * B);
+    }
+    return ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+}
+
 // In-kernel completion of the per-replica sums: every pair team and every bead
 // thread counts one item of its replica (warp-aggregated atomics after a
 // fence); the block whose count completes replica r sums r's pair partials (a
 // contiguous range, pairs being stored by lower bead) and bead partials in a
-// fixed order -- strided over the block, then a shuffle tree and the warps in
+// fixed order -- block_strided_sum, then a shuffle tree and the warps in
 // order, whichever block finishes -- and runs the scalar recurrence.
 struct PMRed {
     int *cnt;                  // per replica, zero between launches
@@ -1118,15 +1132,9 @@ __device__ void pm_count_and_finish(int myrep, const Seg *__restrict__ segs, con
         const int r = s_list[i];
         __threadfence();
         const Seg &s = segs[r];
-        double v0 = 0.0, v1 = 0.0;
-        for (long q = red.cptr[s.bead_off] + threadIdx.x; q < red.cptr[s.bead_off + s.Np]; q += blockDim.x) {
-            v0 += __ldcg(A.part + q);
-            v1 += __ldcg(A.part2 + q);
-        }
-        for (long b = s.bead_off + threadIdx.x; b < (long)s.bead_off + s.Np; b += blockDim.x) {
-            v0 += __ldcg(A.sA + b);
-            v1 += __ldcg(A.sB + b);
-        }
+        const long q0 = red.cptr[s.bead_off], q1 = red.cptr[s.bead_off + s.Np];
+        double v0 = block_strided_sum(A.part, q0, q1) + block_strided_sum(A.sA, s.bead_off, (long)s.bead_off + s.Np);
+        double v1 = block_strided_sum(A.part2, q0, q1) + block_strided_sum(A.sB, s.bead_off, (long)s.bead_off + s.Np);
         for (int o = 16; o > 0; o >>= 1) {
             v0 += __shfl_down_sync(0xffffffffu, v0, o);
             v1 += __shfl_down_sync(0xffffffffu, v1, o);
