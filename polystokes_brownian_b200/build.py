@@ -25,6 +25,12 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
           "-Xptxas", "-v", "-I" + os.path.join(HERE, "..", "include")]
 # translation units whose arithmetic must round like the reference's C++
 NO_FMA = {"stage.cu", "step.cu", "pairs.cu", "lub.cu"}
+# FP32 subnormals flushed to zero: the far-field kernels' FP32 operands (pair
+# separations and their squares, reciprocal square roots, inputs of order one)
+# stay many decades above the subnormal range (1e-38), and without the flag every
+# rsqrtf carries a subnormal guard (4 of 25 instructions per pair in the FP32x2
+# monomer kernel, measured with ncu's per-pipe instruction counts)
+FTZ = {"rpy.cu"}
 
 
 def sources():
@@ -45,7 +51,7 @@ def _compile(src):
     if not _needs(obj, deps):
         return obj, ""
     cmd = [NVCC] + ARCH + COMMON + (["--fmad=false"] if src in NO_FMA else []) + \
-          ["-c", os.path.join(CSRC, src), "-o", obj]
+          (["-ftz=true"] if src in FTZ else []) + ["-c", os.path.join(CSRC, src), "-o", obj]
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{p.stdout}\n{p.stderr}")
