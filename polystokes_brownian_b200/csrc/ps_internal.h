@@ -52,7 +52,7 @@ struct Seg {
 
 // Column chunk widths of the far-field pair kernels.
 constexpr int AA_CHUNK_COLS = 256;        // default; ps_autotune may pick another, process-wide
-constexpr int BB_CHUNK_COLS = 32;        // colloid columns per chunk, for up to BB_MAX_CHUNKS chunks
+constexpr int BB_CHUNK_COLS = 64;        // colloid columns per chunk, for up to BB_MAX_CHUNKS chunks
 constexpr int BB_MAX_CHUNKS = 64;
 
 // Row tile of the far-field pair kernels.

@@ -501,7 +501,7 @@ k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
 // columns h, h + BB_SPLIT, ...; the groups' sums are joined in group order in
 // shared memory, so a replica of a thousand colloids fills the SMs without
 // more chunk partials.
-constexpr int BB_SPLIT = 2;
+constexpr int BB_SPLIT = 4;
 template <class T>
 __global__ void __launch_bounds__(RPY_THREADS * BB_SPLIT)
 k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typename V4<T>::t *__restrict__ pos,
