@@ -3,6 +3,7 @@
 // over the engine functions.
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <algorithm>
 #include <mutex>
@@ -70,7 +71,7 @@ static void free_engine(Engine &E)
                     E.d_pms[4], E.d_pms[5], E.d_pms[6], E.d_pms[7], E.d_pms[8], E.d_obs_acc, E.d_obs_prev,
                     E.d_obs_ring, E.d_obs_msd, E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.d_obs_msdn,
                     E.d_sl_reps, E.d_sl_skip, E.d_slV, E.d_slT, E.d_sl_sc, E.d_sl_u, E.d_sl_y, E.d_sl_y2,
-                    E.d_cell_big, E.d_cell_nbig, E.d_cell_tmp, E.d_ref_r, E.d_ref_d, E.d_pm_cnt};
+                    E.d_cell_big, E.d_cell_nbig, E.d_cell_tmp, E.d_ref_r, E.d_ref_d, E.d_pm_cnt, E.d_fresh};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
@@ -284,6 +285,9 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     bptr[bead] = (int)bnbr.size();
     if ((rc = upload(E.d_chain, chain))) return rc;
     if ((rc = upload(E.d_coll_rep, coll_rep))) return rc;
+    std::vector<int> fresh(R);
+    for (int r = 0; r < R; r++) fresh[r] = descs[r].restart ? 0 : 1;
+    if ((rc = upload(E.d_fresh, fresh))) return rc;
     if ((rc = upload(E.d_bond_ptr, bptr))) return rc;
     if ((rc = upload(E.d_bond_nbr, bnbr))) return rc;
     if ((rc = upload(E.d_bond_sgn, bsgn))) return rc;
@@ -523,6 +527,42 @@ int ps_get_replica_steps(ps_ctx *ctx, uint64_t *steps)
     return PS_OK;
 }
 
+// index of the first non-finite value of v[0, n), or -1; the exponent test runs
+// over the whole array without a branch (it vectorises), the search only on failure
+static long first_nonfinite(const double *v, long n)
+{
+    uint64_t bad = 0;
+    for (long i = 0; i < n; i++) {
+        uint64_t u;
+        std::memcpy(&u, v + i, sizeof u);
+        bad |= (uint64_t)(((u >> 52) & 0x7ff) == 0x7ff);
+    }
+    if (!bad) return -1;
+    for (long i = 0; i < n; i++)
+        if (!std::isfinite(v[i])) return i;
+    return -1;
+}
+
+// trap centres from the colloids of the replicas that start fresh (Stokes.cpp:279-287)
+__global__ void k_trap_centres(long ncoll, const int *__restrict__ coll_rep, const Seg *__restrict__ segs,
+                               const int *__restrict__ fresh, const double *__restrict__ x, double *__restrict__ xpos0)
+{
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncoll) return;
+    const int r = coll_rep[c];
+    if (!fresh[r]) return;
+    const Seg &s = segs[r];
+    const long b = s.bead_off + s.Nm + (c - s.coll_off);
+    for (int d = 0; d < 3; d++) xpos0[3 * c + d] = x[3 * b + d];
+}
+
+__global__ void k_quat_identity(long ncoll, double *__restrict__ q)
+{
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncoll) return;
+    q[4 * c] = 1.0; q[4 * c + 1] = 0.0; q[4 * c + 2] = 0.0; q[4 * c + 3] = 0.0;
+}
+
 int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
 {
     if (!ctx || !x) return PS_ERR_ARG;
@@ -530,33 +570,30 @@ int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
     cudaStream_t st = S(stream);
     // host inputs are scanned before anything is copied or launched: a non-finite
     // coordinate would otherwise travel through the cell grid and every pair kernel
-    if (ps::is_host_ptr(x))
-        for (long i = 0; i < 3 * E.ntot; i++)
-            if (!std::isfinite(x[i])) {
-                ps::set_error("non-finite position at index " + std::to_string(i));
-                return PS_ERR_ARG;
-            }
-    if (q && ps::is_host_ptr(q))
-        for (long i = 0; i < 4 * E.ncoll; i++)
-            if (!std::isfinite(q[i])) {
-                ps::set_error("non-finite quaternion at index " + std::to_string(i));
-                return PS_ERR_ARG;
-            }
+    if (ps::is_host_ptr(x)) {
+        const long i = first_nonfinite(x, 3 * E.ntot);
+        if (i >= 0) {
+            ps::set_error("non-finite position at index " + std::to_string(i));
+            return PS_ERR_ARG;
+        }
+    }
+    if (q && ps::is_host_ptr(q)) {
+        const long i = first_nonfinite(q, 4 * E.ncoll);
+        if (i >= 0) {
+            ps::set_error("non-finite quaternion at index " + std::to_string(i));
+            return PS_ERR_ARG;
+        }
+    }
     PS_CK(cudaMemcpyAsync(E.d_x, x, sizeof(double) * 3 * E.ntot, cudaMemcpyDefault, st));
+    const int thr = 128;
+    const unsigned nbc = (unsigned)((E.ncoll + thr - 1) / thr);
     if (q) PS_CK(cudaMemcpyAsync(E.d_q, q, sizeof(double) * 4 * E.ncoll, cudaMemcpyDefault, st));
-    else if (E.ncoll) {
-        std::vector<double> qi(4 * E.ncoll, 0.0);
-        for (long c = 0; c < E.ncoll; c++) qi[4 * c] = 1.0;
-        PS_CK(cudaMemcpyAsync(E.d_q, qi.data(), sizeof(double) * qi.size(), cudaMemcpyHostToDevice, st));
-        PS_CK(cudaStreamSynchronize(st));
-    }
-    // trap centres from the colloids on a fresh start (Stokes.cpp:279-287)
-    for (int r = 0; r < E.R; r++) {
-        const Seg &s = E.segs[r];
-        if (E.desc[r].restart || s.Nc == 0) continue;
-        PS_CK(cudaMemcpyAsync(E.d_xpos0 + 3L * s.coll_off, E.d_x + 3L * (s.bead_off + s.Nm),
-                              sizeof(double) * 3 * s.Nc, cudaMemcpyDeviceToDevice, st));
-    }
+    else if (E.ncoll) ::ps_launch_count++, k_quat_identity<<<nbc, thr, 0, st>>>(E.ncoll, E.d_q);
+    // trap centres from the colloids on a fresh start (Stokes.cpp:279-287), one launch for the batch
+    if (E.ncoll)
+        ::ps_launch_count++, k_trap_centres<<<nbc, thr, 0, st>>>(E.ncoll, E.d_coll_rep, E.d_segs, E.d_fresh, E.d_x,
+                                                              E.d_xpos0);
+    PS_CK(cudaGetLastError());
     int rc = ps::stage_pack(E, st);
     return rc;
 }

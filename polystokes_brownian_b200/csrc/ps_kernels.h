@@ -55,6 +55,7 @@ struct Engine {
     float *d_aa_te2 = nullptr;   // per replica: squared exact radius of the FP32 monomer kernel
     double *d_chain = nullptr;      // chain id per bead (monomers), -1-c for colloid c
     int *d_coll_rep = nullptr;      // replica of each colloid
+    int *d_fresh = nullptr;         // per replica: 1 if it starts fresh (trap centres from its colloids)
     double *d_chs = nullptr;        // per colloid: its colloid-monomer HS sum (3 doubles)
     double *d_time = nullptr;       // per replica time
     double *d_ktrap = nullptr;      // per replica (weaken_trap mutates it)
