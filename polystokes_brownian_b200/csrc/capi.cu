@@ -75,6 +75,9 @@ static void free_engine(Engine &E)
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (E.h_nactive) cudaFreeHost(E.h_nactive);
+    if (E.ev_fork) cudaEventDestroy(E.ev_fork);
+    if (E.ev_join) cudaEventDestroy(E.ev_join);
+    if (E.side) cudaStreamDestroy(E.side);
     ps::free_red_table(E.red);
     ps::free_red_table(E.red_top);
     ps::free_red_table(E.red_vel);
@@ -343,6 +346,12 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     TRY_ALLOC(E.d_sinv, sizeof(double) * R);
     TRY_ALLOC(E.d_nactive, sizeof(int));
     PS_CK(cudaMallocHost(&E.h_nactive, sizeof(int)));
+    // side stream for the far field's small pair kernels (monomer-colloid, colloid-colloid),
+    // which run beside the monomer pair kernel; non-blocking so that the legacy default
+    // stream does not serialise it, ordered by the fork and join events only
+    PS_CK(cudaStreamCreateWithFlags(&E.side, cudaStreamNonBlocking));
+    PS_CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
+    PS_CK(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
     if ((rc = ps::build_red_table(E, E.red, 0))) return rc;
     if ((rc = ps::build_red_table(E, E.red_top, 1))) return rc;
     // step workspace

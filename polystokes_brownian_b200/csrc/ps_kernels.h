@@ -165,7 +165,8 @@ struct Engine {
     double *d_lzV = nullptr, *d_lzT = nullptr, *d_lzw = nullptr, *d_lzq = nullptr;
     double *d_lzs = nullptr;
 
-    cudaStream_t internal = nullptr;
+    cudaStream_t side = nullptr;                   // far field: small pair kernels beside the monomer kernel
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // monomer column chunk width of the far-field AA kernels: process-wide (every

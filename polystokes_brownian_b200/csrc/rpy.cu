@@ -666,6 +666,16 @@ template <class T>
 void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const char *done, int dstride, bool skip_aa)
 {
     const typename V4<T>::t *pos = (const typename V4<T>::t *)(sizeof(T) == 8 ? (const void *)E.d_pos64 : (const void *)E.d_pos32);
+    // the monomer-colloid and colloid-colloid kernels (a few microseconds each, few blocks)
+    // run on the side stream beside the monomer kernel; they write their own partials,
+    // and the join orders them before the combine
+    const bool fork = E.side && E.n_aa_tiles && !skip_aa && (E.n_ab_tiles || E.n_bb_tiles);
+    cudaStream_t ss = st;
+    if (fork) {
+        cudaEventRecord(E.ev_fork, st);
+        cudaStreamWaitEvent(E.side, E.ev_fork, 0);
+        ss = E.side;
+    }
     if (E.n_aa_tiles && !skip_aa) {
         if constexpr (sizeof(T) == 4)
         {
@@ -683,15 +693,19 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
                 E.d_segs, E.d_aa_tiles, E.d_pos64, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
     }
     if (E.n_ab_tiles)
-        ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
+        ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, ss>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
                                                          E.d_partBA, done, dstride);
     // colloid-colloid FTS blocks stay FP64 in the mixed form: near contact the
     // far-field FTS mobility is ill-conditioned and FP32 blocks leave a 1.2e-6
     // velocity error on a suspension at gap 0.01 (FP64: tracks rtol); they are
     // cheap wherever monomers carry the O(N^2) work
     if (E.n_bb_tiles)
-        ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, st>>>(
+        ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, ss>>>(
             E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, in_top, E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
+    if (fork) {
+        cudaEventRecord(E.ev_join, E.side);
+        cudaStreamWaitEvent(st, E.ev_join, 0);
+    }
 }
 
 void apply_operator(Engine &E, int mode, const double *x, double *y, const double *scale, bool fp32, cudaStream_t st,
