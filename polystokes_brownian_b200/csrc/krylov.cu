@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <vector>
+#include <cooperative_groups.h>
 #include "ps_internal.h"
 #include "ps_kernels.h"
 #include "ps_reduce.cuh"
@@ -594,6 +595,100 @@ __global__ void k_lz_breakdown(int R, LzScal *__restrict__ lz, const double *__r
     if (sqrt(nrm2[r]) <= 1e-12 * lz[r].b0) lz[r].done = 2;   // 2: finalise with m = j+1
 }
 
+// One Lanczos iteration's orthogonalisation for small batches, in one launch:
+// one cluster of LZC_CTAS blocks per replica, each block owning a slice of the
+// replica's vector.  Both passes of the reorthogonalisation (dots against
+// V_0..V_j, then q -= V h), the norm, the breakdown test and the next basis
+// vector; the cross-block sums go through distributed shared memory (every
+// block sums the blocks' partials in rank order, so all hold the same h), and
+// cluster barriers order the passes.  The arithmetic per element is that of
+// k_lz_dots / k_lz_sub / k_lz_next; only the order of the partial sums differs.
+// Used when the batch fits one wave of clusters; a replica that is done leaves
+// with its whole cluster (the flag is read before any block writes it).
+namespace cgr = cooperative_groups;
+constexpr int LZC_CTAS = 8, LZC_THREADS = 512;
+
+__device__ __forceinline__ void lzc_block_sum8(double (&v)[8], double (*ws)[8], double *out, int nval)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        double t = v[c];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) ws[wid][c] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < nval) {
+        double t = 0.0;
+        for (int w = 0; w < LZC_THREADS / 32; w++) t += ws[w][threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+__global__ void __cluster_dims__(LZC_CTAS, 1, 1) __launch_bounds__(LZC_THREADS)
+k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv, double *__restrict__ q, int j,
+                  int kmax, LzScal *__restrict__ lz, double *__restrict__ alpha, double *__restrict__ betad)
+{
+    cgr::cluster_group cl = cgr::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int r = blockIdx.x / LZC_CTAS;
+    __shared__ double part[2][LZ_KMAX + 1];     // this block's partial dots, one buffer per pass
+    __shared__ double ws[LZC_THREADS / 32][8];
+    __shared__ double hsh[LZ_KMAX + 1];
+    __shared__ double nsh[8];
+    if (lz[r].done) return;                     // the whole cluster: no block has written lz yet
+    const Seg &s = segs[r];
+    const long n = s.nm3nc11;
+    const long lo = s.top_off + n * rank / LZC_CTAS, hi = s.top_off + n * (rank + 1) / LZC_CTAS;
+    double alpha_j = 0.0;
+    for (int pass = 0; pass < 2; pass++) {
+        for (int i0 = 0; i0 <= j; i0 += 8) {
+            double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) {
+                const double qe = q[e];
+#pragma unroll
+                for (int c = 0; c < 8; c++)
+                    if (i0 + c <= j) v[c] += V[(long)(i0 + c) * ldv + e] * qe;
+            }
+            lzc_block_sum8(v, ws, &part[pass][i0], min(8, j + 1 - i0));
+        }
+        cl.sync();
+        for (int i = threadIdx.x; i <= j; i += LZC_THREADS) {
+            double h = 0.0;
+            for (int k = 0; k < LZC_CTAS; k++) h += cl.map_shared_rank(&part[pass][0], k)[i];
+            hsh[i] = h;
+        }
+        __syncthreads();
+        for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) {
+            double acc = q[e];
+            for (int i = 0; i <= j; i++) acc -= hsh[i] * V[(long)i * ldv + e];
+            q[e] = acc;
+        }
+        alpha_j += hsh[j];
+        __syncthreads();
+    }
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) v[0] += q[e] * q[e];
+    lzc_block_sum8(v, ws, nsh, 1);
+    cl.sync();
+    double nrm2 = 0.0;
+    for (int k = 0; k < LZC_CTAS; k++) nrm2 += cl.map_shared_rank(nsh, k)[0];
+    cl.sync();                                  // no block leaves while others read its shared memory
+    const double bj = sqrt(nrm2);
+    const bool broken = bj <= 1e-12 * lz[r].b0;
+    if (rank == 0 && threadIdx.x == 0) {
+        alpha[(long)LZ_KMAX * r + j] = alpha_j;
+        lz[r].m = j + 1;
+        if (broken) lz[r].done = 2;             // invariant subspace: finalise with m = j + 1
+        else if (j + 1 < kmax) betad[(long)LZ_KMAX * r + j] = bj;
+    }
+    if (!broken && j + 1 < kmax) {
+        const double inv = bj > 0 ? 1.0 / bj : 0.0;
+        for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) V[(long)(j + 1) * ldv + e] = q[e] * inv;
+    }
+}
+
 int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, ps_sqrt_result *res, cudaStream_t st)
 {
     int kmax = o && o->kmax > 0 ? o->kmax : 40;
@@ -612,19 +707,27 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     ::ps_launch_count++, k_lz_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, V, z, lz, nrm2);
     PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
     const int check = 8;   // convergence test every 8 vectors; the cap is handled after the loop
+    // batches that fit one wave of clusters orthogonalise in one cluster launch per vector
+    const bool small = (long)E.R * LZC_CTAS <= 128;
     size_t smem = sizeof(double) * (4 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
     std::vector<LzScal> hl(E.R);
     int j = 0;
     for (j = 0; j < kmax; j++) {
         apply_operator(E, 1, V + (long)j * ldv, q, nullptr, E.precision == PS_PREC_MIXED, st, &lz[0].done,
                        (int)sizeof(LzScal));
-        for (int pass = 0; pass < 2; pass++) {
-            ::ps_launch_count++, k_lz_dots<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h);
-            ::ps_launch_count++, k_lz_sub<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h, alpha, pass == 0);
+        if (small) {
+            ::ps_launch_count++, k_lz_orth_cluster<<<E.R * LZC_CTAS, LZC_THREADS, 0, st>>>(E.d_segs, V, ldv, q, j, kmax, lz,
+                                                                                       alpha, betad);
+        } else {
+            for (int pass = 0; pass < 2; pass++) {
+                ::ps_launch_count++, k_lz_dots<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h);
+                ::ps_launch_count++, k_lz_sub<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h, alpha, pass == 0);
+            }
+            seg_dot(E, T, q, q, nrm2, st);
+            ::ps_launch_count++, k_lz_breakdown<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, nrm2, j);
+            if (j + 1 < kmax)
+                ::ps_launch_count++, k_lz_next<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, nrm2, betad);
         }
-        seg_dot(E, T, q, q, nrm2, st);
-        ::ps_launch_count++, k_lz_breakdown<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, nrm2, j);
-        if (j + 1 < kmax) ::ps_launch_count++, k_lz_next<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, nrm2, betad);
         if ((j + 1) % check == 0 && j + 1 < kmax) {
             ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, j + 1, tol, 0);
             PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
