@@ -608,14 +608,11 @@ __global__ void k_lz_breakdown(int R, LzScal *__restrict__ lz, const double *__r
 namespace cgr = cooperative_groups;
 constexpr int LZC_CTAS = 8, LZC_THREADS = 512;
 
-// block sum of NV per-thread values; thread c < nval writes the sum of value c
-// (a shuffle tree per warp, then the warps in order)
-template <int NV>
-__device__ __forceinline__ void lzc_block_sum(double (&v)[NV], double (*ws)[32], double *out, int nval)
+__device__ __forceinline__ void lzc_block_sum8(double (&v)[8], double (*ws)[8], double *out, int nval)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-    for (int c = 0; c < NV; c++) {
+    for (int c = 0; c < 8; c++) {
         double t = v[c];
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
         if (lane == 0) ws[wid][c] = t;
@@ -637,7 +634,7 @@ k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv
     const int rank = (int)cl.block_rank();
     const int r = blockIdx.x / LZC_CTAS;
     __shared__ double part[2][LZ_KMAX + 1];     // this block's partial dots, one buffer per pass
-    __shared__ double ws[LZC_THREADS / 32][32];
+    __shared__ double ws[LZC_THREADS / 32][8];
     __shared__ double hsh[LZ_KMAX + 1];
     __shared__ double nsh[8];
     if (lz[r].done) return;                     // the whole cluster: no block has written lz yet
@@ -646,17 +643,15 @@ k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv
     const long lo = s.top_off + n * rank / LZC_CTAS, hi = s.top_off + n * (rank + 1) / LZC_CTAS;
     double alpha_j = 0.0;
     for (int pass = 0; pass < 2; pass++) {
-        for (int i0 = 0; i0 <= j; i0 += 32) {          // up to 32 basis vectors per sweep of the slice
-            double v[32];
-#pragma unroll
-            for (int c = 0; c < 32; c++) v[c] = 0.0;
+        for (int i0 = 0; i0 <= j; i0 += 8) {
+            double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) {
                 const double qe = q[e];
 #pragma unroll
-                for (int c = 0; c < 32; c++)
+                for (int c = 0; c < 8; c++)
                     if (i0 + c <= j) v[c] += V[(long)(i0 + c) * ldv + e] * qe;
             }
-            lzc_block_sum<32>(v, ws, &part[pass][i0], min(32, j + 1 - i0));
+            lzc_block_sum8(v, ws, &part[pass][i0], min(8, j + 1 - i0));
         }
         cl.sync();
         for (int i = threadIdx.x; i <= j; i += LZC_THREADS) {
@@ -673,9 +668,9 @@ k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv
         alpha_j += hsh[j];
         __syncthreads();
     }
-    double v[1] = {0.0};
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) v[0] += q[e] * q[e];
-    lzc_block_sum<1>(v, ws, nsh, 1);
+    lzc_block_sum8(v, ws, nsh, 1);
     cl.sync();
     double nrm2 = 0.0;
     for (int k = 0; k < LZC_CTAS; k++) nrm2 += cl.map_shared_rank(nsh, k)[0];
