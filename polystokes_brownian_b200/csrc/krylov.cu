@@ -596,35 +596,22 @@ __global__ void k_lz_breakdown(int R, LzScal *__restrict__ lz, const double *__r
 }
 
 // One Lanczos iteration's orthogonalisation for small batches, in one launch:
-// one cluster of LZC_CTAS blocks per replica, each block owning a slice of the
-// replica's vector.  Both passes of the reorthogonalisation (dots against
-// V_0..V_j, then q -= V h), the norm, the breakdown test and the next basis
-// vector; the cross-block sums go through distributed shared memory (every
-// block sums the blocks' partials in rank order, so all hold the same h), and
-// cluster barriers order the passes.  The arithmetic per element is that of
-// k_lz_dots / k_lz_sub / k_lz_next; only the order of the partial sums differs.
-// Used when the batch fits one wave of clusters; a replica that is done leaves
-// with its whole cluster (the flag is read before any block writes it).
+// one cluster of LZC_CTAS blocks per replica.  Both passes of the
+// reorthogonalisation (dots against V_0..V_j, then q -= V h), the norm, the
+// breakdown test and the next basis vector, with cluster barriers between the
+// phases and the cross-block sums read through distributed shared memory.
+// The arithmetic is bit for bit that of the launch sequence it replaces
+// (k_lz_dots, k_lz_sub, seg_dot, k_lz_breakdown, k_lz_next): the replica's
+// vector is cut into the reduction table's RB_SPAN blocks, each half of a
+// block (RB_THREADS threads) forms an RB block's partials with the same
+// thread-to-element map, shuffle tree and warp order, and every sum over RB
+// blocks runs in block order.  So a replica's noise does not depend on which
+// path its batch takes.  Used when the batch fits one wave of clusters and each
+// replica at most LZC_SLOTS RB blocks per half-block; a replica that is done
+// leaves with its whole cluster (the flag is read before any block writes it).
 namespace cgr = cooperative_groups;
-constexpr int LZC_CTAS = 8, LZC_THREADS = 512;
-
-__device__ __forceinline__ void lzc_block_sum8(double (&v)[8], double (*ws)[8], double *out, int nval)
-{
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-        double t = v[c];
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        if (lane == 0) ws[wid][c] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x < nval) {
-        double t = 0.0;
-        for (int w = 0; w < LZC_THREADS / 32; w++) t += ws[w][threadIdx.x];
-        out[threadIdx.x] = t;
-    }
-    __syncthreads();
-}
+constexpr int LZC_CTAS = 8, LZC_HALVES = 2, LZC_THREADS = RB_THREADS * LZC_HALVES, LZC_SLOTS = 4;
+constexpr int LZC_VB = LZC_CTAS * LZC_HALVES;         // virtual RB-table blocks per cluster
 
 __global__ void __cluster_dims__(LZC_CTAS, 1, 1) __launch_bounds__(LZC_THREADS)
 k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv, double *__restrict__ q, int j,
@@ -633,47 +620,108 @@ k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv
     cgr::cluster_group cl = cgr::this_cluster();
     const int rank = (int)cl.block_rank();
     const int r = blockIdx.x / LZC_CTAS;
-    __shared__ double part[2][LZ_KMAX + 1];     // this block's partial dots, one buffer per pass
-    __shared__ double ws[LZC_THREADS / 32][8];
+    const int half = threadIdx.x / RB_THREADS, t = threadIdx.x % RB_THREADS;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr int HW = RB_THREADS / 32;                   // warps per half
+    __shared__ double part[2][LZC_HALVES][LZC_SLOTS][LZ_KMAX + 1];   // per pass: RB-block partial dots
+    __shared__ double npart[LZC_HALVES][LZC_SLOTS];       // RB-block partial norms
+    __shared__ double sh[LZC_THREADS / 32][8];
     __shared__ double hsh[LZ_KMAX + 1];
-    __shared__ double nsh[8];
     if (lz[r].done) return;                     // the whole cluster: no block has written lz yet
     const Seg &s = segs[r];
-    const long n = s.nm3nc11;
-    const long lo = s.top_off + n * rank / LZC_CTAS, hi = s.top_off + n * (rank + 1) / LZC_CTAS;
+    const int n = s.nm3nc11;
+    const long base = s.top_off;
+    const int nb = (n + RB_SPAN - 1) / RB_SPAN, nslot = (nb + LZC_VB - 1) / LZC_VB;
+    const int vb = rank * LZC_HALVES + half;
     double alpha_j = 0.0;
     for (int pass = 0; pass < 2; pass++) {
-        for (int i0 = 0; i0 <= j; i0 += 8) {
-            double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) {
-                const double qe = q[e];
+        for (int sl = 0; sl < nslot; sl++) {
+            const int rb = vb + LZC_VB * sl;
+            const long st = (long)rb * RB_SPAN;
+            const int len = rb < nb ? min(RB_SPAN, n - rb * RB_SPAN) : 0;
+            double qv[RB_EPT];
 #pragma unroll
-                for (int c = 0; c < 8; c++)
-                    if (i0 + c <= j) v[c] += V[(long)(i0 + c) * ldv + e] * qe;
+            for (int k = 0; k < RB_EPT; k++) {
+                const int e = t + k * RB_THREADS;
+                qv[k] = e < len ? q[base + st + e] : 0.0;
             }
-            lzc_block_sum8(v, ws, &part[pass][i0], min(8, j + 1 - i0));
+            for (int i0 = 0; i0 <= j; i0 += 8) {
+                double v[8];
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    v[c] = 0.0;
+                    if (i0 + c <= j) {
+                        const double *Vi = V + (long)(i0 + c) * ldv + base + st;
+#pragma unroll
+                        for (int k = 0; k < RB_EPT; k++) {
+                            const int e = t + k * RB_THREADS;
+                            if (e < len) v[c] += Vi[e] * qv[k];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    double x = v[c];
+                    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+                    if (lane == 0) sh[wid][c] = x;
+                }
+                __syncthreads();
+                if (t < 8 && i0 + t <= j) {
+                    double x = 0.0;
+                    for (int w = 0; w < HW; w++) x += sh[half * HW + w][t];
+                    part[pass][half][sl][i0 + t] = x;
+                }
+                __syncthreads();
+            }
         }
         cl.sync();
-        for (int i = threadIdx.x; i <= j; i += LZC_THREADS) {
+        for (int i = threadIdx.x; i <= j; i += LZC_THREADS) {   // h_i over the RB blocks in block order
             double h = 0.0;
-            for (int k = 0; k < LZC_CTAS; k++) h += cl.map_shared_rank(&part[pass][0], k)[i];
+            for (int rb = 0; rb < nb; rb++) {
+                const int v2 = rb % LZC_VB;
+                h += cl.map_shared_rank(&part[pass][v2 % LZC_HALVES][rb / LZC_VB][0], v2 / LZC_HALVES)[i];
+            }
             hsh[i] = h;
         }
         __syncthreads();
-        for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) {
-            double acc = q[e];
-            for (int i = 0; i <= j; i++) acc -= hsh[i] * V[(long)i * ldv + e];
-            q[e] = acc;
+        for (int sl = 0; sl < nslot; sl++) {                   // q -= sum_i h_i V_i, i = 0..j per element
+            const int rb = vb + LZC_VB * sl;
+            if (rb >= nb) break;
+            const long st = (long)rb * RB_SPAN;
+            const int len = min(RB_SPAN, n - rb * RB_SPAN);
+            for (int k = 0; k < RB_EPT; k++) {
+                const int e = t + k * RB_THREADS;
+                if (e >= len) break;
+                double acc = q[base + st + e];
+                for (int i = 0; i <= j; i++) acc -= hsh[i] * V[(long)i * ldv + base + st + e];
+                q[base + st + e] = acc;
+            }
         }
         alpha_j += hsh[j];
         __syncthreads();
     }
-    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) v[0] += q[e] * q[e];
-    lzc_block_sum8(v, ws, nsh, 1);
+    for (int sl = 0; sl < nslot; sl++) {                       // RB-block norms, as seg_dot
+        const int rb = vb + LZC_VB * sl;
+        const long st = (long)rb * RB_SPAN;
+        const int len = rb < nb ? min(RB_SPAN, n - rb * RB_SPAN) : 0;
+        double x = 0.0;
+        for (int e = t; e < len; e += RB_THREADS) x += q[base + st + e] * q[base + st + e];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[wid][0] = x;
+        __syncthreads();
+        if (t == 0) {
+            double y = 0.0;
+            for (int w = 0; w < HW; w++) y += sh[half * HW + w][0];
+            npart[half][sl] = y;
+        }
+        __syncthreads();
+    }
     cl.sync();
     double nrm2 = 0.0;
-    for (int k = 0; k < LZC_CTAS; k++) nrm2 += cl.map_shared_rank(nsh, k)[0];
+    for (int rb = 0; rb < nb; rb++) {
+        const int v2 = rb % LZC_VB;
+        nrm2 += cl.map_shared_rank(&npart[v2 % LZC_HALVES][rb / LZC_VB], v2 / LZC_HALVES)[0];
+    }
     cl.sync();                                  // no block leaves while others read its shared memory
     const double bj = sqrt(nrm2);
     const bool broken = bj <= 1e-12 * lz[r].b0;
@@ -685,7 +733,13 @@ k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv
     }
     if (!broken && j + 1 < kmax) {
         const double inv = bj > 0 ? 1.0 / bj : 0.0;
-        for (long e = lo + threadIdx.x; e < hi; e += LZC_THREADS) V[(long)(j + 1) * ldv + e] = q[e] * inv;
+        for (int sl = 0; sl < nslot; sl++) {
+            const int rb = vb + LZC_VB * sl;
+            if (rb >= nb) break;
+            const long st = (long)rb * RB_SPAN;
+            const int len = min(RB_SPAN, n - rb * RB_SPAN);
+            for (int e = t; e < len; e += RB_THREADS) V[(long)(j + 1) * ldv + base + st + e] = q[base + st + e] * inv;
+        }
     }
 }
 
@@ -708,7 +762,9 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
     const int check = 8;   // convergence test every 8 vectors; the cap is handled after the loop
     // batches that fit one wave of clusters orthogonalise in one cluster launch per vector
-    const bool small = (long)E.R * LZC_CTAS <= 128;
+    bool small = (long)E.R * LZC_CTAS <= 128;
+    for (const Seg &sg : E.segs)
+        small = small && (sg.nm3nc11 + RB_SPAN - 1) / RB_SPAN <= LZC_VB * LZC_SLOTS;
     size_t smem = sizeof(double) * (4 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
     std::vector<LzScal> hl(E.R);
     int j = 0;

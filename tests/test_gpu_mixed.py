@@ -73,3 +73,23 @@ def test_iterative_refinement_recovers_fp64(lub):
     e_plain, e_ref = _rel(ups[1], ups[0]), _rel(ups[2], ups[0])
     assert e_plain < 1e-6
     assert e_ref < 5e-8 and e_ref < 0.25 * e_plain, (e_plain, e_ref)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_lanczos_paths_bit_identical(precision):
+    """The Lanczos square root orthogonalises a batch of up to 16 replicas with one
+    thread-block-cluster launch per basis vector and larger batches with the
+    reduction-table launch sequence; both sum in the same order, so a replica's
+    M^{1/2} z is bit-identical whether it runs alone or in a 20-replica batch."""
+    systems = configs.ensemble(20, seed=4, nmin=64, nmax=600)
+    big = Batch(systems, precision=precision)
+    big.stage()
+    z = torch.randn(big.ntop, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    w_big, _ = big.sqrtm(z, kmax=40, tol=1e-6)
+    for r in (0, 7, 19):
+        one = Batch([systems[r]], precision=precision)
+        one.stage()
+        w_one, _ = one.sqrtm(big.seg(z, r, "top").contiguous(), kmax=40, tol=1e-6)
+        assert torch.equal(w_one, big.seg(w_big, r, "top")), r
+        one.close()
+    big.close()
