@@ -78,6 +78,10 @@ static void free_engine(Engine &E)
     if (E.ev_fork) cudaEventDestroy(E.ev_fork);
     if (E.ev_join) cudaEventDestroy(E.ev_join);
     if (E.side) cudaStreamDestroy(E.side);
+    if (E.ev_fork2) cudaEventDestroy(E.ev_fork2);
+    if (E.ev_chk) cudaEventDestroy(E.ev_chk);
+    if (E.side2) cudaStreamDestroy(E.side2);
+    if (E.h_spec) cudaFreeHost(E.h_spec);
     ps::free_red_table(E.red);
     ps::free_red_table(E.red_top);
     ps::free_red_table(E.red_vel);
@@ -352,6 +356,11 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
     PS_CK(cudaStreamCreateWithFlags(&E.side, cudaStreamNonBlocking));
     PS_CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     PS_CK(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
+    // the Lanczos convergence checks run on their own stream beside the next basis vectors
+    PS_CK(cudaStreamCreateWithFlags(&E.side2, cudaStreamNonBlocking));
+    PS_CK(cudaEventCreateWithFlags(&E.ev_fork2, cudaEventDisableTiming));
+    PS_CK(cudaEventCreateWithFlags(&E.ev_chk, cudaEventDisableTiming));
+    PS_CK(cudaMallocHost(&E.h_spec, 16 * (size_t)std::max(E.R, 1)));
     if ((rc = ps::build_red_table(E, E.red, 0))) return rc;
     if ((rc = ps::build_red_table(E, E.red_top, 1))) return rc;
     // step workspace
@@ -388,7 +397,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         TRY_ALLOC(E.d_lzV, sizeof(double) * top * (KM + 1));
         TRY_ALLOC(E.d_lzq, sizeof(double) * top);
         TRY_ALLOC(E.d_lzT, sizeof(double) * ((KM + 1) * R * 2 + KM * R * 2 + R));
-        TRY_ALLOC(E.d_lzs, 32 * R);
+        TRY_ALLOC(E.d_lzs, 96 * R);          // Lanczos scalars, their snapshot, the checks' speculative verdicts
     }
     return PS_OK;
 }

@@ -520,17 +520,38 @@ __device__ void warp_tql(double *d, double *e, double *Z, double *rot, int n)
     }
 }
 
+// A check's verdict for one replica, written by the speculative checks.
+struct LzSpec {
+    int conv;      // converged at m
+    int m;
+    int fin;       // converged, or already done when the check started
+    int pad;
+};
+
 // one warp per replica: eig of T_m, g = b0 U sqrt(max(theta,0)) U^T e1,
-// convergence ||g - g_prev|| <= tol ||g|| (the Lanczos basis is orthonormal)
-__global__ void k_lz_check(int R, LzScal *__restrict__ lz, const double *__restrict__ alpha,
-                           const double *__restrict__ betad, double *__restrict__ gbuf, int m, double tol, int final_)
+// convergence ||g - g_prev|| <= tol ||g|| (the Lanczos basis is orthonormal).
+// final_ = 1: the final estimate, on the replica's own m when it is done, into lz.
+// final_ = 0: a speculative check beside the next basis vectors: it reads the
+// snapshot `snap` of lz taken when it was launched (the vectors that follow
+// move lz on) and writes its verdict into spec; the host applies it later
+// (k_lz_spec_apply).  g_prev is the previous check's g in both cases.
+__global__ void k_lz_check(int R, LzScal *__restrict__ lz, const LzScal *__restrict__ snap, LzSpec *__restrict__ spec,
+                           const double *__restrict__ alpha, const double *__restrict__ betad, double *__restrict__ gbuf,
+                           int m, double tol, int final_)
 {
     extern __shared__ double sm[];
     const int r = blockIdx.x;
-    if (lz[r].done && !final_) return;
+    const LzScal L = final_ ? lz[r] : snap[r];
     const int lane = threadIdx.x;
-    int mr = lz[r].done ? lz[r].m : m;
-    if (mr <= 0) return;
+    if (!final_ && L.done) {
+        if (lane == 0) spec[r] = LzSpec{0, L.m, 1, 0};
+        return;
+    }
+    int mr = L.done ? L.m : m;
+    if (mr <= 0) {
+        if (!final_ && lane == 0) spec[r] = LzSpec{0, 0, 0, 0};
+        return;
+    }
     double *d = sm, *e = sm + LZ_KMAX, *Z = sm + 2 * LZ_KMAX, *rot = Z + LZ_KMAX * LZ_KMAX;
     for (int i = lane; i < mr; i += 32) {
         d[i] = alpha[(long)LZ_KMAX * r + i];
@@ -550,7 +571,7 @@ __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const double *__restr
                 double sq = th > 0 ? sqrt(th) : 0.0;
                 gi += Z[i * mr + j] * sq * Z[0 * mr + j];
             }
-            gi *= lz[r].b0;
+            gi *= L.b0;
         }
         double old = g[i];
         diff2 += (gi - old) * (gi - old);
@@ -564,12 +585,27 @@ __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const double *__restr
         nneg += __shfl_down_sync(0xffffffffu, nneg, o);
     }
     if (lane == 0) {
-        lz[r].nneg = nneg;
-        if (!lz[r].done) {
-            lz[r].m = mr;
-            if (final_ || sqrt(diff2) <= tol * sqrt(nrm2)) lz[r].done = 1;
+        const int conv = sqrt(diff2) <= tol * sqrt(nrm2);
+        if (final_) {
+            lz[r].nneg = nneg;
+            if (!lz[r].done) {
+                lz[r].m = mr;
+                lz[r].done = 1;
+            }
+        } else {
+            spec[r] = LzSpec{conv, mr, conv, 0};
         }
     }
+}
+
+// a speculative check's verdict, applied in stream order after the vectors that
+// ran beside it: a replica that had converged at m stops there (done, m), as if
+// the check had held the vectors back; the vectors it took meanwhile are unused
+__global__ void k_lz_spec_apply(int R, LzScal *__restrict__ lz, const LzSpec *__restrict__ spec)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    if (spec[r].conv) { lz[r].done = 1; lz[r].m = spec[r].m; }
 }
 
 // w = V g (top layout)
@@ -767,6 +803,10 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
         small = small && (sg.nm3nc11 + RB_SPAN - 1) / RB_SPAN <= LZC_VB * LZC_SLOTS;
     size_t smem = sizeof(double) * (4 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
     std::vector<LzScal> hl(E.R);
+    LzScal *snap = lz + E.R;                                 // the scalars when a check was launched
+    LzSpec *spec = (LzSpec *)(snap + E.R);                   // the checks' verdicts
+    LzSpec *hspec = (LzSpec *)E.h_spec;
+    bool pending = false;
     int j = 0;
     for (j = 0; j < kmax; j++) {
         apply_operator(E, 1, V + (long)j * ldv, q, nullptr, E.precision == PS_PREC_MIXED, st, &lz[0].done,
@@ -785,16 +825,34 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
                 ::ps_launch_count++, k_lz_next<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, nrm2, betad);
         }
         if ((j + 1) % check == 0 && j + 1 < kmax) {
-            ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, j + 1, tol, 0);
-            PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
-            PS_CK(cudaStreamSynchronize(st));
-            bool all = true;
-            for (auto &l : hl) all &= (l.done != 0);
-            if (all) break;
+            if (pending) {
+                // the previous check (normally finished long before): apply its verdicts
+                PS_CK(cudaEventSynchronize(E.ev_chk));
+                pending = false;
+                ::ps_launch_count++, k_lz_spec_apply<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, spec);
+                bool all = true;
+                for (int r = 0; r < E.R; r++) all &= hspec[r].fin != 0;
+                if (all) break;
+            }
+            // check at m = j + 1 beside the next vectors, on a snapshot of the scalars
+            PS_CK(cudaMemcpyAsync(snap, lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToDevice, st));
+            PS_CK(cudaEventRecord(E.ev_fork2, st));
+            PS_CK(cudaStreamWaitEvent(E.side2, E.ev_fork2, 0));
+            ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, E.side2>>>(E.R, lz, snap, spec, alpha, betad, gbuf, j + 1,
+                                                                    tol, 0);
+            PS_CK(cudaMemcpyAsync(hspec, spec, sizeof(LzSpec) * E.R, cudaMemcpyDeviceToHost, E.side2));
+            PS_CK(cudaEventRecord(E.ev_chk, E.side2));
+            pending = true;
         }
     }
-    // final estimate: replicas at the cap, and replicas stopped by breakdown
-    ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, alpha, betad, gbuf, std::min(j + 1, kmax), tol, 1);
+    if (pending) {
+        // the last check's verdicts, and its g, ahead of the final estimate
+        PS_CK(cudaStreamWaitEvent(st, E.ev_chk, 0));
+        ::ps_launch_count++, k_lz_spec_apply<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, spec);
+    }
+    // final estimate: replicas at the cap, replicas stopped by breakdown, and the converged ones on their own m
+    ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, snap, spec, alpha, betad, gbuf,
+                                                        std::min(j + 1, kmax), tol, 1);
     ::ps_launch_count++, k_lz_combine<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, lz, gbuf, w);
     PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
