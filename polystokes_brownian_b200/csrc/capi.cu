@@ -565,6 +565,7 @@ static long first_nonfinite(const double *v, long n)
 __global__ void k_trap_centres(long ncoll, const int *__restrict__ coll_rep, const Seg *__restrict__ segs,
                                const int *__restrict__ fresh, const double *__restrict__ x, double *__restrict__ xpos0)
 {
+    pdl_enter();
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncoll) return;
     const int r = coll_rep[c];
@@ -576,6 +577,7 @@ __global__ void k_trap_centres(long ncoll, const int *__restrict__ coll_rep, con
 
 __global__ void k_quat_identity(long ncoll, double *__restrict__ q)
 {
+    pdl_enter();
     const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncoll) return;
     q[4 * c] = 1.0; q[4 * c + 1] = 0.0; q[4 * c + 2] = 0.0; q[4 * c + 3] = 0.0;
@@ -606,10 +608,10 @@ int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
     const int thr = 128;
     const unsigned nbc = (unsigned)((E.ncoll + thr - 1) / thr);
     if (q) PS_CK(cudaMemcpyAsync(E.d_q, q, sizeof(double) * 4 * E.ncoll, cudaMemcpyDefault, st));
-    else if (E.ncoll) ::ps_launch_count++, k_quat_identity<<<nbc, thr, 0, st>>>(E.ncoll, E.d_q);
+    else if (E.ncoll) ps_launch(k_quat_identity, nbc, thr, 0, st, E.ncoll, E.d_q);
     // trap centres from the colloids on a fresh start (Stokes.cpp:279-287), one launch for the batch
     if (E.ncoll)
-        ::ps_launch_count++, k_trap_centres<<<nbc, thr, 0, st>>>(E.ncoll, E.d_coll_rep, E.d_segs, E.d_fresh, E.d_x,
+        ps_launch(k_trap_centres, nbc, thr, 0, st, E.ncoll, E.d_coll_rep, E.d_segs, E.d_fresh, E.d_x,
                                                               E.d_xpos0);
     PS_CK(cudaGetLastError());
     int rc = ps::stage_pack(E, st);

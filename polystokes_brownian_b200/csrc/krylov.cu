@@ -64,6 +64,7 @@ void free_red_table(RedTable &T)
 // generic segmented dot: out[rep] = a.b
 __global__ void k_seg_dot(RedTable T, const double *__restrict__ a, const double *__restrict__ b, double *out)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][1];
     const RBlk B = T.d_blk[blockIdx.x];
     double v[1] = {0.0};
@@ -75,7 +76,7 @@ __global__ void k_seg_dot(RedTable T, const double *__restrict__ a, const double
 
 void seg_dot(Engine &E, RedTable &T, const double *a, const double *b, double *out, cudaStream_t st)
 {
-    ::ps_launch_count++, k_seg_dot<<<T.nblk, RB_THREADS, 0, st>>>(T, a, b, out);
+    ps_launch(k_seg_dot, T.nblk, RB_THREADS, 0, st, T, a, b, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -86,6 +87,7 @@ __global__ void k_mr_init(RedTable T, const Seg *segs, const double *__restrict_
                           double *__restrict__ v, double *__restrict__ w0, double *__restrict__ w1,
                           double *__restrict__ w2, double *__restrict__ sinv)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][3];
     const RBlk B = T.d_blk[blockIdx.x];
     double s[3] = {0.0, 0.0, 0.0};
@@ -131,6 +133,7 @@ __global__ void k_mr_alpha(RedTable T, const double *__restrict__ z, double *__r
                            const double *__restrict__ w1, const double *__restrict__ w2, double *__restrict__ x,
                            MinresScal *mr, int k)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][1];
     const RBlk B = T.d_blk[blockIdx.x];
     const MinresScal m = mr[B.rep];
@@ -168,6 +171,7 @@ __global__ void k_mr_beta(RedTable T, double *__restrict__ Av, const double *__r
                           const double *__restrict__ D, double *__restrict__ z, MinresScal *mr, int maxit,
                           int *nactive, double *__restrict__ sinv)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][1];
     const RBlk B = T.d_blk[blockIdx.x];
     const MinresScal m0 = mr[B.rep];
@@ -223,6 +227,7 @@ __global__ void k_mr_flush(RedTable T, const double *__restrict__ v, double *__r
                            const double *__restrict__ w1, const double *__restrict__ w2, double *__restrict__ x,
                            MinresScal *mr)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][1];
     const RBlk B = T.d_blk[blockIdx.x];
     const MinresScal m = mr[B.rep];
@@ -255,7 +260,7 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
         Ax = E.d_Rr[2];
     }
     // r_1 in slot 1 (slot k % 3 holds r_k)
-    ::ps_launch_count++, k_mr_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, b, Ax, E.d_D, E.d_Rr[1], E.d_z, x, E.d_mr, opt.warm,
+    ps_launch(k_mr_init, T.nblk, RB_THREADS, 0, st, T, E.d_segs, b, Ax, E.d_D, E.d_Rr[1], E.d_z, x, E.d_mr, opt.warm,
                                             opt.rtol, opt.maxit, E.d_v, E.d_W[0], E.d_W[1], E.d_W[2],
                                             E.d_sinv);
     PS_CK(cudaGetLastError());
@@ -281,8 +286,8 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
             // A v_k = (1/beta_k) A z_k: the operator applies the per-replica scale
             apply_operator(E, 0, E.d_z, Av, E.d_sinv, E.precision == PS_PREC_MIXED, st, &E.d_mr[0].done,
                            (int)sizeof(MinresScal));
-            ::ps_launch_count++, k_mr_alpha<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_z, E.d_v, Av, rkm1, wnew, w1, w2, x, E.d_mr, k);
-            ::ps_launch_count++, k_mr_beta<<<T.nblk, RB_THREADS, 0, st>>>(T, Av, rk, E.d_D, E.d_z, E.d_mr, opt.maxit, E.d_nactive,
+            ps_launch(k_mr_alpha, T.nblk, RB_THREADS, 0, st, T, E.d_z, E.d_v, Av, rkm1, wnew, w1, w2, x, E.d_mr, k);
+            ps_launch(k_mr_beta, T.nblk, RB_THREADS, 0, st, T, Av, rk, E.d_D, E.d_z, E.d_mr, opt.maxit, E.d_nactive,
                                                     E.d_sinv);
         }
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -295,7 +300,7 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
         double *wnew = E.d_W[(kk + 2) % 3];
         const double *w1 = E.d_W[(kk + 0) % 3];
         const double *w2 = E.d_W[(kk + 1) % 3];
-        ::ps_launch_count++, k_mr_flush<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_v, wnew, w1, w2, x, E.d_mr);
+        ps_launch(k_mr_flush, T.nblk, RB_THREADS, 0, st, T, E.d_v, wnew, w1, w2, x, E.d_mr);
     }
     PS_CK(cudaMemcpyAsync(hm.data(), E.d_mr, sizeof(MinresScal) * E.R, cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
@@ -330,6 +335,7 @@ constexpr int LZ_KMAX = 64;
 __global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, const double *__restrict__ q, int j,
                           const LzScal *__restrict__ lz, double *__restrict__ h)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][LZ_KMAX + 1];
     __shared__ bool last;
     const RBlk B = T.d_blk[blockIdx.x];
@@ -395,6 +401,7 @@ __global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, co
 __global__ void k_lz_sub(RedTable T, const double *__restrict__ V, long ldv, double *__restrict__ q, int j,
                          const LzScal *__restrict__ lz, const double *__restrict__ h, double *__restrict__ alpha, int first)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     if (lz[B.rep].done) return;
     const double *hr = h + (long)(LZ_KMAX + 1) * B.rep;
@@ -429,6 +436,7 @@ __global__ void k_lz_sub(RedTable T, const double *__restrict__ V, long ldv, dou
 __global__ void k_lz_next(RedTable T, double *__restrict__ V, long ldv, const double *__restrict__ q, int j,
                           LzScal *__restrict__ lz, const double *__restrict__ nrm2, double *__restrict__ betad)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     if (lz[B.rep].done) return;
     double bj = sqrt(nrm2[B.rep]);
@@ -440,6 +448,7 @@ __global__ void k_lz_next(RedTable T, double *__restrict__ V, long ldv, const do
 __global__ void k_lz_init(RedTable T, const Seg *__restrict__ segs, double *__restrict__ V,
                           const double *__restrict__ z, LzScal *__restrict__ lz, const double *__restrict__ nrm2)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     // shell replicas take the block-Cholesky noise path instead
     const bool skip = !segs[B.rep].mm_HI;
@@ -539,6 +548,7 @@ __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const LzScal *__restr
                            const double *__restrict__ alpha, const double *__restrict__ betad, double *__restrict__ gbuf,
                            int m, double tol, int final_)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const int r = blockIdx.x;
     const LzScal L = final_ ? lz[r] : snap[r];
@@ -603,6 +613,7 @@ __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const LzScal *__restr
 // the check had held the vectors back; the vectors it took meanwhile are unused
 __global__ void k_lz_spec_apply(int R, LzScal *__restrict__ lz, const LzSpec *__restrict__ spec)
 {
+    pdl_enter();
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
     if (spec[r].conv) { lz[r].done = 1; lz[r].m = spec[r].m; }
@@ -612,6 +623,7 @@ __global__ void k_lz_spec_apply(int R, LzScal *__restrict__ lz, const LzSpec *__
 __global__ void k_lz_combine(RedTable T, const double *__restrict__ V, long ldv, const LzScal *__restrict__ lz,
                              const double *__restrict__ gbuf, double *__restrict__ w)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     const int m = lz[B.rep].m;
     const double *g = gbuf + (long)(LZ_KMAX + 1) * B.rep;
@@ -625,6 +637,7 @@ __global__ void k_lz_combine(RedTable T, const double *__restrict__ V, long ldv,
 // breakdown: ||q|| tiny -> invariant subspace, stop extending
 __global__ void k_lz_breakdown(int R, LzScal *__restrict__ lz, const double *__restrict__ nrm2, int j)
 {
+    pdl_enter();
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R || lz[r].done) return;
     lz[r].m = j + 1;
@@ -653,6 +666,7 @@ __global__ void __cluster_dims__(LZC_CTAS, 1, 1) __launch_bounds__(LZC_THREADS)
 k_lz_orth_cluster(const Seg *__restrict__ segs, double *__restrict__ V, long ldv, double *__restrict__ q, int j,
                   int kmax, LzScal *__restrict__ lz, double *__restrict__ alpha, double *__restrict__ betad)
 {
+    pdl_enter();
     cgr::cluster_group cl = cgr::this_cluster();
     const int rank = (int)cl.block_rank();
     const int r = blockIdx.x / LZC_CTAS;
@@ -794,7 +808,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     double *gbuf = betad + (long)LZ_KMAX * E.R;             // [R][LZ_KMAX+1]
     double *nrm2 = gbuf + (long)(LZ_KMAX + 1) * E.R;        // [R]
     seg_dot(E, T, z, z, nrm2, st);
-    ::ps_launch_count++, k_lz_init<<<T.nblk, RB_THREADS, 0, st>>>(T, E.d_segs, V, z, lz, nrm2);
+    ps_launch(k_lz_init, T.nblk, RB_THREADS, 0, st, T, E.d_segs, V, z, lz, nrm2);
     PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
     const int check = 8;   // convergence test every 8 vectors; the cap is handled after the loop
     // batches that fit one wave of clusters orthogonalise in one cluster launch per vector
@@ -816,20 +830,20 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
                                                                                        alpha, betad);
         } else {
             for (int pass = 0; pass < 2; pass++) {
-                ::ps_launch_count++, k_lz_dots<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h);
-                ::ps_launch_count++, k_lz_sub<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, h, alpha, pass == 0);
+                ps_launch(k_lz_dots, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h);
+                ps_launch(k_lz_sub, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h, alpha, pass == 0);
             }
             seg_dot(E, T, q, q, nrm2, st);
-            ::ps_launch_count++, k_lz_breakdown<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, nrm2, j);
+            ps_launch(k_lz_breakdown, (E.R + 127) / 128, 128, 0, st, E.R, lz, nrm2, j);
             if (j + 1 < kmax)
-                ::ps_launch_count++, k_lz_next<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, q, j, lz, nrm2, betad);
+                ps_launch(k_lz_next, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, nrm2, betad);
         }
         if ((j + 1) % check == 0 && j + 1 < kmax) {
             if (pending) {
                 // the previous check (normally finished long before): apply its verdicts
                 PS_CK(cudaEventSynchronize(E.ev_chk));
                 pending = false;
-                ::ps_launch_count++, k_lz_spec_apply<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, spec);
+                ps_launch(k_lz_spec_apply, (E.R + 127) / 128, 128, 0, st, E.R, lz, spec);
                 bool all = true;
                 for (int r = 0; r < E.R; r++) all &= hspec[r].fin != 0;
                 if (all) break;
@@ -838,7 +852,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
             PS_CK(cudaMemcpyAsync(snap, lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToDevice, st));
             PS_CK(cudaEventRecord(E.ev_fork2, st));
             PS_CK(cudaStreamWaitEvent(E.side2, E.ev_fork2, 0));
-            ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, E.side2>>>(E.R, lz, snap, spec, alpha, betad, gbuf, j + 1,
+            ps_launch(k_lz_check, E.R, 32, smem, E.side2, E.R, lz, snap, spec, alpha, betad, gbuf, j + 1,
                                                                     tol, 0);
             PS_CK(cudaMemcpyAsync(hspec, spec, sizeof(LzSpec) * E.R, cudaMemcpyDeviceToHost, E.side2));
             PS_CK(cudaEventRecord(E.ev_chk, E.side2));
@@ -848,12 +862,12 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     if (pending) {
         // the last check's verdicts, and its g, ahead of the final estimate
         PS_CK(cudaStreamWaitEvent(st, E.ev_chk, 0));
-        ::ps_launch_count++, k_lz_spec_apply<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, lz, spec);
+        ps_launch(k_lz_spec_apply, (E.R + 127) / 128, 128, 0, st, E.R, lz, spec);
     }
     // final estimate: replicas at the cap, replicas stopped by breakdown, and the converged ones on their own m
-    ::ps_launch_count++, k_lz_check<<<E.R, 32, smem, st>>>(E.R, lz, snap, spec, alpha, betad, gbuf,
+    ps_launch(k_lz_check, E.R, 32, smem, st, E.R, lz, snap, spec, alpha, betad, gbuf,
                                                         std::min(j + 1, kmax), tol, 1);
-    ::ps_launch_count++, k_lz_combine<<<T.nblk, RB_THREADS, 0, st>>>(T, V, ldv, lz, gbuf, w);
+    ps_launch(k_lz_combine, T.nblk, RB_THREADS, 0, st, T, V, ldv, lz, gbuf, w);
     PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
     PS_CK(cudaGetLastError());
@@ -911,6 +925,7 @@ __device__ double sl_dot(const double *a, const double *b, int n)
 __global__ void k_sl_init(const Seg *__restrict__ segs, const int *__restrict__ reps, const double *__restrict__ fb,
                           double *__restrict__ V, SlScal *__restrict__ sc, int *__restrict__ skip)
 {
+    pdl_enter();
     const int slot = blockIdx.x, r = reps[slot];
     const Seg &s = segs[r];
     const int n = s.nc11;
@@ -930,6 +945,7 @@ __global__ void k_sl_load(long ntop, const int *__restrict__ top_offs, int R, co
                           const double *__restrict__ V, const SlScal *__restrict__ sc, int j, int stage,
                           const double *__restrict__ y, double *__restrict__ u)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ntop) return;
     int lo = 0, hi = R;
@@ -950,6 +966,7 @@ __global__ void k_sl_iter(const Seg *__restrict__ segs, const int *__restrict__ 
                           double *__restrict__ ab, SlScal *__restrict__ sc, int *__restrict__ skip,
                           const double *__restrict__ y, const double *__restrict__ y2, int j)
 {
+    pdl_enter();
     const int slot = blockIdx.x, r = reps[slot];
     if (sc[slot].done) return;
     const Seg &s = segs[r];
@@ -995,6 +1012,7 @@ __global__ void k_sl_finish(const Seg *__restrict__ segs, const int *__restrict_
                             const double *__restrict__ ab, SlScal *__restrict__ sc, const double *__restrict__ fb,
                             const double *__restrict__ ymcm, double *__restrict__ W)
 {
+    pdl_enter();
     __shared__ double d[SL_KMAX], e[SL_KMAX], Z[SL_KMAX * SL_KMAX], g[SL_KMAX], rot[2 * SL_KMAX];
     const int slot = blockIdx.x, r = reps[slot];
     const Seg &s = segs[r];
@@ -1033,20 +1051,20 @@ int schur_lanczos_noise(Engine &E, const double *fb, const double *ymcm, double 
     int kmax = 0;
     for (auto &s : E.segs)
         if (s.sl_slot >= 0) kmax = std::max(kmax, std::min(s.nc11, SL_KMAX));
-    ::ps_launch_count++, k_sl_init<<<ns, SL_THREADS, 0, st>>>(E.d_segs, E.d_sl_reps, fb, E.d_slV, sc, E.d_sl_skip);
+    ps_launch(k_sl_init, ns, SL_THREADS, 0, st, E.d_segs, E.d_sl_reps, fb, E.d_slV, sc, E.d_sl_skip);
     const int thr = 256;
     const unsigned gb = (unsigned)((E.ntop + thr - 1) / thr);
     for (int j = 0; j < kmax; j++) {
-        ::ps_launch_count++, k_sl_load<<<gb, thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 0,
+        ps_launch(k_sl_load, gb, thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 0,
                                                            nullptr, E.d_sl_u);
         apply_operator(E, 1, E.d_sl_u, E.d_sl_y, nullptr, false, st, E.d_sl_skip, (int)sizeof(int));
-        ::ps_launch_count++, k_sl_load<<<gb, thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 1,
+        ps_launch(k_sl_load, gb, thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 1,
                                                            E.d_sl_y, E.d_sl_u);
         apply_operator(E, 1, E.d_sl_u, E.d_sl_y2, nullptr, false, st, E.d_sl_skip, (int)sizeof(int));
-        ::ps_launch_count++, k_sl_iter<<<ns, SL_THREADS, 0, st>>>(E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc,
+        ps_launch(k_sl_iter, ns, SL_THREADS, 0, st, E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc,
                                                                   E.d_sl_skip, E.d_sl_y, E.d_sl_y2, j);
     }
-    ::ps_launch_count++, k_sl_finish<<<ns, SL_THREADS, 0, st>>>(E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc, fb, ymcm, W);
+    ps_launch(k_sl_finish, ns, SL_THREADS, 0, st, E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc, fb, ymcm, W);
     // the operator applies of the next noise draw start from the Lanczos set again
     std::vector<int> skip(E.R, 1);
     for (auto &s : E.segs)

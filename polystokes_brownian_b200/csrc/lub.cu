@@ -37,6 +37,7 @@ __global__ void k_lub_apply(long ntot, const int *__restrict__ bead_offs, int R,
                             const int *__restrict__ ptr, const int *__restrict__ nbr, const double *__restrict__ u,
                             int u_saddle, double *__restrict__ y, double *__restrict__ diag)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int r = rep_of_b(bead_offs, R, b);
@@ -95,6 +96,7 @@ __global__ void k_lub_apply(long ntot, const int *__restrict__ bead_offs, int R,
 
 __global__ void k_canon_count(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr, int *__restrict__ cnt)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int n = 0;
@@ -105,6 +107,7 @@ __global__ void k_canon_count(long ntot, const int *__restrict__ sptr, const int
 __global__ void k_canon_fill(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr,
                              const int *__restrict__ cptr, int *__restrict__ cnbr, int2 *__restrict__ pairs)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int q = cptr[b];
@@ -119,6 +122,7 @@ __global__ void k_canon_fill(long ntot, const int *__restrict__ sptr, const int 
 __global__ void k_canon_map(long ntot, const int *__restrict__ sptr, const int *__restrict__ snbr,
                             const int *__restrict__ cptr, const int *__restrict__ cnbr, int *__restrict__ cidx)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     for (int t = sptr[b]; t < sptr[b + 1]; t++) {
@@ -163,11 +167,11 @@ int lub_build(Engine &E, cudaStream_t st)
     }
     int thr = 128;
     unsigned nb = (unsigned)((E.ntot + thr - 1) / thr);
-    ::ps_launch_count++, k_canon_count<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_nbr_count);
+    ps_launch(k_canon_count, nb, thr, 0, st, E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_nbr_count);
     if ((rc = exclusive_scan(E, E.d_nbr_count, E.d_lubc_ptr, E.ntot, st))) return rc;
-    ::ps_launch_count++, k_canon_fill<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
+    ps_launch(k_canon_fill, nb, thr, 0, st, E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
                                                        E.d_lub_pairs);
-    ::ps_launch_count++, k_canon_map<<<nb, thr, 0, st>>>(E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
+    ps_launch(k_canon_map, nb, thr, 0, st, E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
                                                       E.d_lub_cidx);
     E.lub_npairs = nc;
     PS_CK(cudaGetLastError());
@@ -177,7 +181,7 @@ int lub_build(Engine &E, cudaStream_t st)
 void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st)
 {
     int thr = 128;
-    ::ps_launch_count++, k_lub_apply<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
+    ps_launch(k_lub_apply, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
         E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, x_saddle, 1,
         y_vel, nullptr);
 }
@@ -185,7 +189,7 @@ void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st
 void lub_apply_vel(Engine &E, const double *u_vel, double *y_vel, cudaStream_t st)
 {
     int thr = 128;
-    ::ps_launch_count++, k_lub_apply<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
+    ps_launch(k_lub_apply, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
         E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, u_vel, 0,
         y_vel, nullptr);
 }
@@ -195,7 +199,7 @@ int lub_diag(Engine &E, cudaStream_t st)
     int thr = 128;
     PS_CK(cudaMemsetAsync(E.d_lub_diag, 0, sizeof(double) * E.nvel, st));
     PS_CK(cudaMemsetAsync(E.d_tmp_vel, 0, sizeof(double) * E.nvel, st));
-    ::ps_launch_count++, k_lub_apply<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
+    ps_launch(k_lub_apply, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
         E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_tmp_vel, 0,
         E.d_tmp_vel2, E.d_lub_diag);
     PS_CK(cudaGetLastError());

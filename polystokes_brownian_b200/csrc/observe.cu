@@ -42,6 +42,7 @@ __global__ void k_observe(long ntot, const int *__restrict__ bead_offs, int R, c
                           double *__restrict__ prev, int *__restrict__ has_prev, unsigned long long *__restrict__ hb,
                           unsigned long long *__restrict__ ht, int nbins, double bmax, double tmax)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     const int r = obs_rep(bead_offs, R, b);
@@ -81,6 +82,7 @@ __global__ void k_observe_msd(long ncoll, const int *__restrict__ coll_rep, cons
                               const double *__restrict__ x, double *__restrict__ ring, double *__restrict__ msd,
                               unsigned long long *__restrict__ cnt, int L, long n)
 {
+    pdl_enter();
     long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncoll) return;
     const Seg &s = segs[coll_rep[c]];
@@ -136,11 +138,11 @@ int obs_sample(Engine &E, cudaStream_t st)
 {
     if (!E.d_obs_acc) { set_error("ps_observe: call ps_obs_reset first"); return PS_ERR_STATE; }
     int thr = 128;
-    ::ps_launch_count++, k_observe<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
+    ps_launch(k_observe, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
         E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_bond_ptr, E.d_bond_nbr, E.d_obs_acc, E.d_obs_prev,
         E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.obs_nbins, E.obs_bmax, E.obs_tmax);
     if (E.ncoll)
-        ::ps_launch_count++, k_observe_msd<<<(unsigned)((E.ncoll + thr - 1) / thr), thr, 0, st>>>(
+        ps_launch(k_observe_msd, (unsigned)((E.ncoll + thr - 1) / thr), thr, 0, st,
             E.ncoll, E.d_coll_rep, E.d_segs, E.d_x, E.d_obs_ring, E.d_obs_msd, E.d_obs_msdn, E.obs_lags, E.obs_n);
     PS_CK(cudaGetLastError());
     E.obs_n++;

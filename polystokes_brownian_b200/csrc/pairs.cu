@@ -153,6 +153,7 @@ __global__ void k_pairs_count(long ntot, const int *__restrict__ bead_offs, int 
                               const int *__restrict__ csorted, long ncoll, const int *__restrict__ coll_rep,
                               int which, int *__restrict__ cnt)
 {
+    pdl_enter();
     const long nbb = (ntot + blockDim.x - 1) / blockDim.x;
     if (blockIdx.x >= nbb) {
         const long c = (long)(blockIdx.x - nbb) * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -179,6 +180,7 @@ __global__ void k_pairs_fill(long ntot, const int *__restrict__ bead_offs, int R
                              const int *__restrict__ csorted, long ncoll, const int *__restrict__ coll_rep, int which,
                              const int *__restrict__ ptr, int *__restrict__ nbr)
 {
+    pdl_enter();
     const long nbb = (ntot + blockDim.x - 1) / blockDim.x;
     if (blockIdx.x >= nbb) {
         const long c = (long)(blockIdx.x - nbb) * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -212,6 +214,7 @@ constexpr int SCAN_T = 256, SCAN_E = 16, SCAN_SPAN = SCAN_T * SCAN_E;
 __global__ void __launch_bounds__(SCAN_T) k_scan_local(long n, const int *__restrict__ in, int *__restrict__ out,
                                                        int *__restrict__ sums)
 {
+    pdl_enter();
     __shared__ int ws[SCAN_T / 32];
     const long base = (long)blockIdx.x * SCAN_SPAN + (long)threadIdx.x * SCAN_E;
     int v[SCAN_E], tot = 0;
@@ -253,6 +256,7 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_local(long n, const int *__rest
 // in-place exclusive scan of the m block totals, total into sums[m]
 __global__ void k_scan_sums(int m, int *__restrict__ sums)
 {
+    pdl_enter();
     __shared__ int carry;
     __shared__ int tmp[1024];
     if (threadIdx.x == 0) carry = 0;
@@ -278,6 +282,7 @@ __global__ void k_scan_sums(int m, int *__restrict__ sums)
 
 __global__ void __launch_bounds__(SCAN_T) k_scan_add(long n, int m, const int *__restrict__ sums, int *__restrict__ out)
 {
+    pdl_enter();
     const int off = sums[blockIdx.x];
     const long base = (long)blockIdx.x * SCAN_SPAN;
     for (int e = threadIdx.x; e < SCAN_SPAN; e += SCAN_T) {
@@ -292,9 +297,9 @@ int exclusive_scan(Engine &E, const int *in, int *out, long n, cudaStream_t st)
     long m = (n + SCAN_SPAN - 1) / SCAN_SPAN;
     if (m < 1) m = 1;
     if (m + 1 > E.scan_cap) { set_error("scan scratch too small"); return PS_ERR_STATE; }
-    ::ps_launch_count++, k_scan_local<<<(unsigned)m, SCAN_T, 0, st>>>(n, in, out, E.d_scan_sums);
-    ::ps_launch_count++, k_scan_sums<<<1, 1024, 0, st>>>((int)m, E.d_scan_sums);
-    ::ps_launch_count++, k_scan_add<<<(unsigned)m, SCAN_T, 0, st>>>(n, (int)m, E.d_scan_sums, out);
+    ps_launch(k_scan_local, (unsigned)m, SCAN_T, 0, st, n, in, out, E.d_scan_sums);
+    ps_launch(k_scan_sums, 1, 1024, 0, st, (int)m, E.d_scan_sums);
+    ps_launch(k_scan_add, (unsigned)m, SCAN_T, 0, st, n, (int)m, E.d_scan_sums, out);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
@@ -302,6 +307,7 @@ int exclusive_scan(Engine &E, const int *in, int *out, long n, cudaStream_t st)
 __global__ void k_pairs_expand(long ntot, const int *__restrict__ ptr, const int *__restrict__ nbr,
                                int32_t *__restrict__ pi, int32_t *__restrict__ pj, long maxp)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     for (int k = ptr[b]; k < ptr[b + 1]; k++)
@@ -313,7 +319,7 @@ int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
 {
     int thr = 128;
     unsigned nbk = (unsigned)((E.ntot + thr - 1) / thr + (E.ncoll + thr / 32 - 1) / (thr / 32));
-    ::ps_launch_count++, k_pairs_count<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
+    ps_launch(k_pairs_count, nbk, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
                                        E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_count);
     int rc = exclusive_scan(E, E.d_nbr_count, E.d_nbr_ptr, E.ntot, st);
     if (rc) return rc;
@@ -325,7 +331,7 @@ int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
         E.nbr_cap = (long)tot * 3 / 2 + 1024;
         PS_CK(cudaMalloc(&E.d_nbr, sizeof(int) * E.nbr_cap));
     }
-    ::ps_launch_count++, k_pairs_fill<<<nbk, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
+    ps_launch(k_pairs_fill, nbk, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
                                       E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_ptr, E.d_nbr);
     PS_CK(cudaGetLastError());
     *npairs = tot;
@@ -339,7 +345,7 @@ int pair_list(Engine &E, int which, int32_t *pi, int32_t *pj, int64_t maxp, int6
     if (rc) return rc;
     if (pi && pj && maxp > 0) {
         int thr = 128;
-        ::ps_launch_count++, k_pairs_expand<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_nbr_ptr, E.d_nbr, pi, pj, maxp);
+        ps_launch(k_pairs_expand, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st, E.ntot, E.d_nbr_ptr, E.d_nbr, pi, pj, maxp);
         PS_CK(cudaGetLastError());
     }
     if (count) *count = np;

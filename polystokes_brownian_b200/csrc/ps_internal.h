@@ -18,6 +18,52 @@
 // number of kernels this library has launched (host-side counter)
 extern unsigned long long ps_launch_count;
 
+// Programmatic dependent launch.  Every kernel of the library opens with
+// pdl_enter(): griddepcontrol.wait returns once the grid it was launched behind
+// has completed and its writes are visible (at once when it was launched without
+// a programmatic dependency), and launch_dependents then lets the next kernel of
+// the stream be scheduled into SM slots this grid frees.  So consecutive kernels
+// keep full stream order for every load and store, and only the next grid's
+// launch and block ramp overlap the tail of this one.  Every block passes the
+// wait before anything else, early-exit blocks included, so a grid never
+// completes before its predecessor.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
+
+#ifndef __CUDACC_RTC__
+#include <cstdlib>
+#include <utility>
+// whether launches carry the programmatic-serialisation attribute (PS_PDL=0 turns it off)
+inline bool ps_pdl_on()
+{
+    static const bool on = [] { const char *e = std::getenv("PS_PDL"); return !(e && e[0] == '0'); }();
+    return on;
+}
+
+// launch a kernel of this library behind the previous work of the stream with
+// programmatic dependent launch (the kernel must open with pdl_enter())
+template <class... KArgs, class... Args>
+inline void ps_launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = ps_pdl_on() ? 1 : 0;
+    ++::ps_launch_count;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+#endif
+
 // Per-replica segment descriptor (device resident, one per replica).
 struct Seg {
     int Nm, Nc, Np;

@@ -163,6 +163,7 @@ k_rpy_aa_f2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
             const double *__restrict__ u, int in_top, double *__restrict__ part, long part_stride, int nchunk,
             const char *__restrict__ done, int done_stride)
 {
+    pdl_enter();
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     __shared__ float4 sXY[64], sZU[64], sUU[64], sLA[64], sLB[64];
     __shared__ float sK[12][AAF_THREADS];     // Kahan sums [0, 6) and compensations [6, 12), thread-private
@@ -327,6 +328,7 @@ k_rpy_aa_d2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
             const double *__restrict__ u, int in_top, double *__restrict__ part, long part_stride, int nchunk,
             const char *__restrict__ done, int done_stride)
 {
+    pdl_enter();
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     __shared__ double4 sP[128], sU[128];
     const Tile tl = tiles[blockIdx.x];
@@ -383,6 +385,7 @@ k_rpy_aa_d2(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const 
 // max |own - CUDA| / ulp(CUDA) of the reciprocal square root over a[0..n)
 __global__ void k_rsqrt_check(long n, const double *__restrict__ a, unsigned long long *__restrict__ worst)
 {
+    pdl_enter();
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double ref = rsqrt(a[i]), own = rsqrt_seeded(a[i]);
@@ -402,6 +405,7 @@ k_rpy_ab(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, const double *__restrict__ tab,
          double *__restrict__ part_m, double *__restrict__ part_ba, const char *__restrict__ done, int done_stride)
 {
+    pdl_enter();
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     typedef typename V4<T>::t P4;
     constexpr bool F32 = sizeof(T) == 4;
@@ -508,6 +512,7 @@ k_rpy_bb(const Seg *__restrict__ segs, const Tile *__restrict__ tiles, const typ
          const float4 *__restrict__ plo, const double *__restrict__ u, int in_top, double *__restrict__ part,
          long part_stride, int nchunk, const char *__restrict__ done, int done_stride)
 {
+    pdl_enter();
     if (done && *(const int *)(done + (long)tiles[blockIdx.x].rep * done_stride)) return;
     typedef typename V4<T>::t P4;
     constexpr bool F32 = sizeof(T) == 4;
@@ -604,6 +609,7 @@ __global__ void k_combine(const Seg *__restrict__ segs, RedTable T, int mode, co
                           const double *__restrict__ lub_y, long part_stride, double *__restrict__ y,
                           const char *__restrict__ done, int done_stride)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     const int r = B.rep;
     if (done && *(const int *)(done + (long)r * done_stride)) return;   // converged replica: skip
@@ -680,27 +686,27 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
         if constexpr (sizeof(T) == 4)
         {
             if (E.any_aa_rpy)
-                ::ps_launch_count++, k_rpy_aa_f2<false><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
+                ps_launch(k_rpy_aa_f2<false>, dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st,
                     E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
                     E.part_stride, E.nch_aa, done, dstride);
             if (E.any_aa_ref)
-                ::ps_launch_count++, k_rpy_aa_f2<true><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(
+                ps_launch(k_rpy_aa_f2<true>, dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st,
                     E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
                     E.part_stride, E.nch_aa, done, dstride);
         }
         else
-            ::ps_launch_count++, k_rpy_aa_d2<<<dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st>>>(
+            ps_launch(k_rpy_aa_d2, dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st,
                 E.d_segs, E.d_aa_tiles, E.d_pos64, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
     }
     if (E.n_ab_tiles)
-        ::ps_launch_count++, k_rpy_ab<T><<<E.n_ab_tiles, RPY_THREADS, 0, ss>>>(E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
+        ps_launch(k_rpy_ab<T>, E.n_ab_tiles, RPY_THREADS, 0, ss, E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
                                                          E.d_partBA, done, dstride);
     // colloid-colloid FTS blocks stay FP64 in the mixed form: near contact the
     // far-field FTS mobility is ill-conditioned and FP32 blocks leave a 1.2e-6
     // velocity error on a suspension at gap 0.01 (FP64: tracks rtol); they are
     // cheap wherever monomers carry the O(N^2) work
     if (E.n_bb_tiles)
-        ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, ss>>>(
+        ps_launch(k_rpy_bb<double>, dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, ss,
             E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, in_top, E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
     if (fork) {
         cudaEventRecord(E.ev_join, E.side);
@@ -721,7 +727,7 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
         lub_y = E.d_luby;
     }
     const RedTable &T = mode == 0 ? E.red : E.red_top;
-    ::ps_launch_count++, k_combine<<<dim3((unsigned)T.nblk, RB_EPT), RB_THREADS, 0, st>>>(
+    ps_launch(k_combine, dim3((unsigned)T.nblk, RB_EPT), RB_THREADS, 0, st,
         E.d_segs, T, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
         E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
 }
@@ -759,15 +765,15 @@ int time_pairs(Engine &E, int which, int reps, const double *u, double *ms, cuda
     auto launch = [&]() {
         if (which == 0 && E.n_aa_tiles) {
             if (fp32) {
-                if (E.any_aa_rpy) ::ps_launch_count++, k_rpy_aa_f2<false><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
-                if (E.any_aa_ref) ::ps_launch_count++, k_rpy_aa_f2<true><<<dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+                if (E.any_aa_rpy) ps_launch(k_rpy_aa_f2<false>, dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st, E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+                if (E.any_aa_ref) ps_launch(k_rpy_aa_f2<true>, dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st, E.d_segs, E.d_aa_tiles, (const float4 *)pos, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
             }
-            else ::ps_launch_count++, k_rpy_aa_d2<<<dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st>>>(E.d_segs, E.d_aa_tiles, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
+            else ps_launch(k_rpy_aa_d2, dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st, E.d_segs, E.d_aa_tiles, E.d_pos64, u, 1, E.d_partAA, E.part_stride, E.nch_aa, nullptr, 0);
         } else if (which == 1 && E.n_ab_tiles) {
-            if (fp32) ::ps_launch_count++, k_rpy_ab<float><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
-            else ::ps_launch_count++, k_rpy_ab<double><<<E.n_ab_tiles, RPY_THREADS, 0, st>>>(E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
+            if (fp32) ps_launch(k_rpy_ab<float>, E.n_ab_tiles, RPY_THREADS, 0, st, E.d_segs, E.d_ab_tiles, (const float4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
+            else ps_launch(k_rpy_ab<double>, E.n_ab_tiles, RPY_THREADS, 0, st, E.d_segs, E.d_ab_tiles, (const double4 *)pos, E.d_pos32lo, u, 1, E.d_tab, E.d_partAB, E.d_partBA, nullptr, 0);
         } else if (which == 2 && E.n_bb_tiles) {
-            ::ps_launch_count++, k_rpy_bb<double><<<dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, st>>>(E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
+            ps_launch(k_rpy_bb<double>, dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, st, E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, 1, E.d_partBB, E.part_stride, E.nch_bb, nullptr, 0);
         } else if (which == 3) {
             apply_operator(E, 1, u, E.d_tmp_top2, nullptr, fp32, st);
         }
@@ -792,7 +798,7 @@ int rsqrt_check(const double *a, long n, unsigned long long *max_ulp, cudaStream
     unsigned long long *d = nullptr;
     PS_CK(cudaMallocAsync(&d, sizeof(unsigned long long), st));
     PS_CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), st));
-    if (n > 0) ::ps_launch_count++, k_rsqrt_check<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, d);
+    if (n > 0) ps_launch(k_rsqrt_check, (unsigned)((n + 255) / 256), 256, 0, st, n, a, d);
     PS_CK(cudaMemcpyAsync(max_ulp, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     PS_CK(cudaFreeAsync(d, st));
     PS_CK(cudaStreamSynchronize(st));
@@ -803,6 +809,7 @@ int rsqrt_check(const double *a, long n, unsigned long long *max_ulp, cudaStream
 template <class T>
 __global__ void k_fma(T *out, int iters, T seed)
 {
+    pdl_enter();
     T a[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) a[k] = seed + T(k) * T(1e-3) + T(threadIdx.x) * T(1e-7);
@@ -820,6 +827,7 @@ __global__ void k_fma(T *out, int iters, T seed)
 // the same with packed FP32x2 FMAs (FFMA2): 8 independent float2 chains per thread
 __global__ void k_fma2(float *out, int iters, float seed)
 {
+    pdl_enter();
     float2 a[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) a[k] = make_float2(seed + k * 1e-3f + threadIdx.x * 1e-7f, seed - k * 1e-3f);

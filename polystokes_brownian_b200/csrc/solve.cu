@@ -46,6 +46,7 @@ __device__ __forceinline__ int rep_at(const int *__restrict__ offs, int R, long 
 __global__ void k_struct_init(long nvec, const int *__restrict__ vec_offs, int R, const Seg *__restrict__ segs,
                               const double *__restrict__ b, double *__restrict__ x)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvec) return;
     int r = rep_at(vec_offs, R, k);
@@ -86,6 +87,7 @@ __global__ void k_struct_ss(const Seg *__restrict__ segs, const int *__restrict_
                             const double *__restrict__ delta, const double *__restrict__ b,
                             const double *__restrict__ y, double *__restrict__ x)
 {
+    pdl_enter();
     __shared__ double A[SS_MAX][SS_MAX + 1];
     __shared__ int piv;
     const int r = reps[blockIdx.x];
@@ -130,6 +132,7 @@ __global__ void k_struct_ss(const Seg *__restrict__ segs, const int *__restrict_
 __global__ void k_struct_u(long nvec, const int *__restrict__ vec_offs, int R, const Seg *__restrict__ segs,
                            const double *__restrict__ b, const double *__restrict__ y, double *__restrict__ x)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvec) return;
     int r = rep_at(vec_offs, R, k);
@@ -149,6 +152,7 @@ __global__ void k_struct_u(long nvec, const int *__restrict__ vec_offs, int R, c
 __global__ void k_ss_inverse(const Seg *__restrict__ segs, const int *__restrict__ reps, const double *__restrict__ pos_x,
                              const double *__restrict__ delta, double *__restrict__ ssinv)
 {
+    pdl_enter();
     __shared__ double A[SS_MAX][SS_MAX + 1];
     __shared__ int perm[SS_MAX];
     __shared__ int piv;
@@ -201,6 +205,7 @@ __global__ void k_ss_apply(const Seg *__restrict__ segs, const int *__restrict__
                            const double *__restrict__ a, int la, double ca, const double *__restrict__ b, int lb,
                            double cb, double *__restrict__ out, int lo, const char *__restrict__ done, int dstride)
 {
+    pdl_enter();
     __shared__ double in[SS_MAX];
     const int r = reps[blockIdx.x];
     if (done && *(const int *)(done + (long)r * dstride)) return;
@@ -222,6 +227,7 @@ __global__ void k_ss_apply(const Seg *__restrict__ segs, const int *__restrict__
 __global__ void k_pcg_start(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ b,
                             const double *__restrict__ D, PcgScal *pc, double rtol)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][1];
     const RBlk B = T.d_blk[blockIdx.x];
     double v[1] = {0.0};
@@ -246,6 +252,7 @@ __global__ void k_pcg_start(RedTable T, const Seg *__restrict__ segs, const doub
 __global__ void k_pcg_g(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ b,
                         const double *__restrict__ y2, double *__restrict__ g)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     const Seg &s = segs[B.rep];
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
@@ -470,6 +477,7 @@ k_ps_setup(long npair, const int2 *__restrict__ pairs, const int *__restrict__ b
            const double *__restrict__ tab, int nrow, long ncoll, const int *__restrict__ coll_rep,
            const int *__restrict__ cptr, double *__restrict__ Sout, double *__restrict__ Pout)
 {
+    pdl_enter();
     __shared__ PsWarpSmem wsm[PS_THREADS / 32];
     const long nbp = (npair + blockDim.x - 1) / blockDim.x;
     if (blockIdx.x >= nbp) {
@@ -514,7 +522,7 @@ static void launch_ps_setup(Engine &E, cudaStream_t st)
 {
     const long npair = E.lub_npairs;
     const long nbp = (npair + PS_THREADS - 1) / PS_THREADS, nbc = (E.ncoll + PS_THREADS / 32 - 1) / (PS_THREADS / 32);
-    ::ps_launch_count++, k_ps_setup<<<(unsigned)(nbp + nbc), PS_THREADS, 0, st>>>(
+    ps_launch(k_ps_setup, (unsigned)(nbp + nbc), PS_THREADS, 0, st,
         npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.ncoll,
         E.d_coll_rep, E.d_lubc_ptr, E.d_pS, E.d_pP);
 }
@@ -571,6 +579,7 @@ __global__ void k_ps_L(long ntot, long ncoll, const int *__restrict__ coll_rep, 
                        const double *__restrict__ D, double *__restrict__ bead_part, const char *__restrict__ done,
                        int dstride)
 {
+    pdl_enter();
     const long nbb = (ntot + blockDim.x - 1) / blockDim.x;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     if (blockIdx.x >= nbb) {
@@ -612,7 +621,7 @@ static void launch_ps_L(Engine &E, const double *y, const double *add, double *v
 {
     const int thr = 128;
     const long nbb = (E.ntot + thr - 1) / thr, nbc = (E.ncoll + thr / 32 - 1) / (thr / 32);
-    ::ps_launch_count++, k_ps_L<<<(unsigned)(nbb + nbc), thr, 0, st>>>(
+    ps_launch(k_ps_L, (unsigned)(nbb + nbc), thr, 0, st,
         E.ntot, E.ncoll, E.d_coll_rep, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr, E.d_lub_cidx, E.d_pS,
         y, add, vel, top, D, bead_part, done, dstride);
 }
@@ -643,6 +652,7 @@ __global__ void k_ps_LT(long npair, const int2 *__restrict__ pairs, const int *_
                         const double *__restrict__ p, double *__restrict__ w, double *__restrict__ part,
                         const char *__restrict__ done, int dstride)
 {
+    pdl_enter();
     const long q = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LT_LANES;
     const int a = threadIdx.x % LT_LANES;
     const unsigned team = 0xffffu << (threadIdx.x & 16);
@@ -688,6 +698,7 @@ __global__ void k_ps_init(long npair, const int2 *__restrict__ pairs, const int 
                           const double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ pv,
                           double *__restrict__ part)
 {
+    pdl_enter();
     const long q = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LT_LANES;
     const int a = threadIdx.x % LT_LANES;
     const unsigned team = 0xffffu << (threadIdx.x & 16);
@@ -716,6 +727,7 @@ __global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const in
                             const double *__restrict__ pv, const double *__restrict__ Ap, double *__restrict__ yv,
                             double *__restrict__ rv, double *__restrict__ zv, double *__restrict__ part)
 {
+    pdl_enter();
     const long q = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LT_LANES;
     const int a = threadIdx.x % LT_LANES;
     const unsigned team = 0xffffu << (threadIdx.x & 16);
@@ -748,6 +760,7 @@ __global__ void k_ps_update(long npair, const int2 *__restrict__ pairs, const in
 __global__ void k_ps_dir(long npair, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs, int R,
                          const PcgScal *__restrict__ pc, const double *__restrict__ zv, double *__restrict__ pv)
 {
+    pdl_enter();
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= 12 * npair) return;
     const PcgScal &sc = pc[rep_of_b(bead_offs, R, pairs[e / 12].x)];
@@ -763,6 +776,7 @@ __global__ void k_ps_reduce(RedTable T, const int *__restrict__ cptr, const doub
                             const double *__restrict__ bead_part, const double *__restrict__ add0,
                             const double *__restrict__ add1, PcgScal *pc, int mode, int maxit, int *nactive)
 {
+    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][2];
     const RBlk B = T.d_blk[blockIdx.x];
     if (pc[B.rep].done) return;
@@ -802,6 +816,7 @@ __global__ void k_ps_reduce(RedTable T, const int *__restrict__ cptr, const doub
 __global__ void k_ps_c(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ b, double *__restrict__ c,
                        double *__restrict__ u)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     const Seg &s = segs[B.rep];
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
@@ -817,6 +832,7 @@ __global__ void k_ps_c(RedTable T, const Seg *__restrict__ segs, const double *_
 __global__ void k_ps_fin(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ y,
                          const double *__restrict__ y2, const double *__restrict__ g, double *__restrict__ x)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     const Seg &s = segs[B.rep];
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
@@ -830,6 +846,7 @@ __global__ void k_ps_fin(RedTable T, const Seg *__restrict__ segs, const double 
 // copy F_t (velocity layout) into the force rows of the saddle solution
 __global__ void k_ps_ft(RedTable T, const Seg *__restrict__ segs, const double *__restrict__ ft, double *__restrict__ x)
 {
+    pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
     const Seg &s = segs[B.rep];
     for (int e = threadIdx.x; e < B.len; e += RB_THREADS) {
@@ -850,6 +867,7 @@ __global__ void k_ps_S(long ntot, const int *__restrict__ bead_offs, int R, cons
                        double *__restrict__ zS, double *__restrict__ pS, double *__restrict__ ApS,
                        double *__restrict__ u, double *__restrict__ x, double *__restrict__ a0, double *__restrict__ a1)
 {
+    pdl_enter();
     long bd = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (bd >= ntot) return;
     const int r = rep_of_b(bead_offs, R, bd);
@@ -906,7 +924,7 @@ static void mr_apply(Engine &E, bool fp32, const void *dn, int ds, cudaStream_t 
 {
     apply_operator(E, 1, E.d_pu, E.d_py, nullptr, fp32, st, dn, ds);
     if (E.n_ss_reps) {
-        ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, E.d_py, 1, -1.0,
+        ps_launch(k_ss_apply, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_ssinv, E.d_py, 1, -1.0,
                                                                  nullptr, 1, 0.0, E.d_pu2, 1, (const char *)dn, ds);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, dn, ds, true);
     }
@@ -1160,6 +1178,7 @@ __device__ void pm_count_and_finish(int myrep, const Seg *__restrict__ segs, con
 __global__ void k_pm_elem(long npair, long ntot, const int2 *__restrict__ pairs, const int *__restrict__ bead_offs,
                           int R, const Seg *__restrict__ segs, MinresScal *mr, int mode, int k, PMArgs A, PMRed red)
 {
+    pdl_enter();
     const long gt = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long npt = npair * LT_LANES;
     int myrep = -1;                                   // replica of the item this thread counts
@@ -1296,15 +1315,15 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     // rhs into R[1]: pairs L^T (g + Mr b_bot), stresslets b_S + (M b_bot)_S
     mr_apply(E, fp32, dn, ds, st);
     if (npair)
-        ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+        ps_launch(k_ps_LT, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                               E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, A.R[1].pair,
                                                               nullptr, dn, ds);
-    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
+    ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
                                                   E.d_sv[0], A.R[1].s, E.d_sv[2], E.d_sv[3], E.d_sv[4], E.d_pu,
                                                   nullptr, A.sA, A.sB);
     *E.h_nactive = E.R;
     PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
-    ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+    ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                      E.d_pmr, 0, 0, A, red);
     PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
@@ -1315,9 +1334,9 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
             // Az = A z: u = [L z_y ; z_S] (z_S already in u), apply; mode 1 forms z_y + L^T (...)_t itself
             launch_ps_L(E, A.z.pair, nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds, st);
             mr_apply(E, fp32, dn, ds, st);
-            ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
+            ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                              E.d_segs, E.d_pmr, 1, k, A, red);
-            ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
+            ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                              E.d_segs, E.d_pmr, 2, k, A, red);
         }
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1325,7 +1344,7 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
         nact = *E.h_nactive;
     }
     // the last pending w/x update
-    ::ps_launch_count++, k_pm_elem<<<nbe, thr, 0, st>>>(npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+    ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                      E.d_pmr, 3, k + 1, A, red);
     PS_CK(cudaGetLastError());
     *ysol = A.x.pair;
@@ -1371,7 +1390,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     PS_CK(cudaMemsetAsync(E.d_pu, 0, sizeof(double) * E.ntop, st));
     PS_CK(cudaMemsetAsync(E.d_pu2, 0, sizeof(double) * E.ntop, st));
     PS_CK(cudaMemsetAsync(E.d_py2, 0, sizeof(double) * E.ntop, st));
-    ::ps_launch_count++, k_pcg_start<<<E.red.nblk, RB_THREADS, 0, st>>>(E.red, E.d_segs, b, E.d_D, E.d_pcg, o->rtol);
+    ps_launch(k_pcg_start, E.red.nblk, RB_THREADS, 0, st, E.red, E.d_segs, b, E.d_D, E.d_pcg, o->rtol);
     // the pair blocks depend on the staged positions and the table only: solves
     // that share a staging (the deterministic and the noise solve) set them up once
     if (npair && !E.ps_setup_valid) {
@@ -1379,14 +1398,14 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
         E.ps_setup_valid = true;
     }
     if (E.n_ss_reps) {
-        ::ps_launch_count++, k_ss_inverse<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, E.d_ssinv);
+        ps_launch(k_ss_inverse, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, E.d_ssinv);
         // g: u2 = [0 ; M_SS^{-1} b_S]
-        ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, nullptr,
+        ps_launch(k_ss_apply, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, nullptr,
                                                                  0, 0.0, E.d_pu2, 1, nullptr, 0);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, nullptr, 0, true);
     }
-    ::ps_launch_count++, k_pcg_g<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, E.d_py2, g);
-    ::ps_launch_count++, k_ps_c<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, b, cvel, E.d_pu);
+    ps_launch(k_pcg_g, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, b, E.d_py2, g);
+    ps_launch(k_ps_c, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, b, cvel, E.d_pu);
     PS_CK(cudaGetLastError());
     std::vector<PcgScal> hp(E.R);
     PS_CK(cudaMemcpyAsync(hp.data(), E.d_pcg, sizeof(PcgScal) * E.R, cudaMemcpyDeviceToHost, st));
@@ -1404,19 +1423,19 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
             // rhs = L^T (g + Mr b_bot) (joint replicas: Mr -> M, and b_S + (M b_bot)_S) ; r = rhs ; z = P r ; p = z
             mr_apply(E, fp32, dn, ds, st);
             if (npair) {
-                ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+                ps_launch(k_ps_LT, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                                       E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
                                                                       (const char *)dn, ds);
-                ::ps_launch_count++, k_ps_init<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                ps_launch(k_ps_init, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                         E.d_segs, E.d_pP, yv, rv, zv, pv, E.d_ppart);
             }
         }
         if (joint)
-            ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
+            ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
                                                       yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
         // initial residual ||D^{-1} L r||^2 + ||D^{-1} r_S||^2
         launch_ps_L(E, rv, nullptr, nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds, st);
-        ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA, sB,
+        ps_launch(k_ps_reduce, TB.nblk, RB_THREADS, 0, st, TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA, sB,
                                                                       E.d_pcg, 1, maxit, E.d_nactive);
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
@@ -1428,29 +1447,29 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                 launch_ps_L(E, pv, nullptr, nullptr, E.d_pu, nullptr, nullptr, (const char *)dn, ds, st);
                 mr_apply(E, fp32, dn, ds, st);
                 if (npair)
-                    ::ps_launch_count++, k_ps_LT<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                    ps_launch(k_ps_LT, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                           E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
                                                                           pv, Ap, E.d_ppart, (const char *)dn, ds);
                 if (joint)
-                    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 1, E.d_pcg, b, E.d_py,
+                    ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 1, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, nullptr);
-                ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, nullptr, sA,
+                ps_launch(k_ps_reduce, TB.nblk, RB_THREADS, 0, st, TB, E.d_lubc_ptr, E.d_ppart, nullptr, sA,
                                                                               nullptr, E.d_pcg, 0, maxit, E.d_nactive);
                 if (npair)
-                    ::ps_launch_count++, k_ps_update<<<nbp_lt, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                    ps_launch(k_ps_update, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                               E.d_segs, E.d_pcg, E.d_pP, pv, Ap, yv, rv,
                                                                               zv, E.d_ppart);
                 if (joint)
-                    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
+                    ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
                 launch_ps_L(E, rv, nullptr, nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds, st);
-                ::ps_launch_count++, k_ps_reduce<<<TB.nblk, RB_THREADS, 0, st>>>(TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA,
+                ps_launch(k_ps_reduce, TB.nblk, RB_THREADS, 0, st, TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA,
                                                                               sB, E.d_pcg, 2, maxit, E.d_nactive);
                 if (npair)
-                    ::ps_launch_count++, k_ps_dir<<<nbp_e, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R,
+                    ps_launch(k_ps_dir, nbp_e, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
                                                                            E.d_pcg, zv, pv);
                 if (joint)
-                    ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
+                    ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
                                                               E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
             }
             PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1460,14 +1479,14 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     }
     // F_t = -b_bot + L y (into u_t and the force rows), then U = Mr F_t - g, F_S
     launch_ps_L(E, yv, cvel, tmp, E.d_pu, nullptr, nullptr, nullptr, 0, st);
-    ::ps_launch_count++, k_ps_ft<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, tmp, x);
+    ps_launch(k_ps_ft, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, tmp, x);
     if (joint)
-        ::ps_launch_count++, k_ps_S<<<nbb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
+        ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
                                                   yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
     mr_apply(E, fp32, nullptr, 0, st);
-    ::ps_launch_count++, k_ps_fin<<<TV.nblk, RB_THREADS, 0, st>>>(TV, E.d_segs, E.d_py, E.d_py2, g, x);
+    ps_launch(k_ps_fin, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, E.d_py, E.d_py2, g, x);
     if (E.n_ss_reps)
-        ::ps_launch_count++, k_ss_apply<<<E.n_ss_reps, 64, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, E.d_py,
+        ps_launch(k_ss_apply, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, E.d_py,
                                                                  1, -1.0, x, 0, nullptr, 0);
     PS_CK(cudaGetLastError());
     int worst = 1000, itmax = 0;
@@ -1535,13 +1554,13 @@ int structured_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o
     unsigned nb = (unsigned)((E.nvec + thr - 1) / thr);
     double *y = E.d_Rr[0];
     bool fp32 = E.precision == PS_PREC_MIXED;
-    ::ps_launch_count++, k_struct_init<<<nb, thr, 0, st>>>(E.nvec, E.d_vec_offs, E.R, E.d_segs, b, x);
+    ps_launch(k_struct_init, nb, thr, 0, st, E.nvec, E.d_vec_offs, E.R, E.d_segs, b, x);
     if (E.n_ss_reps) {
         apply_operator(E, 0, x, y, nullptr, fp32, st);   // y_top = M [F_t ; 0]
-        ::ps_launch_count++, k_struct_ss<<<E.n_ss_reps, 256, 0, st>>>(E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, b, y, x);
+        ps_launch(k_struct_ss, E.n_ss_reps, 256, 0, st, E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, b, y, x);
     }
     apply_operator(E, 0, x, y, nullptr, fp32, st);       // y_top = M F
-    ::ps_launch_count++, k_struct_u<<<nb, thr, 0, st>>>(E.nvec, E.d_vec_offs, E.R, E.d_segs, b, y, x);
+    ps_launch(k_struct_u, nb, thr, 0, st, E.nvec, E.d_vec_offs, E.R, E.d_segs, b, y, x);
     PS_CK(cudaGetLastError());
     ps_ksp_result r0 = {2, 0, 0, 0.0};
     if (E.n_ss_polish) {
@@ -1567,6 +1586,7 @@ __global__ void k_lub_z(long npair, const int2 *__restrict__ pairs, const int *_
                         const Seg *__restrict__ segs, const int *__restrict__ cptr, const uint64_t *__restrict__ rseed,
                         const uint64_t *__restrict__ rstep, double *__restrict__ z)
 {
+    pdl_enter();
     const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npair) return;
     const int r = rep_of_b(bead_offs, R, pairs[q].x);
@@ -1578,6 +1598,7 @@ __global__ void k_lub_z(long npair, const int2 *__restrict__ pairs, const int *_
 __global__ void k_lub_noise_add(long nvel, const int *__restrict__ vel_offs, int R, const Seg *__restrict__ segs,
                                 const double *__restrict__ v, double *__restrict__ rhs)
 {
+    pdl_enter();
     const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvel) return;
     const Seg &s = segs[rep_at(vel_offs, R, k)];
@@ -1602,13 +1623,13 @@ int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st)
             E.zlub_cap = nz * 3 / 2 + 1024;
             PS_CK(cudaMalloc(&E.d_zlub, sizeof(double) * E.zlub_cap));
         }
-        ::ps_launch_count++, k_lub_z<<<nbp, PS_THREADS, 0, st>>>(npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
+        ps_launch(k_lub_z, nbp, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
                                                               E.d_lubc_ptr, E.d_rseed, E.d_rstep, E.d_zlub);
         z = E.d_zlub;
     }
     launch_ps_L(E, z, nullptr, E.d_tmp_vel, nullptr, nullptr, nullptr, nullptr, 0, st);
     const int thr = 256;
-    ::ps_launch_count++, k_lub_noise_add<<<(unsigned)((E.nvel + thr - 1) / thr), thr, 0, st>>>(
+    ps_launch(k_lub_noise_add, (unsigned)((E.nvel + thr - 1) / thr), thr, 0, st,
         E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_tmp_vel, rhs);
     PS_CK(cudaGetLastError());
     return PS_OK;

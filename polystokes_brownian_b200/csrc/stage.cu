@@ -46,6 +46,7 @@ __device__ __forceinline__ int rep_of(const int *__restrict__ offs, int R, long 
 __global__ void k_pack(long ntot, const double *__restrict__ x, const double *__restrict__ chain,
                        double4 *__restrict__ p64, float4 *__restrict__ p32, float4 *__restrict__ p32lo)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     double cx = x[3 * b], cy = x[3 * b + 1], cz = x[3 * b + 2], ch = chain[b];
@@ -63,6 +64,7 @@ __global__ void k_pack(long ntot, const double *__restrict__ x, const double *__
 // A max over the replica's own beads: independent of the other replicas.
 __global__ void k_aa_radius(const Seg *__restrict__ segs, const double *__restrict__ x, float *__restrict__ te2)
 {
+    pdl_enter();
     const Seg &s = segs[blockIdx.x];
     __shared__ double red[256];
     double m = 0.0;
@@ -83,9 +85,9 @@ int stage_pack(Engine &E, cudaStream_t st)
 {
     int thr = 256;
     E.ps_setup_valid = false;     // positions change: the pair-space blocks are stale
-    ::ps_launch_count++, k_pack<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(E.ntot, E.d_x, E.d_chain, E.d_pos64, E.d_pos32, E.d_pos32lo);
+    ps_launch(k_pack, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st, E.ntot, E.d_x, E.d_chain, E.d_pos64, E.d_pos32, E.d_pos32lo);
     if (E.n_aa_tiles)
-        ::ps_launch_count++, k_aa_radius<<<E.R, 256, 0, st>>>(E.d_segs, E.d_x, E.d_aa_te2);
+        ps_launch(k_aa_radius, E.R, 256, 0, st, E.d_segs, E.d_x, E.d_aa_te2);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
@@ -109,6 +111,7 @@ __device__ __forceinline__ int cell_coord(double v, double org, double size, int
 __global__ void k_cell_geo(const Seg *__restrict__ segs, const double *__restrict__ x, double *__restrict__ geo,
                            const long *__restrict__ cell_off)
 {
+    pdl_enter();
     // geo per replica (20 doubles): [0,10) the search grid, [10,20) the
     // reference's own grid of build_monomer_cell_list (cell_list.cpp:23-62),
     // each as org[3], size[3], nc[3], periodic.
@@ -207,6 +210,7 @@ __global__ void k_cell_assign(long ntot, const int *__restrict__ bead_offs, int 
                               const double *__restrict__ x, const double *__restrict__ geo,
                               const long *__restrict__ cell_off, int *__restrict__ cell, int *__restrict__ count)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int r = rep_of(bead_offs, R, b);
@@ -228,6 +232,7 @@ __global__ void k_cell_assign(long ntot, const int *__restrict__ bead_offs, int 
 __global__ void k_cell_fill(long ntot, const int *__restrict__ cell, const int *__restrict__ start,
                             int *__restrict__ fillc, int *__restrict__ sorted)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int c = cell[b];
@@ -243,6 +248,7 @@ constexpr int CELL_SORT_SERIAL = 64;
 __global__ void k_cell_sort(long ncells, const int *__restrict__ start, int *__restrict__ sorted,
                             int *__restrict__ big, int *__restrict__ nbig)
 {
+    pdl_enter();
     long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     int a = start[c], e = start[c + 1];
@@ -262,6 +268,7 @@ __global__ void k_cell_sort(long ncells, const int *__restrict__ start, int *__r
 __global__ void k_cell_sort_big(const int *__restrict__ start, int *__restrict__ sorted, const int *__restrict__ big,
                                 const int *__restrict__ nbig, int *__restrict__ tmp)
 {
+    pdl_enter();
     const int n = *nbig;
     for (int q = blockIdx.x; q < n; q += gridDim.x) {
         const int c = big[q], a = start[c], k = start[c + 1] - a;
@@ -279,20 +286,20 @@ __global__ void k_cell_sort_big(const int *__restrict__ start, int *__restrict__
 
 int stage_cells(Engine &E, cudaStream_t st, const long *d_cell_off, long ncells)
 {
-    ::ps_launch_count++, k_cell_geo<<<E.R, 256, 0, st>>>(E.d_segs, E.d_x, E.d_cellgeo, d_cell_off);
+    ps_launch(k_cell_geo, E.R, 256, 0, st, E.d_segs, E.d_x, E.d_cellgeo, d_cell_off);
     PS_CK(cudaMemsetAsync(E.d_cell_count, 0, sizeof(int) * (ncells + 1), st));
     int thr = 256;
     unsigned nb = (unsigned)((E.ntot + thr - 1) / thr);
-    ::ps_launch_count++, k_cell_assign<<<nb, thr, 0, st>>>(E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, d_cell_off, E.d_cell,
+    ps_launch(k_cell_assign, nb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, d_cell_off, E.d_cell,
                                       E.d_cell_count);
     int rc = exclusive_scan(E, E.d_cell_count, E.d_cell_start, ncells, st);
     if (rc) return rc;
     PS_CK(cudaMemsetAsync(E.d_cell_count, 0, sizeof(int) * (ncells + 1), st));
-    ::ps_launch_count++, k_cell_fill<<<nb, thr, 0, st>>>(E.ntot, E.d_cell, E.d_cell_start, E.d_cell_count, E.d_cell_sorted);
+    ps_launch(k_cell_fill, nb, thr, 0, st, E.ntot, E.d_cell, E.d_cell_start, E.d_cell_count, E.d_cell_sorted);
     PS_CK(cudaMemsetAsync(E.d_cell_nbig, 0, sizeof(int), st));
-    ::ps_launch_count++, k_cell_sort<<<(unsigned)((ncells + thr - 1) / thr), thr, 0, st>>>(ncells, E.d_cell_start, E.d_cell_sorted,
+    ps_launch(k_cell_sort, (unsigned)((ncells + thr - 1) / thr), thr, 0, st, ncells, E.d_cell_start, E.d_cell_sorted,
                                                                                         E.d_cell_big, E.d_cell_nbig);
-    ::ps_launch_count++, k_cell_sort_big<<<148, 256, 0, st>>>(E.d_cell_start, E.d_cell_sorted, E.d_cell_big, E.d_cell_nbig,
+    ps_launch(k_cell_sort_big, 148, 256, 0, st, E.d_cell_start, E.d_cell_sorted, E.d_cell_big, E.d_cell_nbig,
                                                              E.d_cell_tmp);
     PS_CK(cudaGetLastError());
     return PS_OK;
@@ -363,6 +370,7 @@ __device__ __forceinline__ double pair_geom(const Seg &s, const double *__restri
 __global__ void k_colloid_hs(long ncoll, const int *__restrict__ coll_rep, const Seg *__restrict__ segs,
                              const double *__restrict__ x, double *__restrict__ chs)
 {
+    pdl_enter();
     const long g = blockIdx.x;
     if (g >= ncoll) return;
     const int lane = threadIdx.x;
@@ -403,6 +411,7 @@ __global__ void k_forces(long ntot, const int *__restrict__ bead_offs, int R, co
                          const double *__restrict__ time, double *__restrict__ ktrap, const double *__restrict__ trapinfo,
                          const double *__restrict__ chs, double *__restrict__ rhs)
 {
+    pdl_enter();
     long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= ntot) return;
     int r = rep_of(bead_offs, R, b);
@@ -523,6 +532,7 @@ __global__ void k_forces(long ntot, const int *__restrict__ bead_offs, int R, co
 __global__ void k_trap_weaken(int R, const Seg *__restrict__ segs, const double *__restrict__ time,
                               double *__restrict__ ktrap, const double *__restrict__ trapinfo)
 {
+    pdl_enter();
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
     const double *ti = trapinfo + 3 * r;
@@ -534,6 +544,7 @@ __global__ void k_rhs_zero(long nvec, const int *__restrict__ vec_offs, int R, c
                            int drift, const double *__restrict__ fext, const int *__restrict__ vel_offs,
                            double *__restrict__ rhs)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvec) return;
     int r = rep_of(vec_offs, R, k);
@@ -553,17 +564,17 @@ __global__ void k_rhs_zero(long nvec, const int *__restrict__ vec_offs, int R, c
 int stage_rhs(Engine &E, int drift, const double *fext, double *rhs, cudaStream_t st)
 {
     int thr = 256;
-    ::ps_launch_count++, k_rhs_zero<<<(unsigned)((E.nvec + thr - 1) / thr), thr, 0, st>>>(E.nvec, E.d_vec_offs, E.R, E.d_segs, drift, fext,
+    ps_launch(k_rhs_zero, (unsigned)((E.nvec + thr - 1) / thr), thr, 0, st, E.nvec, E.d_vec_offs, E.R, E.d_segs, drift, fext,
                                                                      E.d_vel_offs, rhs);
     if (!drift) {
         if (E.ncoll)
-            ::ps_launch_count++, k_colloid_hs<<<(unsigned)E.ncoll, 32, 0, st>>>(E.ncoll, E.d_coll_rep, E.d_segs, E.d_x,
+            ps_launch(k_colloid_hs, (unsigned)E.ncoll, 32, 0, st, E.ncoll, E.d_coll_rep, E.d_segs, E.d_x,
                                                                              E.d_chs);
-        ::ps_launch_count++, k_forces<<<(unsigned)((E.ntot + thr - 1) / thr), thr, 0, st>>>(
+        ps_launch(k_forces, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
             E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_cellgeo, E.d_cell_offs,
             E.d_cell_start, E.d_cell_sorted, E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_time, E.d_ktrap,
             E.d_trapinfo, E.d_chs, rhs);
-        ::ps_launch_count++, k_trap_weaken<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_segs, E.d_time, E.d_ktrap, E.d_trapinfo);
+        ps_launch(k_trap_weaken, (E.R + 127) / 128, 128, 0, st, E.R, E.d_segs, E.d_time, E.d_ktrap, E.d_trapinfo);
     }
     PS_CK(cudaGetLastError());
     return PS_OK;
@@ -590,6 +601,7 @@ int stage_pairs(Engine &E, cudaStream_t st)
 __global__ void k_assemble(int R, const Seg *__restrict__ segs, const double *__restrict__ x,
                            const int *__restrict__ aa_last, double *__restrict__ tab, double *__restrict__ stale)
 {
+    pdl_enter();
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
     const Seg &s = segs[r];
@@ -681,6 +693,7 @@ __global__ void k_schur(const Seg *__restrict__ segs, const int *__restrict__ re
                         double *__restrict__ delta, double *__restrict__ schurQ, double *__restrict__ schurL,
                         const double *__restrict__ tab)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const int r = reps[blockIdx.x];
     const Seg &s = segs[r];
@@ -785,7 +798,7 @@ __global__ void k_schur(const Seg *__restrict__ segs, const int *__restrict__ re
 
 int stage_assemble(Engine &E, cudaStream_t st)
 {
-    ::ps_launch_count++, k_assemble<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_segs, E.d_x, E.d_aa_last, E.d_tab, E.d_stale);
+    ps_launch(k_assemble, (E.R + 127) / 128, 128, 0, st, E.R, E.d_segs, E.d_x, E.d_aa_last, E.d_tab, E.d_stale);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
@@ -795,7 +808,7 @@ int stage_schur(Engine &E, cudaStream_t st)
     if (!E.n_schur_reps) return PS_OK;
     size_t smem = sizeof(double) * (2 * 64 * 64 + 64);
     PS_CK(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ::ps_launch_count++, k_schur<<<E.n_schur_reps, 256, smem, st>>>(E.d_segs, E.d_schur_reps, E.d_x, E.d_delta, E.d_schurQ, E.d_schurL,
+    ps_launch(k_schur, E.n_schur_reps, 256, smem, st, E.d_segs, E.d_schur_reps, E.d_x, E.d_delta, E.d_schurQ, E.d_schurL,
                                                 E.d_tab);
     PS_CK(cudaGetLastError());
     return PS_OK;
@@ -806,6 +819,7 @@ int stage_schur(Engine &E, cudaStream_t st)
 __global__ void k_diag(long nvec, const int *__restrict__ vec_offs, int R, const Seg *__restrict__ segs,
                        const double *__restrict__ delta, const double *__restrict__ luby_diag, double *__restrict__ d)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvec) return;
     int r = rep_of(vec_offs, R, k);
@@ -829,7 +843,7 @@ __global__ void k_diag(long nvec, const int *__restrict__ vec_offs, int R, const
 int diag_saddle(Engine &E, double *d, cudaStream_t st)
 {
     int thr = 256;
-    ::ps_launch_count++, k_diag<<<(unsigned)((E.nvec + thr - 1) / thr), thr, 0, st>>>(E.nvec, E.d_vec_offs, E.R, E.d_segs, E.d_delta,
+    ps_launch(k_diag, (unsigned)((E.nvec + thr - 1) / thr), thr, 0, st, E.nvec, E.d_vec_offs, E.R, E.d_segs, E.d_delta,
                                                                  E.any_lub ? E.d_lub_diag : nullptr, d);
     PS_CK(cudaGetLastError());
     return PS_OK;

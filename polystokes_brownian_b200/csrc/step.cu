@@ -29,6 +29,7 @@ __device__ __forceinline__ int rep_lookup(const int *__restrict__ offs, int R, l
 __global__ void k_zero_colloid_dofs(long ntop, const int *__restrict__ top_offs, int R, const Seg *__restrict__ segs,
                                     const double *__restrict__ fb, double *__restrict__ u)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ntop) return;
     int r = rep_lookup(top_offs, R, k);
@@ -41,6 +42,7 @@ __global__ void k_shell_noise(const Seg *__restrict__ segs, const int *__restric
                               const double *__restrict__ ymcm, const double *__restrict__ schurQ,
                               const double *__restrict__ schurL, double *__restrict__ W)
 {
+    pdl_enter();
     __shared__ double yv[PS_MAX_NC11_SCHUR];
     const int r = reps[blockIdx.x];
     const Seg &s = segs[r];
@@ -70,11 +72,11 @@ int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps
     }
     if (E.n_schur_reps || E.n_sl_reps) {
         int thr = 256;
-        ::ps_launch_count++, k_zero_colloid_dofs<<<(unsigned)((E.ntop + thr - 1) / thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs,
+        ps_launch(k_zero_colloid_dofs, (unsigned)((E.ntop + thr - 1) / thr), thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs,
                                                                                   fb, E.d_tmp_top);
         apply_operator(E, 1, E.d_tmp_top, E.d_tmp_top2, nullptr, false, st);
         if (E.n_schur_reps)
-            ::ps_launch_count++, k_shell_noise<<<E.n_schur_reps, 128, 0, st>>>(E.d_segs, E.d_schur_reps, fb, E.d_tmp_top2,
+            ps_launch(k_shell_noise, E.n_schur_reps, 128, 0, st, E.d_segs, E.d_schur_reps, fb, E.d_tmp_top2,
                                                                                E.d_schurQ, E.d_schurL, W);
         if (E.n_sl_reps) {
             // above the dense Schur limit: Lanczos on the colloid Schur complement
@@ -96,6 +98,7 @@ int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps
 __global__ void k_normals(long n, const int *__restrict__ offs, int R, const uint64_t *__restrict__ rseed,
                           const uint64_t *__restrict__ rstep, int which, double *__restrict__ out)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     int r = rep_lookup(offs, R, k);
@@ -110,6 +113,7 @@ __global__ void k_normals(long n, const int *__restrict__ offs, int R, const uin
 __global__ void k_extract_vel(long nvel, const int *__restrict__ vel_offs, int R, const Seg *__restrict__ segs,
                               const double *__restrict__ X, double *__restrict__ out, int from)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvel) return;
     int r = rep_lookup(vel_offs, R, k);
@@ -122,6 +126,7 @@ __global__ void k_extract_vel(long nvel, const int *__restrict__ vel_offs, int R
 __global__ void k_add_noise(long ntop, const int *__restrict__ top_offs, int R, const Seg *__restrict__ segs,
                             const double *__restrict__ W, double *__restrict__ rhs)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ntop) return;
     int r = rep_lookup(top_offs, R, k);
@@ -135,6 +140,7 @@ __global__ void k_add_noise(long ntop, const int *__restrict__ top_offs, int R, 
 __global__ void k_probe(long n3, const int *__restrict__ bead_offs, int R, const Seg *__restrict__ segs,
                         double *__restrict__ x, const double *__restrict__ fext, double mult)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n3) return;
     long b = k / 3;
@@ -151,6 +157,7 @@ __global__ void k_step_pred(long n3, const int *__restrict__ bead_offs, int R, c
                             double *__restrict__ x, const double *__restrict__ fext, const double *__restrict__ ud,
                             const double *__restrict__ up)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n3) return;
     long b = k / 3;
@@ -174,6 +181,7 @@ __global__ void k_step_corr(long n3, const int *__restrict__ bead_offs, int R, c
                             double *__restrict__ up, const double *__restrict__ vdn, const double *__restrict__ vdc,
                             const double *__restrict__ vb)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n3) return;
     long b = k / 3;
@@ -199,6 +207,7 @@ __global__ void k_step_rot(long ncoll, const Seg *__restrict__ segs, const int *
                            double *__restrict__ up, const double *__restrict__ vdn, const double *__restrict__ vdc,
                            const double *__restrict__ vb, double *__restrict__ q)
 {
+    pdl_enter();
     long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncoll) return;
     int r = coll_rep[c];
@@ -224,6 +233,7 @@ __global__ void k_step_rot(long ncoll, const Seg *__restrict__ segs, const int *
 // v_brown = up - v_det_n
 __global__ void k_sub(long n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ out)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     out[k] = a[k] - b[k];
@@ -234,6 +244,7 @@ __global__ void k_drift_fin(long nvel, const int *__restrict__ vel_offs, int R, 
                             const double *__restrict__ Xd, const double *__restrict__ drift, double *__restrict__ ud,
                             double *__restrict__ sb, const double *__restrict__ sbp)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nvel) return;
     int r = rep_lookup(vel_offs, R, k);
@@ -244,12 +255,14 @@ __global__ void k_drift_fin(long nvel, const int *__restrict__ vel_offs, int R, 
 }
 __global__ void k_time(int R, const Seg *__restrict__ segs, double *__restrict__ t)
 {
+    pdl_enter();
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < R) t[r] += segs[r].dt;
 }
 
 __global__ void k_step_count(int R, uint64_t *__restrict__ rstep)
 {
+    pdl_enter();
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < R) rstep[r]++;
 }
@@ -276,6 +289,7 @@ static int stage(Engine &E, double *rhs, cudaStream_t st)
 // r = b - y
 __global__ void k_resid(long n, const double *__restrict__ b, const double *__restrict__ y, double *__restrict__ r)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) r[k] = b[k] - y[k];
 }
@@ -283,6 +297,7 @@ __global__ void k_resid(long n, const double *__restrict__ b, const double *__re
 // x += d
 __global__ void k_add(long n, const double *__restrict__ d, double *__restrict__ x)
 {
+    pdl_enter();
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) x[k] += d[k];
 }
@@ -313,12 +328,12 @@ static int solve(Engine &E, const double *b, double *x, int warm, const ps_step_
         const unsigned g = (unsigned)((E.nvec + thr - 1) / thr);
         for (int k = 0; k < sweeps; k++) {
             apply_operator(E, 0, x, E.d_ref_d, nullptr, false, st);
-            ::ps_launch_count++, k_resid<<<g, thr, 0, st>>>(E.nvec, b, E.d_ref_d, E.d_ref_r);
+            ps_launch(k_resid, g, thr, 0, st, E.nvec, b, E.d_ref_d, E.d_ref_r);
             ps_ksp_opts oc = o;
             oc.warm = 0;
             reason = run(E.d_ref_r, E.d_ref_d, oc);
             if (reason == PS_ERR_CUDA) return reason;
-            ::ps_launch_count++, k_add<<<g, thr, 0, st>>>(E.nvec, E.d_ref_d, x);
+            ps_launch(k_add, g, thr, 0, st, E.nvec, E.d_ref_d, x);
             its += kr.iters_max;
             worst = std::min(worst, kr.reason);
         }
@@ -336,12 +351,12 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
     const int thr = 256;
     int rc;
     if (res) { for (int k = 0; k < 5; k++) res->iters[k] = 0; res->reason = 1000; res->lanczos_iters = 0; res->lanczos_nneg = 0; }
-    ::ps_launch_count++, k_time<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_segs, E.d_time);
+    ps_launch(k_time, (E.R + 127) / 128, 128, 0, st, E.R, E.d_segs, E.d_time);
     PS_CK(cudaMemcpyAsync(E.d_xn, E.d_x, sizeof(double) * 3 * E.ntot, cudaMemcpyDeviceToDevice, st));
     // predictor stage at x_n
     if ((rc = stage(E, E.d_rhs, st))) return rc;
     if ((rc = solve(E, E.d_rhs, E.d_Xdet, 0, in, res, 0, st))) return rc;
-    ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xdet, E.d_vdn, 0);
+    ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xdet, E.d_vdn, 0);
     if (E.any_kT) {
         const double *fb = in ? in->fb : nullptr;
         const double *wr = in ? in->wrfd : nullptr;
@@ -354,18 +369,18 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
             wr = E.d_wr;
         }
         if (!fb) {
-            ::ps_launch_count++, k_normals<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_rseed, E.d_rstep, 0, E.d_fb);
+            ps_launch(k_normals, nb(E.ntop, thr), thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_rseed, E.d_rstep, 0, E.d_fb);
             fb = E.d_fb;
         }
         if (!wr) {
-            ::ps_launch_count++, k_normals<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_rseed, E.d_rstep, 1, E.d_wr);
+            ps_launch(k_normals, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_rseed, E.d_rstep, 1, E.d_wr);
             wr = E.d_wr;
         }
         ps_sqrt_opts so = {in && in->sqrt_kmax > 0 ? in->sqrt_kmax : 40, in && in->sqrt_tol > 0 ? in->sqrt_tol : 1e-6};
         ps_sqrt_result sr = {0, 0};
         if ((rc = slip_noise(E, fb, E.d_Wn, &so, &sr, st))) return rc;
         if (res) { res->lanczos_iters = sr.iters_max; res->lanczos_nneg = sr.nneg; }
-        ::ps_launch_count++, k_add_noise<<<nb(E.ntop, thr), thr, 0, st>>>(E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
+        ps_launch(k_add_noise, nb(E.ntop, thr), thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_Wn, E.d_rhs);
         if (E.any_lub && E.lub_npairs > 0) {
             // Brownian lubrication force: 12 normals per canonical pair, injected
             // or drawn from the replica's Philox stream
@@ -383,45 +398,45 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
             if ((rc = lub_noise(E, zl, E.d_rhs, st))) return rc;
         }
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
-        ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
-        ::ps_launch_count++, k_sub<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_up, E.d_vdn, E.d_vb);
+        ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
+        ps_launch(k_sub, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_up, E.d_vdn, E.d_vb);
         // drift(): fext <- W (the quirk of drift.cpp:13 overwrites the recorded forces)
         PS_CK(cudaMemcpyAsync(E.d_fext, wr, sizeof(double) * E.nvel, cudaMemcpyDeviceToDevice, st));
         long n3 = 3 * E.ntot;
-        ::ps_launch_count++, k_probe<<<nb(n3, thr), thr, 0, st>>>(n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, 1.0);
+        ps_launch(k_probe, nb(n3, thr), thr, 0, st, n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, 1.0);
         if ((rc = E.any_lub ? stage_pairs(E, st) : stage_pack(E, st))) return rc;
         if ((rc = stage_assemble(E, st))) return rc;
         if ((rc = stage_rhs(E, 1, E.d_fext, E.d_rhs, st))) return rc;
         if ((rc = solve(E, E.d_rhs, E.d_Xd, 0, in, res, 2, st))) return rc;
-        ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xd, E.d_drift, 0);
+        ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xd, E.d_drift, 0);
         PS_CK(cudaMemcpyAsync(E.d_X, E.d_Xd, sizeof(double) * E.nvec, cudaMemcpyDeviceToDevice, st));  // keep S(+)
-        ::ps_launch_count++, k_probe<<<nb(n3, thr), thr, 0, st>>>(n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, -2.0);
+        ps_launch(k_probe, nb(n3, thr), thr, 0, st, n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, -2.0);
         if ((rc = E.any_lub ? stage_pairs(E, st) : stage_pack(E, st))) return rc;
         if ((rc = stage_assemble(E, st))) return rc;
         if ((rc = stage_rhs(E, 1, E.d_fext, E.d_rhs, st))) return rc;
         if ((rc = solve(E, E.d_rhs, E.d_Xd, 1, in, res, 3, st))) return rc;
-        ::ps_launch_count++, k_drift_fin<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xd, E.d_drift, E.d_ud,
+        ps_launch(k_drift_fin, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xd, E.d_drift, E.d_ud,
                                                      E.d_sb, E.d_X);
     } else {
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
-        ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
-        ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_fext, 1);
+        ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
+        ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_fext, 1);
         PS_CK(cudaMemsetAsync(E.d_vb, 0, sizeof(double) * E.nvel, st));
         PS_CK(cudaMemsetAsync(E.d_ud, 0, sizeof(double) * E.nvel, st));
     }
     long n3 = 3 * E.ntot;
-    ::ps_launch_count++, k_step_pred<<<nb(n3, thr), thr, 0, st>>>(n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, E.d_ud, E.d_up);
+    ps_launch(k_step_pred, nb(n3, thr), thr, 0, st, n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_fext, E.d_ud, E.d_up);
     // corrector stage at x_pred
     if ((rc = stage(E, E.d_rhs, st))) return rc;
     if ((rc = solve(E, E.d_rhs, E.d_Xdet, 0, in, res, 4, st))) return rc;
-    ::ps_launch_count++, k_extract_vel<<<nb(E.nvel, thr), thr, 0, st>>>(E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xdet, E.d_vdc, 0);
-    ::ps_launch_count++, k_step_corr<<<nb(n3, thr), thr, 0, st>>>(n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xn, E.d_ud, E.d_up, E.d_vdn,
+    ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xdet, E.d_vdc, 0);
+    ps_launch(k_step_corr, nb(n3, thr), thr, 0, st, n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xn, E.d_ud, E.d_up, E.d_vdn,
                                              E.d_vdc, E.d_vb);
     if (E.ncoll)
-        ::ps_launch_count++, k_step_rot<<<nb(E.ncoll, 128), 128, 0, st>>>(E.ncoll, E.d_segs, E.d_coll_rep, E.d_up, E.d_vdn, E.d_vdc, E.d_vb,
+        ps_launch(k_step_rot, nb(E.ncoll, 128), 128, 0, st, E.ncoll, E.d_segs, E.d_coll_rep, E.d_up, E.d_vdn, E.d_vdc, E.d_vb,
                                                      E.d_q);
     E.step_counter++;
-    ::ps_launch_count++, k_step_count<<<(E.R + 127) / 128, 128, 0, st>>>(E.R, E.d_rstep);
+    ps_launch(k_step_count, (E.R + 127) / 128, 128, 0, st, E.R, E.d_rstep);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
