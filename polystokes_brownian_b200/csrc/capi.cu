@@ -396,7 +396,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         const int KM = 64;
         TRY_ALLOC(E.d_lzV, sizeof(double) * top * (KM + 1));
         TRY_ALLOC(E.d_lzq, sizeof(double) * top);
-        TRY_ALLOC(E.d_lzT, sizeof(double) * ((KM + 1) * R * 2 + KM * R * 2 + R));
+        TRY_ALLOC(E.d_lzT, sizeof(double) * ((KM + 1) * R * 3 + KM * R * 2 + R));
         TRY_ALLOC(E.d_lzs, 96 * R);          // Lanczos scalars, their snapshot, the checks' speculative verdicts
     }
     return PS_OK;

@@ -331,25 +331,17 @@ struct LzScal {
 };
 constexpr int LZ_KMAX = 64;
 
-// per block: partial dots of q against V_0..V_j, then last block stores h[]
-__global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, const double *__restrict__ q, int j,
-                          const LzScal *__restrict__ lz, double *__restrict__ h)
+// Partial dots of q (held by the block's threads in qv) against V_0..V_j, one
+// block of the table; the last block of the replica sums the partials in block
+// order into h[].  An inactive block contributes zeros.
+__device__ __forceinline__ void lz_dots_block(const RedTable &T, const RBlk &B, const double *__restrict__ V, long ldv,
+                                              const double (&qv)[RB_EPT], bool act, int j, double *__restrict__ h)
 {
-    pdl_enter();
     __shared__ double sh[RB_THREADS / 32][LZ_KMAX + 1];
     __shared__ bool last;
-    const RBlk B = T.d_blk[blockIdx.x];
-    const bool act = !lz[B.rep].done;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    // q held in registers (a block spans at most RB_EPT elements per thread);
     // eight basis vectors per pass keep 8 x RB_EPT loads in flight.  Each dot is
     // summed in element order and reduced by the same shuffle tree as one at a time.
-    double qv[RB_EPT];
-#pragma unroll
-    for (int k = 0; k < RB_EPT; k++) {
-        const int e = threadIdx.x + k * RB_THREADS;
-        qv[k] = (act && e < B.len) ? q[B.start + e] : 0.0;
-    }
     for (int i0 = 0; i0 <= j; i0 += 8) {
         double v[8];
 #pragma unroll
@@ -397,39 +389,125 @@ __global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, co
     if (threadIdx.x == 0) T.d_counter[B.rep] = 0;
 }
 
-// q -= sum_i h_i V_i ; accumulate h_j into the Lanczos diagonal
-__global__ void k_lz_sub(RedTable T, const double *__restrict__ V, long ldv, double *__restrict__ q, int j,
-                         const LzScal *__restrict__ lz, const double *__restrict__ h, double *__restrict__ alpha, int first)
+// h = V_0..V_j dotted with q (first pass of the Gram-Schmidt step)
+__global__ void k_lz_dots(RedTable T, const double *__restrict__ V, long ldv, const double *__restrict__ q, int j,
+                          const LzScal *__restrict__ lz, double *__restrict__ h)
 {
     pdl_enter();
     const RBlk B = T.d_blk[blockIdx.x];
-    if (lz[B.rep].done) return;
-    const double *hr = h + (long)(LZ_KMAX + 1) * B.rep;
-    // the thread's RB_EPT elements advance together, so each basis vector's
-    // loads are independent; per element the subtraction order is i = 0..j
+    const bool act = !lz[B.rep].done;
+    // q held in registers (a block spans at most RB_EPT elements per thread)
+    double qv[RB_EPT];
+#pragma unroll
+    for (int k = 0; k < RB_EPT; k++) {
+        const int e = threadIdx.x + k * RB_THREADS;
+        qv[k] = (act && e < B.len) ? q[B.start + e] : 0.0;
+    }
+    lz_dots_block(T, B, V, ldv, qv, act, j, h);
+}
+
+// The first pass's subtraction and the second pass's dots in one sweep:
+// q -= sum_i h_i V_i (per element in the order i = 0..j), alpha_j = h_j, then
+// h2 = V_0..V_j dotted with the new q, which the block still holds in registers.
+// The block's slices of V are read twice, the second time from cache.  Same
+// arithmetic, in the same order, as the subtraction and dots kernels one after
+// the other.
+__global__ void k_lz_sub_dots(RedTable T, const double *__restrict__ V, long ldv, double *__restrict__ q, int j,
+                              const LzScal *__restrict__ lz, const double *__restrict__ h, double *__restrict__ alpha,
+                              double *__restrict__ h2)
+{
+    pdl_enter();
+    const RBlk B = T.d_blk[blockIdx.x];
+    const bool act = !lz[B.rep].done;
+    double acc[RB_EPT];
+    if (act) {
+        const double *hr = h + (long)(LZ_KMAX + 1) * B.rep;
+#pragma unroll
+        for (int k = 0; k < RB_EPT; k++) {
+            const int e = threadIdx.x + k * RB_THREADS;
+            acc[k] = e < B.len ? q[B.start + e] : 0.0;
+        }
+#pragma unroll 4
+        for (int i = 0; i <= j; i++) {
+            const double hi = hr[i];
+            const double *Vi = V + (long)i * ldv + B.start;
+#pragma unroll
+            for (int k = 0; k < RB_EPT; k++) {
+                const int e = threadIdx.x + k * RB_THREADS;
+                if (e < B.len) acc[k] -= hi * Vi[e];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RB_EPT; k++) {
+            const int e = threadIdx.x + k * RB_THREADS;
+            if (e < B.len) q[B.start + e] = acc[k];
+            else acc[k] = 0.0;
+        }
+        if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start))
+            alpha[(long)LZ_KMAX * B.rep + j] = 0.0 + hr[j];
+    } else {
+#pragma unroll
+        for (int k = 0; k < RB_EPT; k++) acc[k] = 0.0;
+    }
+    lz_dots_block(T, B, V, ldv, acc, act, j, h2);
+}
+
+// The second pass's subtraction, the norm and the breakdown test in one sweep:
+// q -= sum_i h2_i V_i, alpha_j += h2_j, nrm2 = q.q summed as the segmented dot
+// sums it (the same elements per thread, shuffle tree and block order), and the
+// replica's last block records m = j + 1 and stops the replica on an invariant
+// subspace.  A done replica's blocks only take part in the norm, of its
+// unchanged q, as the segmented dot would.
+__global__ void k_lz_sub_norm(RedTable T, const double *__restrict__ V, long ldv, double *__restrict__ q, int j,
+                              LzScal *__restrict__ lz, const double *__restrict__ h2, double *__restrict__ alpha,
+                              double *__restrict__ nrm2)
+{
+    pdl_enter();
+    __shared__ double sh[RB_THREADS / 32][1];
+    const RBlk B = T.d_blk[blockIdx.x];
+    const bool act = !lz[B.rep].done;
     double acc[RB_EPT];
 #pragma unroll
     for (int k = 0; k < RB_EPT; k++) {
         const int e = threadIdx.x + k * RB_THREADS;
         acc[k] = e < B.len ? q[B.start + e] : 0.0;
     }
+    if (act) {
+        const double *hr = h2 + (long)(LZ_KMAX + 1) * B.rep;
 #pragma unroll 4
-    for (int i = 0; i <= j; i++) {
-        const double hi = hr[i];
-        const double *Vi = V + (long)i * ldv + B.start;
+        for (int i = 0; i <= j; i++) {
+            const double hi = hr[i];
+            const double *Vi = V + (long)i * ldv + B.start;
+#pragma unroll
+            for (int k = 0; k < RB_EPT; k++) {
+                const int e = threadIdx.x + k * RB_THREADS;
+                if (e < B.len) acc[k] -= hi * Vi[e];
+            }
+        }
 #pragma unroll
         for (int k = 0; k < RB_EPT; k++) {
             const int e = threadIdx.x + k * RB_THREADS;
-            if (e < B.len) acc[k] -= hi * Vi[e];
+            if (e < B.len) q[B.start + e] = acc[k];
         }
+        if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start))
+            alpha[(long)LZ_KMAX * B.rep + j] = alpha[(long)LZ_KMAX * B.rep + j] + hr[j];
     }
+    double v[1] = {0.0};
 #pragma unroll
     for (int k = 0; k < RB_EPT; k++) {
         const int e = threadIdx.x + k * RB_THREADS;
-        if (e < B.len) q[B.start + e] = acc[k];
+        if (e < B.len) v[0] += acc[k] * acc[k];
     }
-    if (threadIdx.x == 0 && (B.start == T.d_blk[T.d_first[B.rep]].start))
-        alpha[(long)LZ_KMAX * B.rep + j] = (first ? 0.0 : alpha[(long)LZ_KMAX * B.rep + j]) + hr[j];
+    block_sum<1>(v, sh);
+    double tot[1];
+    if (finish_block<1>(T, B, blockIdx.x, v, tot)) {
+        nrm2[B.rep] = tot[0];
+        LzScal &l = lz[B.rep];
+        if (!l.done) {
+            l.m = j + 1;
+            if (sqrt(tot[0]) <= 1e-12 * l.b0) l.done = 2;   // 2: finalise with m = j+1
+        }
+    }
 }
 
 // V_{j+1} = q / ||q||; beta_j = ||q||  (norm from nrm[rep])
@@ -634,23 +712,13 @@ __global__ void k_lz_combine(RedTable T, const double *__restrict__ V, long ldv,
     }
 }
 
-// breakdown: ||q|| tiny -> invariant subspace, stop extending
-__global__ void k_lz_breakdown(int R, LzScal *__restrict__ lz, const double *__restrict__ nrm2, int j)
-{
-    pdl_enter();
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= R || lz[r].done) return;
-    lz[r].m = j + 1;
-    if (sqrt(nrm2[r]) <= 1e-12 * lz[r].b0) lz[r].done = 2;   // 2: finalise with m = j+1
-}
-
 // One Lanczos iteration's orthogonalisation for small batches, in one launch:
 // one cluster of LZC_CTAS blocks per replica.  Both passes of the
 // reorthogonalisation (dots against V_0..V_j, then q -= V h), the norm, the
 // breakdown test and the next basis vector, with cluster barriers between the
 // phases and the cross-block sums read through distributed shared memory.
 // The arithmetic is bit for bit that of the launch sequence it replaces
-// (k_lz_dots, k_lz_sub, seg_dot, k_lz_breakdown, k_lz_next): the replica's
+// (k_lz_dots, k_lz_sub_dots, k_lz_sub_norm, k_lz_next): the replica's
 // vector is cut into the reduction table's RB_SPAN blocks, each half of a
 // block (RB_THREADS threads) forms an RB block's partials with the same
 // thread-to-element map, shuffle tree and warp order, and every sum over RB
@@ -807,6 +875,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     double *betad = alpha + (long)LZ_KMAX * E.R;            // [R][LZ_KMAX]
     double *gbuf = betad + (long)LZ_KMAX * E.R;             // [R][LZ_KMAX+1]
     double *nrm2 = gbuf + (long)(LZ_KMAX + 1) * E.R;        // [R]
+    double *h2 = nrm2 + E.R;                                // [R][LZ_KMAX+1]: the second pass's dots
     seg_dot(E, T, z, z, nrm2, st);
     ps_launch(k_lz_init, T.nblk, RB_THREADS, 0, st, T, E.d_segs, V, z, lz, nrm2);
     PS_CK(cudaMemsetAsync(gbuf, 0, sizeof(double) * (LZ_KMAX + 1) * E.R, st));
@@ -829,12 +898,10 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
             ::ps_launch_count++, k_lz_orth_cluster<<<E.R * LZC_CTAS, LZC_THREADS, 0, st>>>(E.d_segs, V, ldv, q, j, kmax, lz,
                                                                                        alpha, betad);
         } else {
-            for (int pass = 0; pass < 2; pass++) {
-                ps_launch(k_lz_dots, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h);
-                ps_launch(k_lz_sub, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h, alpha, pass == 0);
-            }
-            seg_dot(E, T, q, q, nrm2, st);
-            ps_launch(k_lz_breakdown, (E.R + 127) / 128, 128, 0, st, E.R, lz, nrm2, j);
+            // two-pass classical Gram-Schmidt in three sweeps over the basis, then the next vector
+            ps_launch(k_lz_dots, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h);
+            ps_launch(k_lz_sub_dots, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h, alpha, h2);
+            ps_launch(k_lz_sub_norm, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, h2, alpha, nrm2);
             if (j + 1 < kmax)
                 ps_launch(k_lz_next, T.nblk, RB_THREADS, 0, st, T, V, ldv, q, j, lz, nrm2, betad);
         }
