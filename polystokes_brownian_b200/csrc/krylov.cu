@@ -543,7 +543,9 @@ __global__ void k_lz_init(RedTable T, const Seg *__restrict__ segs, double *__re
 // the iteration's rotations (c, s) in rot; then every lane applies them, in the
 // recurrence's order, to its own rows of Z.  A row sees the same rotations in
 // the same order as when each rotation is applied to all rows at once, so Z is
-// the same, without a warp barrier per rotation.  rot holds 2 n doubles.
+// the same, without a warp barrier per rotation.  rot holds 2 n doubles;
+// n <= 64 (two rows of Z per lane).  The warp's lanes search for the split
+// point together.  Every lane of the warp takes part.
 __device__ void warp_tql(double *d, double *e, double *Z, double *rot, int n)
 {
     const int lane = threadIdx.x & 31;
@@ -552,13 +554,20 @@ __device__ void warp_tql(double *d, double *e, double *Z, double *rot, int n)
     for (int l = 0; l < n; l++) {
         int iter = 0;
         while (true) {
-            int m = l, go = 0, iend = l;
-            if (lane == 0) {
-                for (m = l; m < n - 1; m++) {
-                    double dd = fabs(d[m]) + fabs(d[m + 1]);
-                    if (fabs(e[m]) <= 1e-16 * dd) break;
+            // the first m >= l with a negligible e[m] (n - 1 if none), tested 32 at a time
+            int m = n - 1, iend = l;
+            for (int m0 = l; m0 < n - 1; m0 += 32) {
+                const int mm = m0 + lane;
+                bool hit = false;
+                if (mm < n - 1) {
+                    const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+                    hit = fabs(e[mm]) <= 1e-16 * dd;
                 }
-                go = (m != l) && (iter < 60);
+                const unsigned b = __ballot_sync(0xffffffffu, hit);
+                if (b) { m = m0 + __ffs(b) - 1; break; }
+            }
+            const bool go = (m != l) && (iter < 60);
+            if (lane == 0) {
                 if (go) {
                     double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
                     double r = hypot(g, 1.0);
@@ -590,18 +599,27 @@ __device__ void warp_tql(double *d, double *e, double *Z, double *rot, int n)
                 }
             }
             iter++;
-            m = __shfl_sync(0xffffffffu, m, 0);
-            go = __shfl_sync(0xffffffffu, go, 0);
             iend = __shfl_sync(0xffffffffu, iend, 0);
             if (!go) break;
             __syncwarp();                       // rot, d, e written by lane 0 are visible
-            for (int k = lane; k < n; k += 32)
+            // rows lane and lane + 32 (n <= 64) advance together, each in the order i = m-1 .. iend
+            const int k0 = lane, k1 = lane + 32;
+            if (k0 < n) {
+                double *Z0 = Z + k0 * n, *Z1 = Z + (k1 < n ? k1 : k0) * n;
+                const bool two = k1 < n;
                 for (int i = m - 1; i >= iend; i--) {
                     const double c = rot[2 * i], sn = rot[2 * i + 1];
-                    const double fz = Z[k * n + i + 1];
-                    Z[k * n + i + 1] = sn * Z[k * n + i] + c * fz;
-                    Z[k * n + i] = c * Z[k * n + i] - sn * fz;
+                    const double f0 = Z0[i + 1], g0 = Z0[i];
+                    double f1 = 0.0, g1 = 0.0;
+                    if (two) { f1 = Z1[i + 1]; g1 = Z1[i]; }
+                    Z0[i + 1] = sn * g0 + c * f0;
+                    Z0[i] = c * g0 - sn * f0;
+                    if (two) {
+                        Z1[i + 1] = sn * g1 + c * f1;
+                        Z1[i] = c * g1 - sn * f1;
+                    }
                 }
+            }
             __syncwarp();
         }
     }
