@@ -397,7 +397,7 @@ static int build(Engine &E, const ps_desc *descs, int R, int precision)
         TRY_ALLOC(E.d_lzV, sizeof(double) * top * (KM + 1));
         TRY_ALLOC(E.d_lzq, sizeof(double) * top);
         TRY_ALLOC(E.d_lzT, sizeof(double) * ((KM + 1) * R * 3 + KM * R * 2 + R));
-        TRY_ALLOC(E.d_lzs, 96 * R);          // Lanczos scalars, their snapshot, the checks' speculative verdicts
+        TRY_ALLOC(E.d_lzs, 96 * R);          // Lanczos scalars, their snapshot, the checks' speculative outcomes
     }
     return PS_OK;
 }

@@ -625,7 +625,7 @@ __device__ void warp_tql(double *d, double *e, double *Z, double *rot, int n)
     }
 }
 
-// A check's verdict for one replica, written by the speculative checks.
+// A check's outcome for one replica, written by the speculative checks.
 struct LzSpec {
     int conv;      // converged at m
     int m;
@@ -638,7 +638,7 @@ struct LzSpec {
 // final_ = 1: the final estimate, on the replica's own m when it is done, into lz.
 // final_ = 0: a speculative check beside the next basis vectors: it reads the
 // snapshot `snap` of lz taken when it was launched (the vectors that follow
-// move lz on) and writes its verdict into spec; the host applies it later
+// move lz on) and writes its outcome into spec; the host applies it later
 // (k_lz_spec_apply).  g_prev is the previous check's g in both cases.
 __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const LzScal *__restrict__ snap, LzSpec *__restrict__ spec,
                            const double *__restrict__ alpha, const double *__restrict__ betad, double *__restrict__ gbuf,
@@ -704,7 +704,7 @@ __global__ void k_lz_check(int R, LzScal *__restrict__ lz, const LzScal *__restr
     }
 }
 
-// a speculative check's verdict, applied in stream order after the vectors that
+// a speculative check's outcome, applied in stream order after the vectors that
 // ran beside it: a replica that had converged at m stops there (done, m), as if
 // the check had held the vectors back; the vectors it took meanwhile are unused
 __global__ void k_lz_spec_apply(int R, LzScal *__restrict__ lz, const LzSpec *__restrict__ spec)
@@ -905,7 +905,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     size_t smem = sizeof(double) * (4 * LZ_KMAX + LZ_KMAX * LZ_KMAX);
     std::vector<LzScal> hl(E.R);
     LzScal *snap = lz + E.R;                                 // the scalars when a check was launched
-    LzSpec *spec = (LzSpec *)(snap + E.R);                   // the checks' verdicts
+    LzSpec *spec = (LzSpec *)(snap + E.R);                   // the checks' outcomes
     LzSpec *hspec = (LzSpec *)E.h_spec;
     bool pending = false;
     int j = 0;
@@ -925,7 +925,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
         }
         if ((j + 1) % check == 0 && j + 1 < kmax) {
             if (pending) {
-                // the previous check (normally finished long before): apply its verdicts
+                // the previous check (normally finished long before): apply its outcomes
                 PS_CK(cudaEventSynchronize(E.ev_chk));
                 pending = false;
                 ps_launch(k_lz_spec_apply, (E.R + 127) / 128, 128, 0, st, E.R, lz, spec);
@@ -945,7 +945,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
         }
     }
     if (pending) {
-        // the last check's verdicts, and its g, ahead of the final estimate
+        // the last check's outcomes, and its g, ahead of the final estimate
         PS_CK(cudaStreamWaitEvent(st, E.ev_chk, 0));
         ps_launch(k_lz_spec_apply, (E.R + 127) / 128, 128, 0, st, E.R, lz, spec);
     }

@@ -169,7 +169,7 @@ struct Engine {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaStream_t side2 = nullptr;                  // Lanczos convergence checks beside the next basis vectors
     cudaEvent_t ev_fork2 = nullptr, ev_chk = nullptr;
-    void *h_spec = nullptr;                        // pinned copy of the checks' verdicts
+    void *h_spec = nullptr;                        // pinned copy of the checks' outcomes
 };
 
 // monomer column chunk width of the far-field AA kernels: process-wide (every
