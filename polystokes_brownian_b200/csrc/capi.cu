@@ -612,7 +612,7 @@ int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
     // trap centres from the colloids on a fresh start (Stokes.cpp:279-287), one launch for the batch
     if (E.ncoll)
         ps_launch(k_trap_centres, nbc, thr, 0, st, E.ncoll, E.d_coll_rep, E.d_segs, E.d_fresh, E.d_x,
-                                                              E.d_xpos0);
+                E.d_xpos0);
     PS_CK(cudaGetLastError());
     int rc = ps::stage_pack(E, st);
     return rc;

@@ -261,8 +261,8 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
     }
     // r_1 in slot 1 (slot k % 3 holds r_k)
     ps_launch(k_mr_init, T.nblk, RB_THREADS, 0, st, T, E.d_segs, b, Ax, E.d_D, E.d_Rr[1], E.d_z, x, E.d_mr, opt.warm,
-                                            opt.rtol, opt.maxit, E.d_v, E.d_W[0], E.d_W[1], E.d_W[2],
-                                            E.d_sinv);
+            opt.rtol, opt.maxit, E.d_v, E.d_W[0], E.d_W[1], E.d_W[2],
+            E.d_sinv);
     PS_CK(cudaGetLastError());
     // count active replicas
     std::vector<MinresScal> hm(E.R);
@@ -288,7 +288,7 @@ int minres_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *o, ps
                            (int)sizeof(MinresScal));
             ps_launch(k_mr_alpha, T.nblk, RB_THREADS, 0, st, T, E.d_z, E.d_v, Av, rkm1, wnew, w1, w2, x, E.d_mr, k);
             ps_launch(k_mr_beta, T.nblk, RB_THREADS, 0, st, T, Av, rk, E.d_D, E.d_z, E.d_mr, opt.maxit, E.d_nactive,
-                                                    E.d_sinv);
+                    E.d_sinv);
         }
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
@@ -938,7 +938,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
             PS_CK(cudaEventRecord(E.ev_fork2, st));
             PS_CK(cudaStreamWaitEvent(E.side2, E.ev_fork2, 0));
             ps_launch(k_lz_check, E.R, 32, smem, E.side2, E.R, lz, snap, spec, alpha, betad, gbuf, j + 1,
-                                                                    tol, 0);
+                    tol, 0);
             PS_CK(cudaMemcpyAsync(hspec, spec, sizeof(LzSpec) * E.R, cudaMemcpyDeviceToHost, E.side2));
             PS_CK(cudaEventRecord(E.ev_chk, E.side2));
             pending = true;
@@ -951,7 +951,7 @@ int lanczos_sqrt(Engine &E, const double *z, double *w, const ps_sqrt_opts *o, p
     }
     // final estimate: replicas at the cap, replicas stopped by breakdown, and the converged ones on their own m
     ps_launch(k_lz_check, E.R, 32, smem, st, E.R, lz, snap, spec, alpha, betad, gbuf,
-                                                        std::min(j + 1, kmax), tol, 1);
+            std::min(j + 1, kmax), tol, 1);
     ps_launch(k_lz_combine, T.nblk, RB_THREADS, 0, st, T, V, ldv, lz, gbuf, w);
     PS_CK(cudaMemcpyAsync(hl.data(), lz, sizeof(LzScal) * E.R, cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
@@ -1141,13 +1141,13 @@ int schur_lanczos_noise(Engine &E, const double *fb, const double *ymcm, double 
     const unsigned gb = (unsigned)((E.ntop + thr - 1) / thr);
     for (int j = 0; j < kmax; j++) {
         ps_launch(k_sl_load, gb, thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 0,
-                                                           nullptr, E.d_sl_u);
+                nullptr, E.d_sl_u);
         apply_operator(E, 1, E.d_sl_u, E.d_sl_y, nullptr, false, st, E.d_sl_skip, (int)sizeof(int));
         ps_launch(k_sl_load, gb, thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs, E.d_slV, sc, j, 1,
-                                                           E.d_sl_y, E.d_sl_u);
+                E.d_sl_y, E.d_sl_u);
         apply_operator(E, 1, E.d_sl_u, E.d_sl_y2, nullptr, false, st, E.d_sl_skip, (int)sizeof(int));
         ps_launch(k_sl_iter, ns, SL_THREADS, 0, st, E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc,
-                                                                  E.d_sl_skip, E.d_sl_y, E.d_sl_y2, j);
+                E.d_sl_skip, E.d_sl_y, E.d_sl_y2, j);
     }
     ps_launch(k_sl_finish, ns, SL_THREADS, 0, st, E.d_segs, E.d_sl_reps, E.d_slV, E.d_slT, sc, fb, ymcm, W);
     // the operator applies of the next noise draw start from the Lanczos set again

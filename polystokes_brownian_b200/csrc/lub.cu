@@ -170,9 +170,9 @@ int lub_build(Engine &E, cudaStream_t st)
     ps_launch(k_canon_count, nb, thr, 0, st, E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_nbr_count);
     if ((rc = exclusive_scan(E, E.d_nbr_count, E.d_lubc_ptr, E.ntot, st))) return rc;
     ps_launch(k_canon_fill, nb, thr, 0, st, E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
-                                                       E.d_lub_pairs);
+            E.d_lub_pairs);
     ps_launch(k_canon_map, nb, thr, 0, st, E.ntot, E.d_lub_ptr, E.d_lub_nbr, E.d_lubc_ptr, E.d_lubc_nbr,
-                                                      E.d_lub_cidx);
+            E.d_lub_cidx);
     E.lub_npairs = nc;
     PS_CK(cudaGetLastError());
     return PS_OK;
@@ -182,16 +182,16 @@ void lub_apply(Engine &E, const double *x_saddle, double *y_vel, cudaStream_t st
 {
     int thr = 128;
     ps_launch(k_lub_apply, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, x_saddle, 1,
-        y_vel, nullptr);
+            E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, x_saddle, 1,
+            y_vel, nullptr);
 }
 
 void lub_apply_vel(Engine &E, const double *u_vel, double *y_vel, cudaStream_t st)
 {
     int thr = 128;
     ps_launch(k_lub_apply, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, u_vel, 0,
-        y_vel, nullptr);
+            E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, u_vel, 0,
+            y_vel, nullptr);
 }
 
 int lub_diag(Engine &E, cudaStream_t st)
@@ -200,8 +200,8 @@ int lub_diag(Engine &E, cudaStream_t st)
     PS_CK(cudaMemsetAsync(E.d_lub_diag, 0, sizeof(double) * E.nvel, st));
     PS_CK(cudaMemsetAsync(E.d_tmp_vel, 0, sizeof(double) * E.nvel, st));
     ps_launch(k_lub_apply, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_tmp_vel, 0,
-        E.d_tmp_vel2, E.d_lub_diag);
+            E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_lubtab, E.lub_nrow, E.d_lub_ptr, E.d_lub_nbr, E.d_tmp_vel, 0,
+            E.d_tmp_vel2, E.d_lub_diag);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

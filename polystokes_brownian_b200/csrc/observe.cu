@@ -139,11 +139,11 @@ int obs_sample(Engine &E, cudaStream_t st)
     if (!E.d_obs_acc) { set_error("ps_observe: call ps_obs_reset first"); return PS_ERR_STATE; }
     int thr = 128;
     ps_launch(k_observe, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
-        E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_bond_ptr, E.d_bond_nbr, E.d_obs_acc, E.d_obs_prev,
-        E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.obs_nbins, E.obs_bmax, E.obs_tmax);
+            E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_bond_ptr, E.d_bond_nbr, E.d_obs_acc, E.d_obs_prev,
+            E.d_obs_hasprev, E.d_obs_hb, E.d_obs_ht, E.obs_nbins, E.obs_bmax, E.obs_tmax);
     if (E.ncoll)
         ps_launch(k_observe_msd, (unsigned)((E.ncoll + thr - 1) / thr), thr, 0, st,
-            E.ncoll, E.d_coll_rep, E.d_segs, E.d_x, E.d_obs_ring, E.d_obs_msd, E.d_obs_msdn, E.obs_lags, E.obs_n);
+                E.ncoll, E.d_coll_rep, E.d_segs, E.d_x, E.d_obs_ring, E.d_obs_msd, E.d_obs_msdn, E.obs_lags, E.obs_n);
     PS_CK(cudaGetLastError());
     E.obs_n++;
     return PS_OK;

@@ -320,7 +320,7 @@ int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
     int thr = 128;
     unsigned nbk = (unsigned)((E.ntot + thr - 1) / thr + (E.ncoll + thr / 32 - 1) / (thr / 32));
     ps_launch(k_pairs_count, nbk, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
-                                       E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_count);
+            E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_count);
     int rc = exclusive_scan(E, E.d_nbr_count, E.d_nbr_ptr, E.ntot, st);
     if (rc) return rc;
     int tot = 0;
@@ -332,7 +332,7 @@ int build_list(Engine &E, int which, long *npairs, cudaStream_t st)
         PS_CK(cudaMalloc(&E.d_nbr, sizeof(int) * E.nbr_cap));
     }
     ps_launch(k_pairs_fill, nbk, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, E.d_cell_offs,
-                                      E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_ptr, E.d_nbr);
+            E.d_cell_start, E.d_cell_sorted, E.ncoll, E.d_coll_rep, which, E.d_nbr_ptr, E.d_nbr);
     PS_CK(cudaGetLastError());
     *npairs = tot;
     return PS_OK;

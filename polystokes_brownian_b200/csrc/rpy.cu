@@ -687,27 +687,27 @@ void launch_pairs(Engine &E, const double *u, int in_top, cudaStream_t st, const
         {
             if (E.any_aa_rpy)
                 ps_launch(k_rpy_aa_f2<false>, dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st,
-                    E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
-                    E.part_stride, E.nch_aa, done, dstride);
+                        E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
+                        E.part_stride, E.nch_aa, done, dstride);
             if (E.any_aa_ref)
                 ps_launch(k_rpy_aa_f2<true>, dim3(E.n_aa_tiles, E.nch_aa), AAF_THREADS, 0, st,
-                    E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
-                    E.part_stride, E.nch_aa, done, dstride);
+                        E.d_segs, E.d_aa_tiles, E.d_pos32, E.d_pos32lo, E.d_aa_te2, E.d_pos64, u, in_top, E.d_partAA,
+                        E.part_stride, E.nch_aa, done, dstride);
         }
         else
             ps_launch(k_rpy_aa_d2, dim3(E.n_aa_tiles, E.nch_aa), AAD_THREADS, 0, st,
-                E.d_segs, E.d_aa_tiles, E.d_pos64, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
+                    E.d_segs, E.d_aa_tiles, E.d_pos64, u, in_top, E.d_partAA, E.part_stride, E.nch_aa, done, dstride);
     }
     if (E.n_ab_tiles)
         ps_launch(k_rpy_ab<T>, E.n_ab_tiles, RPY_THREADS, 0, ss, E.d_segs, E.d_ab_tiles, pos, E.d_pos32lo, u, in_top, E.d_tab, E.d_partAB,
-                                                         E.d_partBA, done, dstride);
+                E.d_partBA, done, dstride);
     // colloid-colloid FTS blocks stay FP64 in the mixed form: near contact the
     // far-field FTS mobility is ill-conditioned and FP32 blocks leave a 1.2e-6
     // velocity error on a suspension at gap 0.01 (FP64: tracks rtol); they are
     // cheap wherever monomers carry the O(N^2) work
     if (E.n_bb_tiles)
         ps_launch(k_rpy_bb<double>, dim3(E.n_bb_tiles, E.nch_bb), RPY_THREADS * BB_SPLIT, 0, ss,
-            E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, in_top, E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
+                E.d_segs, E.d_bb_tiles, E.d_pos64, E.d_pos32lo, u, in_top, E.d_partBB, E.part_stride, E.nch_bb, done, dstride);
     if (fork) {
         cudaEventRecord(E.ev_join, E.side);
         cudaStreamWaitEvent(st, E.ev_join, 0);
@@ -728,8 +728,8 @@ void apply_operator(Engine &E, int mode, const double *x, double *y, const doubl
     }
     const RedTable &T = mode == 0 ? E.red : E.red_top;
     ps_launch(k_combine, dim3((unsigned)T.nblk, RB_EPT), RB_THREADS, 0, st,
-        E.d_segs, T, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
-        E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
+            E.d_segs, T, mode, x, scale, E.d_partAA, skip_aa ? 0 : E.nch_aa, E.d_partAB, E.d_partBB, E.nch_bb,
+            E.d_partBA, E.d_delta, lub_y, E.part_stride, y, dn, done_stride);
 }
 
 

@@ -523,8 +523,8 @@ static void launch_ps_setup(Engine &E, cudaStream_t st)
     const long npair = E.lub_npairs;
     const long nbp = (npair + PS_THREADS - 1) / PS_THREADS, nbc = (E.ncoll + PS_THREADS / 32 - 1) / (PS_THREADS / 32);
     ps_launch(k_ps_setup, (unsigned)(nbp + nbc), PS_THREADS, 0, st,
-        npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.ncoll,
-        E.d_coll_rep, E.d_lubc_ptr, E.d_pS, E.d_pP);
+            npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_chain, E.d_lubtab, E.lub_nrow, E.ncoll,
+            E.d_coll_rep, E.d_lubc_ptr, E.d_pS, E.d_pP);
 }
 
 // v = L y (+ add): per bead, the rows of S_q y_q that belong to it, summed over
@@ -622,8 +622,8 @@ static void launch_ps_L(Engine &E, const double *y, const double *add, double *v
     const int thr = 128;
     const long nbb = (E.ntot + thr - 1) / thr, nbc = (E.ncoll + thr / 32 - 1) / (thr / 32);
     ps_launch(k_ps_L, (unsigned)(nbb + nbc), thr, 0, st,
-        E.ntot, E.ncoll, E.d_coll_rep, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr, E.d_lub_cidx, E.d_pS,
-        y, add, vel, top, D, bead_part, done, dstride);
+            E.ntot, E.ncoll, E.d_coll_rep, E.d_bead_offs, E.R, E.d_segs, E.d_lub_ptr, E.d_lub_nbr, E.d_lub_cidx, E.d_pS,
+            y, add, vel, top, D, bead_part, done, dstride);
 }
 
 // w_q = sign * S_q z_q (+ p_q), z gathered from the velocity rows of the Mr apply
@@ -925,7 +925,7 @@ static void mr_apply(Engine &E, bool fp32, const void *dn, int ds, cudaStream_t 
     apply_operator(E, 1, E.d_pu, E.d_py, nullptr, fp32, st, dn, ds);
     if (E.n_ss_reps) {
         ps_launch(k_ss_apply, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_ssinv, E.d_py, 1, -1.0,
-                                                                 nullptr, 1, 0.0, E.d_pu2, 1, (const char *)dn, ds);
+                nullptr, 1, 0.0, E.d_pu2, 1, (const char *)dn, ds);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, dn, ds, true);
     }
 }
@@ -1316,15 +1316,15 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     mr_apply(E, fp32, dn, ds, st);
     if (npair)
         ps_launch(k_ps_LT, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                              E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, A.R[1].pair,
-                                                              nullptr, dn, ds);
+                E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, A.R[1].pair,
+                nullptr, dn, ds);
     ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
-                                                  E.d_sv[0], A.R[1].s, E.d_sv[2], E.d_sv[3], E.d_sv[4], E.d_pu,
-                                                  nullptr, A.sA, A.sB);
+            E.d_sv[0], A.R[1].s, E.d_sv[2], E.d_sv[3], E.d_sv[4], E.d_pu,
+            nullptr, A.sA, A.sB);
     *E.h_nactive = E.R;
     PS_CK(cudaMemcpyAsync(E.d_nactive, E.h_nactive, sizeof(int), cudaMemcpyHostToDevice, st));
     ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                     E.d_pmr, 0, 0, A, red);
+            E.d_pmr, 0, 0, A, red);
     PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
     PS_CK(cudaStreamSynchronize(st));
     int nact = *E.h_nactive, k = 0;
@@ -1335,9 +1335,9 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
             launch_ps_L(E, A.z.pair, nullptr, nullptr, E.d_pu, nullptr, nullptr, dn, ds, st);
             mr_apply(E, fp32, dn, ds, st);
             ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                             E.d_segs, E.d_pmr, 1, k, A, red);
+                    E.d_segs, E.d_pmr, 1, k, A, red);
             ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                             E.d_segs, E.d_pmr, 2, k, A, red);
+                    E.d_segs, E.d_pmr, 2, k, A, red);
         }
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
@@ -1345,7 +1345,7 @@ static int pair_minres(Engine &E, const double *b, const double *g, int maxit, d
     }
     // the last pending w/x update
     ps_launch(k_pm_elem, nbe, thr, 0, st, npair, E.ntot, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                     E.d_pmr, 3, k + 1, A, red);
+            E.d_pmr, 3, k + 1, A, red);
     PS_CK(cudaGetLastError());
     *ysol = A.x.pair;
     *ssol = A.x.s;
@@ -1401,7 +1401,7 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
         ps_launch(k_ss_inverse, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_x, E.d_delta, E.d_ssinv);
         // g: u2 = [0 ; M_SS^{-1} b_S]
         ps_launch(k_ss_apply, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, nullptr,
-                                                                 0, 0.0, E.d_pu2, 1, nullptr, 0);
+                0, 0.0, E.d_pu2, 1, nullptr, 0);
         apply_operator(E, 1, E.d_pu2, E.d_py2, nullptr, fp32, st, nullptr, 0, true);
     }
     ps_launch(k_pcg_g, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, b, E.d_py2, g);
@@ -1424,19 +1424,19 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
             mr_apply(E, fp32, dn, ds, st);
             if (npair) {
                 ps_launch(k_ps_LT, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                                      E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
-                                                                      (const char *)dn, ds);
+                        E.d_pS, E.d_py, E.d_py2, g, 1.0, nullptr, rv, nullptr,
+                        (const char *)dn, ds);
                 ps_launch(k_ps_init, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                        E.d_segs, E.d_pP, yv, rv, zv, pv, E.d_ppart);
+                        E.d_segs, E.d_pP, yv, rv, zv, pv, E.d_ppart);
             }
         }
         if (joint)
             ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 0, E.d_pcg, b, E.d_py, E.d_D,
-                                                      yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
+                    yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
         // initial residual ||D^{-1} L r||^2 + ||D^{-1} r_S||^2
         launch_ps_L(E, rv, nullptr, nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds, st);
         ps_launch(k_ps_reduce, TB.nblk, RB_THREADS, 0, st, TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA, sB,
-                                                                      E.d_pcg, 1, maxit, E.d_nactive);
+                E.d_pcg, 1, maxit, E.d_nactive);
         PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
         PS_CK(cudaStreamSynchronize(st));
         nact = *E.h_nactive;
@@ -1448,29 +1448,29 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
                 mr_apply(E, fp32, dn, ds, st);
                 if (npair)
                     ps_launch(k_ps_LT, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                          E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
-                                                                          pv, Ap, E.d_ppart, (const char *)dn, ds);
+                            E.d_segs, E.d_pS, E.d_py, E.d_py2, nullptr, 1.0,
+                            pv, Ap, E.d_ppart, (const char *)dn, ds);
                 if (joint)
                     ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 1, E.d_pcg, b, E.d_py,
-                                                              E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, nullptr);
+                            E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, nullptr);
                 ps_launch(k_ps_reduce, TB.nblk, RB_THREADS, 0, st, TB, E.d_lubc_ptr, E.d_ppart, nullptr, sA,
-                                                                              nullptr, E.d_pcg, 0, maxit, E.d_nactive);
+                        nullptr, E.d_pcg, 0, maxit, E.d_nactive);
                 if (npair)
                     ps_launch(k_ps_update, nbp_lt, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                              E.d_segs, E.d_pcg, E.d_pP, pv, Ap, yv, rv,
-                                                                              zv, E.d_ppart);
+                            E.d_segs, E.d_pcg, E.d_pP, pv, Ap, yv, rv,
+                            zv, E.d_ppart);
                 if (joint)
                     ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 2, E.d_pcg, b, E.d_py,
-                                                              E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
+                            E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, sA, sB);
                 launch_ps_L(E, rv, nullptr, nullptr, nullptr, E.d_D, bead_part, (const char *)dn, ds, st);
                 ps_launch(k_ps_reduce, TB.nblk, RB_THREADS, 0, st, TB, E.d_lubc_ptr, E.d_ppart, bead_part, sA,
-                                                                              sB, E.d_pcg, 2, maxit, E.d_nactive);
+                        sB, E.d_pcg, 2, maxit, E.d_nactive);
                 if (npair)
                     ps_launch(k_ps_dir, nbp_e, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R,
-                                                                           E.d_pcg, zv, pv);
+                            E.d_pcg, zv, pv);
                 if (joint)
                     ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 3, E.d_pcg, b, E.d_py,
-                                                              E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
+                            E.d_D, yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
             }
             PS_CK(cudaMemcpyAsync(E.h_nactive, E.d_nactive, sizeof(int), cudaMemcpyDeviceToHost, st));
             PS_CK(cudaStreamSynchronize(st));
@@ -1482,12 +1482,12 @@ static int pair_solve(Engine &E, const double *b, double *x, const ps_ksp_opts *
     ps_launch(k_ps_ft, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, tmp, x);
     if (joint)
         ps_launch(k_ps_S, nbb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, 4, E.d_pcg, b, E.d_py, E.d_D,
-                                                  yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
+                yS, rS, zS, pS, ApS, E.d_pu, x, nullptr, nullptr);
     mr_apply(E, fp32, nullptr, 0, st);
     ps_launch(k_ps_fin, TV.nblk, RB_THREADS, 0, st, TV, E.d_segs, E.d_py, E.d_py2, g, x);
     if (E.n_ss_reps)
         ps_launch(k_ss_apply, E.n_ss_reps, 64, 0, st, E.d_segs, E.d_ss_reps, E.d_ssinv, b, 0, 1.0, E.d_py,
-                                                                 1, -1.0, x, 0, nullptr, 0);
+                1, -1.0, x, 0, nullptr, 0);
     PS_CK(cudaGetLastError());
     int worst = 1000, itmax = 0;
     long itsum = 0;
@@ -1624,13 +1624,13 @@ int lub_noise(Engine &E, const double *z, double *rhs, cudaStream_t st)
             PS_CK(cudaMalloc(&E.d_zlub, sizeof(double) * E.zlub_cap));
         }
         ps_launch(k_lub_z, nbp, PS_THREADS, 0, st, npair, E.d_lub_pairs, E.d_bead_offs, E.R, E.d_segs,
-                                                              E.d_lubc_ptr, E.d_rseed, E.d_rstep, E.d_zlub);
+                E.d_lubc_ptr, E.d_rseed, E.d_rstep, E.d_zlub);
         z = E.d_zlub;
     }
     launch_ps_L(E, z, nullptr, E.d_tmp_vel, nullptr, nullptr, nullptr, nullptr, 0, st);
     const int thr = 256;
     ps_launch(k_lub_noise_add, (unsigned)((E.nvel + thr - 1) / thr), thr, 0, st,
-        E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_tmp_vel, rhs);
+            E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_tmp_vel, rhs);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

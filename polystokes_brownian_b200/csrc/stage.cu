@@ -291,16 +291,16 @@ int stage_cells(Engine &E, cudaStream_t st, const long *d_cell_off, long ncells)
     int thr = 256;
     unsigned nb = (unsigned)((E.ntot + thr - 1) / thr);
     ps_launch(k_cell_assign, nb, thr, 0, st, E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_cellgeo, d_cell_off, E.d_cell,
-                                      E.d_cell_count);
+            E.d_cell_count);
     int rc = exclusive_scan(E, E.d_cell_count, E.d_cell_start, ncells, st);
     if (rc) return rc;
     PS_CK(cudaMemsetAsync(E.d_cell_count, 0, sizeof(int) * (ncells + 1), st));
     ps_launch(k_cell_fill, nb, thr, 0, st, E.ntot, E.d_cell, E.d_cell_start, E.d_cell_count, E.d_cell_sorted);
     PS_CK(cudaMemsetAsync(E.d_cell_nbig, 0, sizeof(int), st));
     ps_launch(k_cell_sort, (unsigned)((ncells + thr - 1) / thr), thr, 0, st, ncells, E.d_cell_start, E.d_cell_sorted,
-                                                                                        E.d_cell_big, E.d_cell_nbig);
+            E.d_cell_big, E.d_cell_nbig);
     ps_launch(k_cell_sort_big, 148, 256, 0, st, E.d_cell_start, E.d_cell_sorted, E.d_cell_big, E.d_cell_nbig,
-                                                             E.d_cell_tmp);
+            E.d_cell_tmp);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
@@ -565,15 +565,15 @@ int stage_rhs(Engine &E, int drift, const double *fext, double *rhs, cudaStream_
 {
     int thr = 256;
     ps_launch(k_rhs_zero, (unsigned)((E.nvec + thr - 1) / thr), thr, 0, st, E.nvec, E.d_vec_offs, E.R, E.d_segs, drift, fext,
-                                                                     E.d_vel_offs, rhs);
+            E.d_vel_offs, rhs);
     if (!drift) {
         if (E.ncoll)
             ps_launch(k_colloid_hs, (unsigned)E.ncoll, 32, 0, st, E.ncoll, E.d_coll_rep, E.d_segs, E.d_x,
-                                                                             E.d_chs);
+                    E.d_chs);
         ps_launch(k_forces, (unsigned)((E.ntot + thr - 1) / thr), thr, 0, st,
-            E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_cellgeo, E.d_cell_offs,
-            E.d_cell_start, E.d_cell_sorted, E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_time, E.d_ktrap,
-            E.d_trapinfo, E.d_chs, rhs);
+                E.ntot, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xpos0, E.d_cellgeo, E.d_cell_offs,
+                E.d_cell_start, E.d_cell_sorted, E.d_bond_ptr, E.d_bond_nbr, E.d_bond_sgn, E.d_time, E.d_ktrap,
+                E.d_trapinfo, E.d_chs, rhs);
         ps_launch(k_trap_weaken, (E.R + 127) / 128, 128, 0, st, E.R, E.d_segs, E.d_time, E.d_ktrap, E.d_trapinfo);
     }
     PS_CK(cudaGetLastError());
@@ -809,7 +809,7 @@ int stage_schur(Engine &E, cudaStream_t st)
     size_t smem = sizeof(double) * (2 * 64 * 64 + 64);
     PS_CK(cudaFuncSetAttribute(k_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ps_launch(k_schur, E.n_schur_reps, 256, smem, st, E.d_segs, E.d_schur_reps, E.d_x, E.d_delta, E.d_schurQ, E.d_schurL,
-                                                E.d_tab);
+            E.d_tab);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }
@@ -844,7 +844,7 @@ int diag_saddle(Engine &E, double *d, cudaStream_t st)
 {
     int thr = 256;
     ps_launch(k_diag, (unsigned)((E.nvec + thr - 1) / thr), thr, 0, st, E.nvec, E.d_vec_offs, E.R, E.d_segs, E.d_delta,
-                                                                 E.any_lub ? E.d_lub_diag : nullptr, d);
+            E.any_lub ? E.d_lub_diag : nullptr, d);
     PS_CK(cudaGetLastError());
     return PS_OK;
 }

@@ -73,11 +73,11 @@ int slip_noise(Engine &E, const double *fb, double *W, const ps_sqrt_opts *o, ps
     if (E.n_schur_reps || E.n_sl_reps) {
         int thr = 256;
         ps_launch(k_zero_colloid_dofs, (unsigned)((E.ntop + thr - 1) / thr), thr, 0, st, E.ntop, E.d_top_offs, E.R, E.d_segs,
-                                                                                  fb, E.d_tmp_top);
+                fb, E.d_tmp_top);
         apply_operator(E, 1, E.d_tmp_top, E.d_tmp_top2, nullptr, false, st);
         if (E.n_schur_reps)
             ps_launch(k_shell_noise, E.n_schur_reps, 128, 0, st, E.d_segs, E.d_schur_reps, fb, E.d_tmp_top2,
-                                                                               E.d_schurQ, E.d_schurL, W);
+                    E.d_schurQ, E.d_schurL, W);
         if (E.n_sl_reps) {
             // above the dense Schur limit: Lanczos on the colloid Schur complement
             int nneg = 0;
@@ -416,7 +416,7 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
         if ((rc = stage_rhs(E, 1, E.d_fext, E.d_rhs, st))) return rc;
         if ((rc = solve(E, E.d_rhs, E.d_Xd, 1, in, res, 3, st))) return rc;
         ps_launch(k_drift_fin, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xd, E.d_drift, E.d_ud,
-                                                     E.d_sb, E.d_X);
+                E.d_sb, E.d_X);
     } else {
         if ((rc = solve(E, E.d_rhs, E.d_X, 0, in, res, 1, st))) return rc;
         ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_X, E.d_up, 0);
@@ -431,10 +431,10 @@ int step_all(Engine &E, const ps_step_inputs *in, ps_step_result *res, cudaStrea
     if ((rc = solve(E, E.d_rhs, E.d_Xdet, 0, in, res, 4, st))) return rc;
     ps_launch(k_extract_vel, nb(E.nvel, thr), thr, 0, st, E.nvel, E.d_vel_offs, E.R, E.d_segs, E.d_Xdet, E.d_vdc, 0);
     ps_launch(k_step_corr, nb(n3, thr), thr, 0, st, n3, E.d_bead_offs, E.R, E.d_segs, E.d_x, E.d_xn, E.d_ud, E.d_up, E.d_vdn,
-                                             E.d_vdc, E.d_vb);
+            E.d_vdc, E.d_vb);
     if (E.ncoll)
         ps_launch(k_step_rot, nb(E.ncoll, 128), 128, 0, st, E.ncoll, E.d_segs, E.d_coll_rep, E.d_up, E.d_vdn, E.d_vdc, E.d_vb,
-                                                     E.d_q);
+                E.d_q);
     E.step_counter++;
     ps_launch(k_step_count, (E.R + 127) / 128, 128, 0, st, E.R, E.d_rstep);
     PS_CK(cudaGetLastError());
