@@ -5,7 +5,6 @@
 #include <cstdio>
 #include <cstdint>
 #include <cstring>
-#include <thread>
 #include <algorithm>
 #include <mutex>
 #include <string>
@@ -546,39 +545,16 @@ int ps_get_replica_steps(ps_ctx *ctx, uint64_t *steps)
     return PS_OK;
 }
 
-// index of the first non-finite value of v[0, n), or -1.  The exponent test runs
-// over the whole array without a branch (it vectorises), on up to eight threads
-// for large arrays; the search for the index runs only on failure, serially, so
-// the answer does not depend on the split.
-static bool any_nonfinite(const double *v, long a, long b)
+// index of the first non-finite value of v[0, n), or -1; the exponent test runs
+// over the whole array without a branch (it vectorises), the search only on failure
+static long first_nonfinite(const double *v, long n)
 {
     uint64_t bad = 0;
-    for (long i = a; i < b; i++) {
+    for (long i = 0; i < n; i++) {
         uint64_t u;
         std::memcpy(&u, v + i, sizeof u);
         bad |= (uint64_t)(((u >> 52) & 0x7ff) == 0x7ff);
     }
-    return bad != 0;
-}
-
-static long first_nonfinite(const double *v, long n)
-{
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int nt = n >= (1L << 19) ? (int)std::min<unsigned>(8u, hw ? hw : 1u) : 1;
-    std::vector<char> flag(nt, 0);
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; t++) {
-        const long a = n * t / nt, b = n * (t + 1) / nt;
-        try {
-            th.emplace_back([&flag, v, a, b, t] { flag[t] = any_nonfinite(v, a, b); });
-        } catch (...) {
-            flag[t] = any_nonfinite(v, a, b);   // no thread to be had: scan it here
-        }
-    }
-    flag[0] = any_nonfinite(v, 0, n / nt);
-    for (auto &x : th) x.join();
-    bool bad = false;
-    for (char f : flag) bad = bad || f != 0;
     if (!bad) return -1;
     for (long i = 0; i < n; i++)
         if (!std::isfinite(v[i])) return i;
@@ -612,17 +588,11 @@ int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
     if (!ctx || !x) return PS_ERR_ARG;
     Engine &E = ctx->E;
     cudaStream_t st = S(stream);
-    // host inputs are scanned before the state changes or a kernel runs: a non-finite
-    // coordinate would otherwise travel through the cell grid and every pair kernel.
-    // Host positions go first into the step's start-of-step copy (free between steps),
-    // so the transfer runs beside the scan; they replace the state only if it passes.
-    const size_t xbytes = sizeof(double) * 3 * E.ntot;
-    const bool xhost = ps::is_host_ptr(x);
-    if (xhost) {
-        PS_CK(cudaMemcpyAsync(E.d_xn, x, xbytes, cudaMemcpyHostToDevice, st));
+    // host inputs are scanned before anything is copied or launched: a non-finite
+    // coordinate would otherwise travel through the cell grid and every pair kernel
+    if (ps::is_host_ptr(x)) {
         const long i = first_nonfinite(x, 3 * E.ntot);
         if (i >= 0) {
-            cudaStreamSynchronize(st);   // the caller may reuse its buffer once this returns
             ps::set_error("non-finite position at index " + std::to_string(i));
             return PS_ERR_ARG;
         }
@@ -630,13 +600,11 @@ int ps_set_state(ps_ctx *ctx, const double *x, const double *q, void *stream)
     if (q && ps::is_host_ptr(q)) {
         const long i = first_nonfinite(q, 4 * E.ncoll);
         if (i >= 0) {
-            if (xhost) cudaStreamSynchronize(st);
             ps::set_error("non-finite quaternion at index " + std::to_string(i));
             return PS_ERR_ARG;
         }
     }
-    if (xhost) PS_CK(cudaMemcpyAsync(E.d_x, E.d_xn, xbytes, cudaMemcpyDeviceToDevice, st));
-    else PS_CK(cudaMemcpyAsync(E.d_x, x, xbytes, cudaMemcpyDefault, st));
+    PS_CK(cudaMemcpyAsync(E.d_x, x, sizeof(double) * 3 * E.ntot, cudaMemcpyDefault, st));
     const int thr = 128;
     const unsigned nbc = (unsigned)((E.ncoll + thr - 1) / thr);
     if (q) PS_CK(cudaMemcpyAsync(E.d_q, q, sizeof(double) * 4 * E.ncoll, cudaMemcpyDefault, st));
