@@ -201,3 +201,43 @@ def test_gpu_lub_device_noise_runs():
     assert np.all(np.isfinite(x))
     assert np.linalg.norm(x - sysm.x.ravel()) > 0
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", [0, 1])
+def test_gpu_lub_step_ragged_batch(solver):
+    """Three lubricated replicas in one context with 17, 0 and 27 near pairs (and
+    different gap and bonded options): one step with injected noise, each replica
+    against its own oracle run, at the single-replica bound."""
+    import torch
+    from polystokes_brownian_b200.engine import Batch
+    systems = [CASES["mixed"](),
+               with_lub(configs.small_mixed(seed=5, Nm_chain=(3, 4), Nc=2, mm_HI=1, spread=12.0), 0.5),
+               CASES["ensemble"]()]
+    fbs, wrs, zls, want = [], [], [], []
+    for i, s in enumerate(systems):
+        o = oracle_for(s)
+        o.stage()
+        npairs = len(o.lub_pairs()[0])
+        o = oracle_for(s)
+        rng = np.random.default_rng(40 + i)
+        fb = rng.normal(size=o.nm3nc11)
+        wr = rng.normal(size=o.nm3nc6)
+        zl = rng.normal(size=12 * npairs)
+        o.step(fb=fb, wrfd=wr, zlub=zl, rtol=1e-13)
+        fbs.append(fb)
+        wrs.append(wr)
+        zls.append(zl)
+        want.append((s.x.ravel().copy(), o.state()[0]))
+    assert [len(z) // 12 for z in zls] == [17, 0, 27]
+    b = Batch(systems)
+    b.step(fb=torch.from_numpy(np.concatenate(fbs)).cuda(), wrfd=torch.from_numpy(np.concatenate(wrs)).cuda(),
+           zlub=torch.from_numpy(np.concatenate(zls)).cuda(), rtol=1e-13, sqrt_kmax=64, sqrt_tol=1e-15,
+           solver=solver)
+    xg = b.state()[0]
+    for i, s in enumerate(systems):
+        x0, xo = want[i]
+        xr = b.seg(xg, i, "bead").cpu().numpy()
+        disp = np.linalg.norm(xo - x0)
+        assert np.linalg.norm(xr - xo) <= 5e-10 * disp, (i, np.linalg.norm(xr - xo), disp)
+    b.close()
